@@ -1,0 +1,710 @@
+/*
+ * oracle.c -- CPU restatement of the PAGANI hot path (FP64 where the text says
+ * so).  TEST INFRASTRUCTURE ONLY: this is the checker used by tests/, by
+ * __graft_entry__.smoke() and by bench.py's cpu_baseline/reference legs.  The
+ * product library never links it.
+ *
+ * Every function names the reference function it restates.  Paths are relative
+ * to the reference project root:
+ *   U/ = src/BNAPlatform-win64-cuda7.0-20151118/src/
+ *   W/ = src/BNAPlatform-weighted-network-win64-cuda7.0-20151118/src/
+ *
+ * Pinning: tests/test_oracle_ref.py compares these functions with the
+ * reference's own CPU sources compiled by oracle/Makefile into oracle/_ref/,
+ * and tests/golden/ holds fixtures generated from that compiled reference.
+ *
+ * Build: gcc -O2 -ffp-contract=off (no fused multiply-add anywhere).
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#include <limits.h>
+
+/* ---------------------------------------------------------------- z-score */
+/* Restates the normalisation loop of CorMat_gpu, U/CorMat/CUCorMat/CUCORMAT/
+ * CorMat.cu:34-53 (same as CorMat_cpu, CorMat.cpp:872-890): FP64 mean and
+ * root of the sum of squares, z = (x - mean) / s.  The reference stores z as
+ * float; the oracle keeps it in FP64.  A row with s == 0 (or NaN input) gives
+ * NaN r in the reference, which post_block (CorMat.cpp:821) then stores as 0;
+ * here the row becomes the zero vector so that every r involving it is 0. */
+int or_zscore(const float* bold, int N, int T, double* z)
+{
+    int zero = 0;
+    for (int i = 0; i < N; i++) {
+        double s1 = 0.0, s2 = 0.0;
+        for (int t = 0; t < T; t++) s1 += (double)bold[(int64_t)t * N + i];
+        s1 /= T;
+        for (int t = 0; t < T; t++) {
+            double d = (double)bold[(int64_t)t * N + i] - s1;
+            s2 += d * d;
+        }
+        s2 = sqrt(s2);
+        double* zi = z + (int64_t)i * T;
+        if (!(s2 > 0.0) || !isfinite(s2)) {
+            zero++;
+            for (int t = 0; t < T; t++) zi[t] = 0.0;
+            continue;
+        }
+        for (int t = 0; t < T; t++) zi[t] = ((double)bold[(int64_t)t * N + i] - s1) / s2;
+    }
+    return zero;
+}
+
+/* Range rule of post_block: unweighted keeps r in [-1, 1]
+ * (U/CorMat/CUCorMat/CUCORMAT/CorMat.cpp:821-822); weighted keeps r in
+ * (-1-1e-6, 1+1e-6) (W/CorMat/CUCorMat/CUCorMat/CorMat.cpp:821-822 with
+ * ep = 1e-6 from :17).  Anything else (including NaN) is stored as 0. */
+static inline double range_rule(double r, int weighted)
+{
+    if (weighted) return (r > -1.0 - 1e-6 && r < 1.0 + 1e-6) ? r : 0.0;
+    return (r >= -1.0 && r <= 1.0) ? r : 0.0;
+}
+
+double or_pair_r(const double* z, int T, int i, int j, int weighted)
+{
+    const double* a = z + (int64_t)i * T;
+    const double* b = z + (int64_t)j * T;
+    double r = 0.0;
+    for (int t = 0; t < T; t++) r += a[t] * b[t];
+    return range_rule(r, weighted);
+}
+
+/* Packed upper triangle, row-major, i < j: the .cormat layout
+ * (CorMat.cpp:285-294, manual p11). */
+void or_corr_packed(const double* z, int N, int T, int weighted, double* r)
+{
+    int64_t k = 0;
+    for (int i = 0; i < N; i++)
+        for (int j = i + 1; j < N; j++) r[k++] = or_pair_r(z, T, i, j, weighted);
+}
+
+/* Edge count for a sparsity threshold, exactly as main() computes it,
+ * CorMat.cpp:310-312: Clength = (long long)2*M1*s/100.0 -- the long long
+ * product is converted to float and multiplied by the float s in single
+ * precision before the double division -- then rounded up to even.  The
+ * number of undirected edges is Clength/2. */
+int64_t or_sparsity_k(int N, float s)
+{
+    long long M1 = (long long)(N - 1) * N / 2;
+    float prod = (float)(2LL * M1) * s;
+    long long Clength = (long long)((double)prod / 100.0);
+    Clength += Clength % 2;
+    return Clength / 2;
+}
+
+/* Weighted r threshold: W/CorMat/CUCorMat/CUCorMat/CorMat.cpp:310 passes
+ * r_thresh - ep (double) to a float parameter, so the effective threshold is
+ * the float nearest to thr - 1e-6. */
+float or_weighted_r_threshold(float thr) { return (float)((double)thr - 1e-6); }
+
+static inline double keyof(double r, int abs_mode) { return abs_mode ? fabs(r) : r; }
+
+/* Append undirected edge (i, j), i < j, in lexicographic pair order; rows end
+ * up with ascending columns, matching FormCSRGraph's O(N^2) scan
+ * (CorMat.cpp:839-857; weighted V from the packed r, W CorMat.cpp:853-882). */
+static int64_t build_csr(const double* r, int N, const unsigned char* keep, int abs_mode,
+                         int32_t* R, int32_t* C, float* V, int64_t cap)
+{
+    int64_t M1 = (int64_t)N * (N - 1) / 2;
+    int64_t* deg = (int64_t*)calloc((size_t)N + 1, sizeof(int64_t));
+    int64_t k = 0;
+    for (int i = 0; i < N; i++)
+        for (int j = i + 1; j < N; j++, k++)
+            if (keep[k]) { deg[i]++; deg[j]++; }
+    int64_t nnz = 0;
+    for (int i = 0; i < N; i++) nnz += deg[i];
+    if (nnz > cap || nnz > INT32_MAX) { free(deg); return -1; }
+    R[0] = 0;
+    for (int i = 0; i < N; i++) R[i + 1] = R[i] + (int32_t)deg[i];
+    int64_t* cur = deg;
+    for (int i = 0; i < N; i++) cur[i] = R[i];
+    k = 0;
+    for (int i = 0; i < N; i++)
+        for (int j = i + 1; j < N; j++, k++)
+            if (keep[k]) {
+                float w = (float)(abs_mode ? fabs(r[k]) : r[k]);
+                C[cur[i]] = j; if (V) V[cur[i]] = w; cur[i]++;
+                C[cur[j]] = i; if (V) V[cur[j]] = w; cur[j]++;
+            }
+    (void)M1;
+    free(deg);
+    return nnz;
+}
+
+/* r-threshold graph: FormFullGraph, CorMat.cpp:633-653 (strict r > thr).
+ * abs_mode thresholds |r| instead, as CorMat_CPU does
+ * (U/CorMat/CorMat_CPU/CorMat/CorMat_CPU.cpp:198). */
+int64_t or_graph_r(const double* r, int N, double thr, int abs_mode,
+                   int32_t* R, int32_t* C, float* V, int64_t cap)
+{
+    int64_t M1 = (int64_t)N * (N - 1) / 2;
+    unsigned char* keep = (unsigned char*)malloc((size_t)(M1 > 0 ? M1 : 1));
+    for (int64_t k = 0; k < M1; k++) keep[k] = keyof(r[k], abs_mode) > thr;
+    int64_t nnz = build_csr(r, N, keep, abs_mode, R, C, V, cap);
+    free(keep);
+    return nnz;
+}
+
+static int cmp_desc(const void* a, const void* b)
+{
+    double x = *(const double*)a, y = *(const double*)b;
+    return (x < y) - (x > y);
+}
+
+/* Sparsity graph: select + FormFullGraph_s, CorMat.cpp:655-773.  tau is the
+ * k-th largest key; every pair with key > tau is kept, and of the pairs with
+ * key == tau only the lexicographically first (k - #above) survive -- the
+ * reference pops the most recently pushed tie whenever the count exceeds k
+ * (:748-759), which leaves exactly the earliest ties. */
+int64_t or_graph_k(const double* r, int N, int64_t k, int abs_mode, double* tau,
+                   int32_t* R, int32_t* C, float* V, int64_t cap)
+{
+    int64_t M1 = (int64_t)N * (N - 1) / 2;
+    unsigned char* keep = (unsigned char*)calloc((size_t)(M1 > 0 ? M1 : 1), 1);
+    double t = INFINITY;
+    if (k > 0 && M1 > 0) {
+        if (k > M1) k = M1;
+        double* s = (double*)malloc((size_t)M1 * sizeof(double));
+        for (int64_t q = 0; q < M1; q++) s[q] = keyof(r[q], abs_mode);
+        qsort(s, (size_t)M1, sizeof(double), cmp_desc);
+        t = s[k - 1];
+        int64_t above = 0;
+        for (int64_t q = 0; q < M1; q++) above += s[q] > t;
+        free(s);
+        int64_t ties = k - above;
+        for (int64_t q = 0; q < M1; q++) {
+            double x = keyof(r[q], abs_mode);
+            if (x > t) keep[q] = 1;
+            else if (x == t && ties > 0) { keep[q] = 1; ties--; }
+        }
+    }
+    if (tau) *tau = t;
+    int64_t nnz = build_csr(r, N, keep, abs_mode, R, C, V, cap);
+    free(keep);
+    return nnz;
+}
+
+/* ----------------------------------------------------------------- degree */
+/* U/Degree/Degree/Degree.cpp:85-91: (float)R[k+1] - R[k]; isolated count.
+ * W/Degree/Degree/Degree.cpp:82-88: strength = float sum of V in CSR order. */
+void or_degree(const int32_t* R, const float* V, int N, float* deg, int32_t* isolated)
+{
+    int32_t iso = 0;
+    for (int k = 0; k < N; k++) {
+        if (V) {
+            float s = 0.0f;
+            for (int32_t e = R[k]; e < R[k + 1]; e++) s += V[e];
+            deg[k] = s;
+        } else {
+            deg[k] = (float)R[k + 1] - (float)R[k];
+        }
+        if (R[k + 1] == R[k]) iso++;
+    }
+    if (isolated) *isolated = iso;
+}
+
+/* ------------------------------------------------------- binary clustering */
+/* U/Cp/Cp/Cp.cpp:78-116: t_k = number of connected neighbour pairs,
+ * Cp[k] = (double)t / k / (k-1) * 2 stored as float, 0 when k < 2; mean over
+ * all N nodes (:64-72).  The mean here is the sequential FP64 sum of the
+ * float Cp values. */
+void or_cp_binary(const int32_t* R, const int32_t* C, int N, int64_t* tri, float* cp, double* mean)
+{
+    int32_t* mark = (int32_t*)malloc((size_t)N * sizeof(int32_t));
+    for (int i = 0; i < N; i++) mark[i] = -1;
+    double sum = 0.0;
+    for (int u = 0; u < N; u++) {
+        int32_t k = R[u + 1] - R[u];
+        for (int32_t e = R[u]; e < R[u + 1]; e++) mark[C[e]] = u;
+        int64_t twice = 0;
+        for (int32_t e = R[u]; e < R[u + 1]; e++) {
+            int32_t v = C[e];
+            for (int32_t f = R[v]; f < R[v + 1]; f++) twice += (mark[C[f]] == u);
+        }
+        int64_t t = twice / 2;
+        if (tri) tri[u] = t;
+        float c = 0.0f;
+        if (k >= 2) {
+            double x = (double)t;
+            x = x / k;
+            x = x / (k - 1);
+            x = x * 2;
+            c = (float)x;
+        }
+        cp[u] = c;
+        sum += (double)c;
+    }
+    free(mark);
+    if (mean) *mean = N > 0 ? sum / N : 0.0;
+}
+
+/* ------------------------------------------------------- Onnela clustering */
+/* W/Cp/Cp/Cp_2.cpp:23-130: w_hat = V / V_max (float division), per node the
+ * sum over connected neighbour pairs j < h of (w_hat_jh w_hat_kj w_hat_kh)^(1/3)
+ * (:123), Cp = 2 sum / k / (k-1) (:125).  vmax_first_n = 1 reproduces the
+ * reference CPU's maximum over V[0..N) only (:27-30); 0 takes the maximum over
+ * all edges as the GPU tool does (W/Cp_GPU/CUCP/Cp.cu cublasIsamax).  The
+ * per-node sum is FP64 here (the reference accumulates in float). */
+void or_onnela(const int32_t* R, const int32_t* C, const float* V, int N, int vmax_first_n,
+               float* cp, double* mean)
+{
+    int64_t nnz = R[N];
+    float vmax = 0.0f;
+    int64_t lim = vmax_first_n ? (N < nnz ? N : nnz) : nnz;
+    if (lim > 0) {
+        vmax = V[0];
+        for (int64_t e = 1; e < lim; e++) if (vmax < V[e]) vmax = V[e];
+    }
+    float* wh = (float*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(float));
+    for (int64_t e = 0; e < nnz; e++) wh[e] = V[e] / vmax;
+    float* roww = (float*)calloc((size_t)N, sizeof(float));
+    int32_t* mark = (int32_t*)malloc((size_t)N * sizeof(int32_t));
+    for (int i = 0; i < N; i++) mark[i] = -1;
+    double sum = 0.0;
+    for (int u = 0; u < N; u++) {
+        int32_t k = R[u + 1] - R[u];
+        for (int32_t e = R[u]; e < R[u + 1]; e++) { mark[C[e]] = u; roww[C[e]] = wh[e]; }
+        double acc = 0.0;
+        for (int32_t e = R[u]; e < R[u + 1]; e++) {
+            int32_t j = C[e];
+            for (int32_t f = R[j]; f < R[j + 1]; f++) {
+                int32_t h = C[f];
+                if (h > j && mark[h] == u && wh[f] != 0.0f)
+                    acc += pow((double)wh[f] * roww[j] * roww[h], 1.0 / 3);
+            }
+        }
+        float c = 0.0f;
+        if (k >= 2) c = (float)(2.0 * acc / k / (k - 1));
+        cp[u] = c;
+        sum += (double)c;
+    }
+    free(wh); free(roww); free(mark);
+    if (mean) *mean = N > 0 ? sum / N : 0.0;
+}
+
+/* ------------------------------------------------- BFS path length (hops) */
+/* U/BFS_MulCPU/BFS_MulCPU/APSP_BFS.cpp:27-192.  For every source a queue BFS
+ * gives hop counts; unreachable pairs contribute nothing.  inv_sum[s] =
+ * sum_v 1/d(s,v) (accumulated as sum_d count_d / d, d ascending);
+ * Li = inv_sum / (N-1) (:126); Lp = N(N-1) / sum_s inv_sum[s], which equals
+ * the reference's 1/(sum_{i<j} 1/d / N / (N-1)) / 2 (:135-138).
+ * hop_hist[d] counts ordered pairs at distance d (d <= max_hop).
+ * Returns the largest finite distance seen. */
+int or_bfs_paths(const int32_t* R, const int32_t* C, int N, double* inv_sum,
+                 int64_t* hop_hist, int max_hop, double* lp)
+{
+    int32_t* dist = (int32_t*)malloc((size_t)N * sizeof(int32_t));
+    int32_t* q = (int32_t*)malloc((size_t)N * sizeof(int32_t));
+    int64_t* cnt = (int64_t*)calloc((size_t)N + 1, sizeof(int64_t));
+    int maxd = 0;
+    double total = 0.0;
+    if (hop_hist) memset(hop_hist, 0, sizeof(int64_t) * (size_t)(max_hop + 1));
+    for (int s = 0; s < N; s++) {
+        for (int i = 0; i < N; i++) dist[i] = -1;
+        int head = 0, tail = 0, dmax = 0;
+        dist[s] = 0; q[tail++] = s;
+        while (head < tail) {
+            int v = q[head++];
+            for (int32_t e = R[v]; e < R[v + 1]; e++) {
+                int w = C[e];
+                if (dist[w] < 0) { dist[w] = dist[v] + 1; q[tail++] = w; cnt[dist[w]]++;
+                                   if (dist[w] > dmax) dmax = dist[w]; }
+            }
+        }
+        double acc = 0.0;
+        for (int d = 1; d <= dmax; d++) {
+            acc += (double)cnt[d] / d;
+            if (hop_hist && d <= max_hop) hop_hist[d] += cnt[d];
+            cnt[d] = 0;
+        }
+        if (dmax > maxd) maxd = dmax;
+        if (inv_sum) inv_sum[s] = acc;
+        total += acc;
+    }
+    if (lp) *lp = total > 0.0 ? (double)N * (N - 1) / total : 0.0;
+    free(dist); free(q); free(cnt);
+    return maxd;
+}
+
+/* Single-source hop distances and exact shortest-path counts (the forward
+ * half of Betweenness_CPU, U/BC/BC_CPU/BC_CPU/BC_CPU.cpp:37-56, with the
+ * float sigma replaced by a 64-bit integer). */
+int or_bfs_source(const int32_t* R, const int32_t* C, int N, int s, int32_t* dist, int64_t* sigma)
+{
+    int32_t* q = (int32_t*)malloc((size_t)N * sizeof(int32_t));
+    for (int i = 0; i < N; i++) { dist[i] = -1; sigma[i] = 0; }
+    int head = 0, tail = 0, dmax = 0;
+    dist[s] = 0; sigma[s] = 1; q[tail++] = s;
+    while (head < tail) {
+        int v = q[head++];
+        for (int32_t e = R[v]; e < R[v + 1]; e++) {
+            int w = C[e];
+            if (dist[w] < 0) { dist[w] = dist[v] + 1; q[tail++] = w; if (dist[w] > dmax) dmax = dist[w]; }
+            if (dist[w] == dist[v] + 1) sigma[w] += sigma[v];
+        }
+    }
+    free(q);
+    return dmax;
+}
+
+/* ------------------------------------------------------------- betweenness */
+/* Brandes, U/BC/BC_CPU/BC_CPU/BC_CPU.cpp:6-82: every vertex is a source and
+ * BC[w] += delta[w] for w != s, i.e. the sum over ORDERED pairs (twice the
+ * undirected textbook value).  sigma is exact int64 and delta FP64 (the
+ * reference uses float for both). */
+void or_brandes(const int32_t* R, const int32_t* C, int N, double* bc)
+{
+    int32_t* dist = (int32_t*)malloc((size_t)N * sizeof(int32_t));
+    int64_t* sigma = (int64_t*)malloc((size_t)N * sizeof(int64_t));
+    double* delta = (double*)malloc((size_t)N * sizeof(double));
+    int32_t* order = (int32_t*)malloc((size_t)N * sizeof(int32_t));
+    for (int i = 0; i < N; i++) bc[i] = 0.0;
+    for (int s = 0; s < N; s++) {
+        for (int i = 0; i < N; i++) { dist[i] = -1; sigma[i] = 0; delta[i] = 0.0; }
+        int head = 0, tail = 0;
+        dist[s] = 0; sigma[s] = 1; order[tail++] = s;
+        while (head < tail) {
+            int v = order[head++];
+            for (int32_t e = R[v]; e < R[v + 1]; e++) {
+                int w = C[e];
+                if (dist[w] < 0) { dist[w] = dist[v] + 1; order[tail++] = w; }
+                if (dist[w] == dist[v] + 1) sigma[w] += sigma[v];
+            }
+        }
+        for (int p = tail - 1; p >= 0; p--) {
+            int w = order[p];
+            double acc = 0.0;
+            for (int32_t e = R[w]; e < R[w + 1]; e++) {
+                int v = C[e];
+                if (dist[v] == dist[w] + 1) acc += (1.0 + delta[v]) / (double)sigma[v];
+            }
+            delta[w] = (double)sigma[w] * acc;
+            if (w != s) bc[w] += delta[w];
+        }
+    }
+    free(dist); free(sigma); free(delta); free(order);
+}
+
+/* ------------------------------------------------------- Floyd-Warshall */
+/* Min-plus closure in FP32, BFW_one_block_C, W/Lp/CUBFW_Lp/CUBFW_Lp/BFW.cpp:26-39,
+ * applied to one block covering the whole matrix (classic k-outer order). */
+void or_fw_dense(float* d, int n)
+{
+    for (int k = 0; k < n; k++) {
+        const float* dk = d + (int64_t)k * n;
+        for (int i = 0; i < n; i++) {
+            float* di = d + (int64_t)i * n;
+            float dik = di[k];
+            for (int j = 0; j < n; j++) {
+                float c = dik + dk[j];
+                if (c < di[j]) di[j] = c;
+            }
+        }
+    }
+}
+
+/* Weighted path length: CUBFW_Lp, W/Lp/CUBFW_Lp/CUBFW_Lp/CUBFW_Lp.cpp:13-162.
+ * Distance of an edge is 1/w (float, init_block FormBlock.cpp:64), 0 on the
+ * diagonal, infinity elsewhere; APSP by min-plus; distances below 0.1 are
+ * skipped (:77); eff[u] = sum_v 1/d(u,v) / (N-1), set to 0 when below 1/N
+ * (:99-104); Lp = N(N-1) / sum_{u != v} 1/d (:107-109).  Sums are FP64. */
+int or_weighted_paths(const int32_t* R, const int32_t* C, const float* V, int N,
+                      float* eff, double* lp)
+{
+    float* d = (float*)malloc((size_t)N * N * sizeof(float));
+    if (!d) return -1;
+    for (int64_t q = 0; q < (int64_t)N * N; q++) d[q] = INFINITY;
+    for (int i = 0; i < N; i++)
+        for (int32_t e = R[i]; e < R[i + 1]; e++) d[(int64_t)i * N + C[e]] = 1.0f / V[e];
+    for (int i = 0; i < N; i++) d[(int64_t)i * N + i] = 0.0f;
+    or_fw_dense(d, N);
+    double total = 0.0;
+    for (int u = 0; u < N; u++) {
+        double acc = 0.0;
+        for (int v = 0; v < N; v++) {
+            if (u == v) continue;
+            float x = d[(int64_t)u * N + v];
+            if (x < 0.1f) continue;
+            acc += 1.0 / (double)x;
+        }
+        total += acc;
+        float e = (float)(acc / (N - 1));
+        if (e < 1.0f / N) e = 0.0f;
+        if (eff) eff[u] = e;
+    }
+    if (lp) *lp = total > 0.0 ? 1.0 / (total / N / (N - 1)) : INFINITY;
+    free(d);
+    return 0;
+}
+
+/* ------------------------------------------------------ Newman modularity */
+/* Leading-eigenvector bisection, restating Partition / Sub_Partition /
+ * Lead_Vector of U/cuda_EC/cuda_EC/Modularity_CPU.cpp:48-298 with the
+ * constants of :18-25 (MAX_ITER 10000, Epsilon 1e-6, LAMBDA 0.01,
+ * MIN_GROUP 1) and the start vector v[i] = original node id (RANDOM_V0, :242).
+ * The tool (modularity_GPU.cu:488) sends sub-graphs with more than 25,000
+ * nodes to Sub_Partition_GPU, whose only rule change is the shift condition
+ * lambda < -LAMBDA instead of lambda < 0 (modularity_GPU.cu:374 vs
+ * Modularity_CPU.cpp:177); gpu_rule_above selects that threshold.
+ * Q (:116-124) is computed from module degree sums: identical in exact
+ * arithmetic to the reference's O(N^2) double loop. */
+typedef struct {
+    int N, M;
+    const int32_t* R;
+    double *v, *v0, *vv, *sumBG;
+    int last_iter;
+    double last_res;
+} nm_state;
+
+static double nm_norm(const double* x, int n)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += x[i] * x[i];
+    return sqrt(s);
+}
+
+static double nm_lead_vector(nm_state* st, const int32_t* sR, const int32_t* sC, int n,
+                             const int32_t* AD, double beta)
+{
+    const int32_t* R = st->R;
+    double *v = st->v, *v0 = st->v0, *vv = st->vv, *sumBG = st->sumBG;
+    int M = st->M;
+    for (int i = 0; i < n; i++) v[i] = AD[i];
+    double err1 = 1, err2 = 1, vNorm = 0;
+    int iter = 0;
+    double* verr = (double*)malloc((size_t)(n > 0 ? n : 1) * sizeof(double));
+    while (err1 > 1e-6 && err2 > 1e-6 && iter < 10000) {
+        for (int i = 0; i < n; i++) { v0[i] = v[i]; vv[AD[i]] = v[i]; }
+        double v_k = 0;
+        for (int i = 0; i < n; i++) v_k += v0[i] * (R[AD[i] + 1] - R[AD[i]]);
+        for (int i = 0; i < n; i++) {
+            double t = 0;
+            for (int32_t j = sR[i]; j < sR[i + 1]; j++) t += vv[sC[j]];
+            t -= v_k / 2 / M * (R[AD[i] + 1] - R[AD[i]]) + (sumBG[i] - beta) * v0[i];
+            v[i] = t;
+        }
+        vNorm = nm_norm(v, n);
+        for (int i = 0; i < n; i++) v[i] = v[i] / vNorm;
+        for (int i = 0; i < n; i++) verr[i] = v[i] - v0[i];
+        err1 = nm_norm(verr, n);
+        for (int i = 0; i < n; i++) verr[i] = v[i] + v0[i];
+        err2 = nm_norm(verr, n);
+        iter++;
+    }
+    free(verr);
+    st->last_iter = iter;
+    st->last_res = err1 < err2 ? err1 : err2;
+    int mx = 0;
+    for (int i = 0; i < n; i++) if (fabs(v[i]) > fabs(v[mx])) mx = i;
+    return (v[mx] * v0[mx] > 0) ? vNorm : -vNorm;
+}
+
+int or_newman(const int32_t* R, const int32_t* C, int N, int gpu_rule_above,
+              int32_t* labels, double* Qout, int* n_modules, int* n_rounds)
+{
+    int M = R[N] / 2;
+    nm_state st;
+    st.N = N; st.M = M; st.R = R;
+    st.v = (double*)calloc((size_t)N + 1, sizeof(double));
+    st.v0 = (double*)calloc((size_t)N + 1, sizeof(double));
+    st.vv = (double*)calloc((size_t)N + 1, sizeof(double));
+    st.sumBG = (double*)calloc((size_t)N + 1, sizeof(double));
+    int32_t* Result = labels;
+    int32_t* Adjust = (int32_t*)calloc((size_t)N + 2, sizeof(int32_t));
+    int32_t* AD = (int32_t*)malloc((size_t)(N + 1) * sizeof(int32_t));
+    int32_t* sR = (int32_t*)malloc((size_t)(N + 1) * sizeof(int32_t));
+    int32_t* sC = (int32_t*)malloc((size_t)(R[N] > 0 ? R[N] : 1) * sizeof(int32_t));
+    unsigned char* G = (unsigned char*)malloc((size_t)(N > 0 ? N : 1));
+    memset(Result, 0, sizeof(int32_t) * (size_t)N);
+    int Round = 0, Max_Result = 0, Module_Num = 1, Index = 1;
+    while (Round <= Max_Result) {
+        long long innerM = 2LL * M;
+        int NumG = 0;
+        for (int i = 0; i < N; i++) {
+            G[i] = (Result[i] == Round);
+            if (G[i]) { AD[NumG++] = i; continue; }
+            innerM -= R[i + 1] - R[i];
+        }
+        int nc = 0, nr = 0;
+        sR[nr++] = 0;
+        for (int i = 0; i < N; i++) {
+            if (!G[i]) continue;
+            for (int32_t j = R[i]; j < R[i + 1]; j++) if (G[C[j]]) sC[nc++] = C[j];
+            sR[nr++] = nc;
+        }
+        if (NumG) {
+            int n = NumG;
+            for (int i = 0; i < n; i++)
+                st.sumBG[i] = (sR[i + 1] - sR[i]) - (R[AD[i] + 1] - R[AD[i]]) * (double)innerM / 2 / M;
+            double lambda = nm_lead_vector(&st, sR, sC, n, AD, 0.0);
+            double shift_below = (n > gpu_rule_above) ? -0.01 : 0.0;
+            if (lambda < shift_below) lambda += nm_lead_vector(&st, sR, sC, n, AD, -lambda);
+            long long subP = 0, subN = 0;
+            for (int i = 0; i < n; i++) { subP += st.v[i] > 0; subN += st.v[i] <= 0; }
+            int Issub = (lambda > 0.01 && subP > 1 && subN > 1);
+            if (Issub) {
+                for (int i = 0; i < n; i++)
+                    Result[AD[i]] = Max_Result + 1 + (st.v[i] * (subP - subN + 0.5) <= 0);
+                Max_Result += 2;
+            } else {
+                Adjust[Round] = Index++;
+            }
+            Module_Num += Issub;
+        }
+        Round++;
+    }
+    /* Q from module degree sums (before relabelling). */
+    double Q = 0.0;
+    if (M > 0) {
+        int64_t inside = 0;
+        double* Kc = (double*)calloc((size_t)Max_Result + 2, sizeof(double));
+        for (int i = 0; i < N; i++) {
+            for (int32_t j = R[i]; j < R[i + 1]; j++) inside += Result[i] == Result[C[j]];
+            Kc[Result[i]] += R[i + 1] - R[i];
+        }
+        double sq = 0.0;
+        for (int c = 0; c <= Max_Result; c++) sq += Kc[c] * Kc[c];
+        Q = ((double)inside - sq / 2 / M) / (2.0 * M);
+        free(Kc);
+    }
+    for (int i = 0; i < N; i++) Result[i] = Adjust[Result[i]];
+    if (Qout) *Qout = Q;
+    if (n_modules) *n_modules = Module_Num;
+    if (n_rounds) *n_rounds = Round;
+    free(st.v); free(st.v0); free(st.vv); free(st.sumBG);
+    free(Adjust); free(AD); free(sR); free(sC); free(G);
+    return 0;
+}
+
+/* --------------------------------------------------------- Maslov rewiring */
+/* Degree-preserving double-edge swaps, restating Rewire/Maslov of
+ * U/cuda_EC/cuda_EC/Maslov.cpp:8-109 and the weighted variant
+ * Maslov_weighted_1, W/Maslov/Maslov/Maslov.cpp:50-196 (weights stay with the
+ * edge slot that carries them).  The reference draws from srand(time(0)) /
+ * rand(); this restatement uses a seeded counter-based generator and runs the
+ * attempts in rounds of B = pg_maslov_round_size(M): inside a round every
+ * attempt reads the state left by the previous round, valid attempts claim
+ * their four end points (lowest attempt index wins) and only attempts that
+ * own all four commit.  Committed attempts of one round touch disjoint
+ * vertices and slots, so they commute.  This is the exact schedule of the
+ * GPU kernel, which makes the two bit-identical for the same seed. */
+static inline uint64_t mix64(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+int64_t or_maslov_round_size(int64_t M);
+int64_t or_maslov_round_size(int64_t M)
+{
+    int64_t b = M / 16;
+    if (b < 1) b = 1;
+    if (b > 65536) b = 65536;
+    return b;
+}
+
+static inline int has_edge(const uint64_t* bits, int64_t N, int a, int b)
+{
+    uint64_t q = (uint64_t)a * (uint64_t)N + (uint64_t)b;
+    return (int)((bits[q >> 6] >> (q & 63)) & 1ULL);
+}
+static inline void set_edge(uint64_t* bits, int64_t N, int a, int b, int on)
+{
+    uint64_t q = (uint64_t)a * (uint64_t)N + (uint64_t)b;
+    if (on) bits[q >> 6] |= 1ULL << (q & 63); else bits[q >> 6] &= ~(1ULL << (q & 63));
+}
+
+int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uint64_t seed,
+                  int64_t attempts, int32_t* R_out, int32_t* C_out, float* V_out)
+{
+    int64_t M = R[N] / 2;
+    int32_t* ea = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
+    int32_t* eb = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
+    float* ew = (float*)malloc((size_t)(M > 0 ? M : 1) * sizeof(float));
+    size_t words = (size_t)(((uint64_t)N * (uint64_t)N + 63) / 64);
+    uint64_t* bits = (uint64_t*)calloc(words > 0 ? words : 1, sizeof(uint64_t));
+    int64_t m = 0;
+    for (int i = 0; i < N; i++)
+        for (int32_t e = R[i]; e < R[i + 1]; e++) {
+            set_edge(bits, N, i, C[e], 1);
+            if (C[e] > i) { ea[m] = i; eb[m] = C[e]; ew[m] = V ? V[e] : 1.0f; m++; }
+        }
+    int64_t committed = 0;
+    int64_t B = or_maslov_round_size(M);
+    int64_t* owner = (int64_t*)malloc((size_t)(N > 0 ? N : 1) * sizeof(int64_t));
+    for (int i = 0; i < N; i++) owner[i] = INT64_MAX;
+    int32_t* av = (int32_t*)malloc((size_t)B * 4 * sizeof(int32_t));
+    int64_t* ai = (int64_t*)malloc((size_t)B * 2 * sizeof(int64_t));
+    unsigned char* ok = (unsigned char*)malloc((size_t)B);
+    unsigned char* coin = (unsigned char*)malloc((size_t)B);
+    for (int64_t base = 0; M >= 2 && base < attempts; base += B) {
+        int64_t nb = attempts - base < B ? attempts - base : B;
+        for (int64_t a = 0; a < nb; a++) {
+            uint64_t idx = (uint64_t)(base + a);
+            uint64_t h1 = mix64(seed ^ (2 * idx)), h2 = mix64(seed ^ (2 * idx + 1));
+            int64_t i = (int64_t)(h1 % (uint64_t)M), j = (int64_t)(h2 % (uint64_t)M);
+            int c = (int)((h1 >> 63) ^ (h2 >> 63));
+            int V1 = ea[i], V2 = eb[i], V3 = ea[j], V4 = eb[j];
+            int valid = !(V1 == V3 || V1 == V4 || V2 == V3 || V2 == V4);
+            if (valid) {
+                if (c) valid = !(has_edge(bits, N, V1, V3) || has_edge(bits, N, V2, V4));
+                else   valid = !(has_edge(bits, N, V1, V4) || has_edge(bits, N, V2, V3));
+            }
+            av[4 * a] = V1; av[4 * a + 1] = V2; av[4 * a + 2] = V3; av[4 * a + 3] = V4;
+            ai[2 * a] = i; ai[2 * a + 1] = j; ok[a] = (unsigned char)valid; coin[a] = (unsigned char)c;
+            if (valid)
+                for (int q = 0; q < 4; q++) if (owner[av[4 * a + q]] > (int64_t)a) owner[av[4 * a + q]] = a;
+        }
+        for (int64_t a = 0; a < nb; a++) {
+            if (!ok[a]) continue;
+            int own = 1;
+            for (int q = 0; q < 4; q++) own &= owner[av[4 * a + q]] == a;
+            if (!own) continue;
+            int V1 = av[4 * a], V2 = av[4 * a + 1], V3 = av[4 * a + 2], V4 = av[4 * a + 3];
+            int64_t i = ai[2 * a], j = ai[2 * a + 1];
+            set_edge(bits, N, V1, V2, 0); set_edge(bits, N, V2, V1, 0);
+            set_edge(bits, N, V3, V4, 0); set_edge(bits, N, V4, V3, 0);
+            if (coin[a]) {   /* 1-3, 2-4 (Maslov.cpp:31-42) */
+                set_edge(bits, N, V1, V3, 1); set_edge(bits, N, V3, V1, 1);
+                set_edge(bits, N, V2, V4, 1); set_edge(bits, N, V4, V2, 1);
+                eb[i] = V3; ea[j] = V2;
+            } else {         /* 1-4, 3-2 (Maslov.cpp:44-55) */
+                set_edge(bits, N, V1, V4, 1); set_edge(bits, N, V4, V1, 1);
+                set_edge(bits, N, V2, V3, 1); set_edge(bits, N, V3, V2, 1);
+                eb[i] = V4; eb[j] = V2;
+            }
+            committed++;
+        }
+        for (int64_t a = 0; a < nb; a++)
+            for (int q = 0; q < 4; q++) owner[av[4 * a + q]] = INT64_MAX;
+    }
+    /* Rebuild CSR with ascending columns; each undirected slot's weight goes to
+     * both directions (Maslov_weighted_1's vu/vl re-attachment, :160-186). */
+    int64_t* cur = (int64_t*)malloc((size_t)(N + 1) * sizeof(int64_t));
+    for (int i = 0; i <= N; i++) R_out[i] = R[i];
+    int32_t* tmpc = (int32_t*)malloc((size_t)(R[N] > 0 ? R[N] : 1) * sizeof(int32_t));
+    float* tmpw = (float*)malloc((size_t)(R[N] > 0 ? R[N] : 1) * sizeof(float));
+    for (int i = 0; i < N; i++) cur[i] = R[i];
+    for (int64_t e = 0; e < M; e++) {
+        int a = ea[e], b = eb[e];
+        tmpc[cur[a]] = b; tmpw[cur[a]] = ew[e]; cur[a]++;
+        tmpc[cur[b]] = a; tmpw[cur[b]] = ew[e]; cur[b]++;
+    }
+    /* sort each row by column (insertion sort is fine for oracle sizes) */
+    for (int i = 0; i < N; i++) {
+        for (int32_t x = R[i] + 1; x < R[i + 1]; x++) {
+            int32_t c = tmpc[x]; float w = tmpw[x]; int32_t y = x - 1;
+            while (y >= R[i] && tmpc[y] > c) { tmpc[y + 1] = tmpc[y]; tmpw[y + 1] = tmpw[y]; y--; }
+            tmpc[y + 1] = c; tmpw[y + 1] = w;
+        }
+    }
+    memcpy(C_out, tmpc, sizeof(int32_t) * (size_t)R[N]);
+    if (V_out) memcpy(V_out, tmpw, sizeof(float) * (size_t)R[N]);
+    free(tmpc); free(tmpw); free(cur);
+    free(ea); free(eb); free(ew); free(bits); free(owner); free(av); free(ai); free(ok); free(coin);
+    return committed;
+}
