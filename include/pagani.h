@@ -1,0 +1,192 @@
+/*
+ * pagani.h -- C ABI of the B200-native PAGANI hot path (libpagani.so).
+ *
+ * The reference has no library API: its boundary is a set of console tools
+ * that exchange .nii/.csr/.nm files, and inside each tool a C function with
+ * host pointers does the work.  Every entry point below names the reference
+ * function it replaces (paths relative to the reference project root,
+ *   U/ = src/BNAPlatform-win64-cuda7.0-20151118/src/,
+ *   W/ = src/BNAPlatform-weighted-network-win64-cuda7.0-20151118/src/).
+ *
+ * Conventions
+ *   - every call returns pg_status and never exits, blocks on stdin or
+ *     prints; pg_last_error() holds the message of the last failure;
+ *   - plain pointers and sizes only; host pointers unless a flag says the
+ *     pointer is device memory of the context's GPU;
+ *   - one pg_ctx per host thread; a context owns one CUDA stream and a
+ *     device workspace that is reused across calls;
+ *   - graphs (pg_graph) are device-resident CSR: row offsets R[n+1],
+ *     ascending column indices C[nnz], optional float weights V[nnz];
+ *     undirected graphs store both directions and no self loops, exactly
+ *     as the reference .csr format (manual p10).
+ */
+#ifndef PAGANI_H
+#define PAGANI_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PG_OK = 0,
+    PG_ERR_INVALID = 1,       /* bad argument */
+    PG_ERR_CUDA = 2,          /* CUDA runtime error (message in pg_last_error) */
+    PG_ERR_NOMEM = 3,         /* device allocation failed */
+    PG_ERR_TOO_LARGE = 4,     /* result does not fit the 32-bit CSR format */
+    PG_ERR_INTERNAL = 5,      /* an internal consistency check failed */
+    PG_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up */
+    PG_ERR_NO_DEVICE = 7      /* no usable sm_100 device */
+} pg_status;
+
+typedef struct pg_ctx pg_ctx;
+typedef struct pg_graph pg_graph;
+
+typedef enum { PG_THRESH_R = 0, PG_THRESH_SPARSITY = 1 } pg_thresh_mode;
+typedef enum { PG_SIGNED = 0, PG_ABS = 1 } pg_sign;
+typedef enum { PG_FP32 = 0, PG_SPLIT_BF16 = 1 } pg_precision;
+
+/* ------------------------------------------------------------- context */
+pg_status   pg_create(pg_ctx** ctx, int device);
+pg_status   pg_destroy(pg_ctx* ctx);
+const char* pg_last_error(const pg_ctx* ctx);
+const char* pg_status_string(pg_status s);
+pg_status   pg_synchronize(pg_ctx* ctx);
+/* The cudaStream_t the context issues its work on. */
+void*       pg_stream(pg_ctx* ctx);
+/* Number of kernel launches issued by this context so far. */
+int64_t     pg_launch_count(const pg_ctx* ctx);
+
+/* ------------------------------------------------------------- graphs */
+/* Replaces the .csr reads of every metric tool (e.g. U/Cp/Cp/Cp_main.cpp:107-116,
+ * W/Lp/CUBFW_Lp/CUBFW_Lp/CUBFW_Lp_main.cpp:100-118).  V may be NULL
+ * (binary graph).  on_device != 0: R/C/V are device pointers. */
+pg_status pg_graph_from_csr(pg_ctx* ctx, const int32_t* R, const int32_t* C, const float* V,
+                            int32_t n, int64_t nnz, int32_t on_device, pg_graph** out);
+pg_status pg_graph_info(const pg_graph* g, int32_t* n, int64_t* nnz, int32_t* weighted);
+/* Copy the CSR out (host or device buffers sized n+1 / nnz / nnz). */
+pg_status pg_graph_to_csr(pg_ctx* ctx, const pg_graph* g, int32_t* R, int32_t* C, float* V,
+                          int32_t on_device);
+pg_status pg_graph_free(pg_graph* g);
+
+/* ------------------------------------------------- network construction */
+typedef struct {
+    int32_t mode;            /* pg_thresh_mode */
+    double  value;           /* r threshold (edge iff key > value) or sparsity in percent */
+    int32_t sign;            /* pg_sign: key = r (GPU tool) or |r| (CorMat_CPU) */
+    int32_t precision;       /* pg_precision of the Gram tiles */
+    int32_t weighted;        /* store V = key, weighted range rule (-1-1e-6, 1+1e-6) */
+    double  guard;           /* half-width of the FP64 recheck band around the threshold */
+    int32_t input_on_device; /* bold is a device pointer */
+    int32_t exact_weights;   /* weighted: V recomputed in FP64 for every edge */
+} pg_build_opts;
+
+typedef struct {
+    double  tau;             /* threshold actually applied (k-th key in sparsity mode) */
+    int64_t edges;           /* undirected edges kept */
+    int64_t band_pairs;      /* pairs decided by the FP64 recheck */
+    int64_t above_pairs;     /* pairs decided by the Gram tile alone */
+    int32_t zero_variance;   /* voxels with zero variance (their r is 0) */
+    double  sparsity_percent;/* 100 * edges / M1 */
+    double  ms_zscore, ms_hist, ms_emit, ms_select, ms_csr; /* device time per stage */
+} pg_build_info;
+
+/* Defaults: r mode 0.3, signed, split-BF16, binary, guard 2e-3, host input. */
+void pg_build_opts_default(pg_build_opts* o);
+
+/* Network construction of CUCorMat: replaces CorMat_gpu (U/CorMat/CUCorMat/
+ * CUCORMAT/CorMat.cu:18) + post_block (CorMat.cpp:775) + FormFullGraph (:633)
+ * / select + FormFullGraph_s (:655-773) + FormCSRGraph (:839); weighted
+ * variant W/CorMat/CUCorMat/CUCorMat/CorMat.cpp:647-882.  bold is time-major
+ * T x N float32 (BOLD[t*N + i], CorMat.cpp:208-231).  The correlation matrix
+ * is never materialised.  The edge set equals the FP64 oracle's: r is
+ * decided from the tensor/FP32 tile unless it lies within `guard` of the
+ * threshold (or of +-1), in which case it is recomputed in FP64. */
+pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, int32_t T,
+                         const pg_build_opts* opts, pg_graph** out, pg_build_info* info);
+
+/* Number of undirected edges for a sparsity of s percent, as CUCorMat's
+ * main() computes it (CorMat.cpp:310-312). */
+int64_t pg_sparsity_edges(int32_t N, float s_percent);
+
+/* Packed upper-triangle r (M1 = N(N-1)/2 floats, row-major i<j): the
+ * .cormat payload written when save_cormat = y (CorMat.cpp:285-294).
+ * r is rounded from the FP64 value. Output is a host buffer. */
+pg_status pg_correlation_packed(pg_ctx* ctx, const float* bold, int32_t N, int32_t T,
+                                int32_t weighted, int32_t input_on_device, float* r_packed);
+
+/* -------------------------------------------------------------- metrics */
+/* Degree (U/Degree/Degree/Degree.cpp:85-91) or strength for weighted graphs
+ * (W/Degree/Degree/Degree.cpp:82-88).  deg: host float[n]. */
+pg_status pg_degree(pg_ctx* ctx, const pg_graph* g, float* deg, int32_t* isolated);
+
+/* Clustering coefficient.  kind 0: binary, Cp (U/Cp/Cp/Cp.cpp:21-116);
+ * triangles (int64[n], optional) are exact.  kind 1: Onnela weighted,
+ * Cp_2 (W/Cp/Cp/Cp_2.cpp:23-130); flags bit 0 = take the weight maximum over
+ * V[0..n) only, as the reference CPU does.  cp: host float[n]; mean over all
+ * n nodes. */
+pg_status pg_clustering(pg_ctx* ctx, const pg_graph* g, int32_t kind, int32_t flags,
+                        float* cp, int64_t* triangles, double* mean);
+
+/* Hop path length and nodal efficiency: APSP_BFS (U/BFS_MulCPU/BFS_MulCPU/
+ * APSP_BFS.cpp:27-147).  eff[i] = sum_j 1/d_ij / (n-1) (float, optional),
+ * inv_sum[i] = sum_j 1/d_ij (double, optional), lp = n(n-1)/sum_ij 1/d_ij,
+ * hop_hist[d] = ordered pairs at distance d for d <= max_hop (optional),
+ * diameter = largest finite distance. */
+pg_status pg_paths(pg_ctx* ctx, const pg_graph* g, float* eff, double* inv_sum, double* lp,
+                   int64_t* hop_hist, int32_t max_hop, int32_t* diameter);
+
+/* Brandes betweenness from all sources: replaces CUBC (U/BC/CUBC/CUBC.cpp:13)
+ * and Betweenness_CPU (U/BC/BC_CPU/BC_CPU/BC_CPU.cpp:6).  Sum over ordered
+ * source/target pairs, as the reference.  Path counts are exact int64,
+ * dependencies FP64.  bc: host float[n] (optional), bc64: host double[n]
+ * (optional).  When eff/lp are given, the hop path length of pg_paths is
+ * produced from the same BFS sweep. */
+pg_status pg_betweenness(pg_ctx* ctx, const pg_graph* g, float* bc, double* bc64,
+                         float* eff, double* lp);
+
+/* Exact single-source hop distances (-1 = unreachable) and shortest-path
+ * counts for ns sources: dist int32[ns*n], sigma int64[ns*n] (host). */
+pg_status pg_bfs_sigma(pg_ctx* ctx, const pg_graph* g, const int32_t* sources, int32_t ns,
+                       int32_t* dist, int64_t* sigma);
+
+/* Weighted path length by blocked Floyd-Warshall on d = 1/w: CUBFW_Lp
+ * (W/Lp/CUBFW_Lp/CUBFW_Lp/CUBFW_Lp.cpp:13-162, cuAPSP CUBFW.cpp:19).
+ * dist: host float[n*n] (optional, row-major), eff: host float[n], lp. */
+pg_status pg_fw_paths(pg_ctx* ctx, const pg_graph* g, float* dist, float* eff, double* lp);
+
+/* Batched weighted path length + Onnela clustering for many small graphs in
+ * grouped launches (one FW sweep over all graphs).  eff and cp are
+ * concatenated per graph (sum of n floats each); lp and cp_mean per graph. */
+pg_status pg_fw_batched(pg_ctx* ctx, const pg_graph* const* graphs, int32_t count,
+                        float* eff, double* lp, float* cp, double* cp_mean);
+
+/* Newman leading-eigenvector modularity: Partition_GPU / Sub_Partition_GPU /
+ * Lead_Vector_GPU (U/cuda_EC/cuda_EC/modularity_GPU.cu:230-530) with the CPU
+ * variant's rules for sub-graphs of at most gpu_rule_above nodes
+ * (Modularity_CPU.cpp:48-298).  labels: host int32[n] numbered from 1 in
+ * division order; Q in FP64.  log (optional) receives one line per round. */
+typedef void (*pg_log_fn)(const char* line, void* user);
+pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_above, int32_t* labels,
+                    double* Q, int32_t* n_modules, pg_log_fn log, void* user);
+
+/* Maslov-Sneppen degree-preserving rewiring: Maslov/Rewire (U/cuda_EC/cuda_EC/
+ * Maslov.cpp:8-109) and Maslov_weighted_1 (W/Maslov/Maslov/Maslov.cpp:106-196).
+ * `attempts` swap attempts from a seeded counter-based generator, in rounds
+ * of pg_maslov_round_size(M) attempts.  Weights stay with their edge slot. */
+pg_status pg_maslov(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t attempts,
+                    pg_graph** out, int64_t* committed);
+int64_t   pg_maslov_round_size(int64_t undirected_edges);
+
+/* Small-world ratios: gamma = Cp/<Cp_rand> (U/Cp/Cp/Cp_main.cpp:173-174),
+ * lambda = Lp/<Lp_rand> (W/Lp/CUBFW_Lp/CUBFW_Lp/CUBFW_Lp_main.cpp:213-227),
+ * sigma = gamma/lambda (W/SmallWorldProperty/SmallWorldProperty.cpp:188). */
+pg_status pg_smallworld(double cp, const double* cp_rand, int32_t n_cp, double lp,
+                        const double* lp_rand, int32_t n_lp, double* gamma, double* lambda,
+                        double* sigma);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,50 @@
+"""Network construction on the GPU against the FP64 oracle (bit-exact edge sets)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pagani import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_graph(bold, mode, value, sign="signed", weighted=False):
+    z, _ = O.zscore(bold)
+    r = O.corr_packed(z, weighted=weighted)
+    N = bold.shape[1]
+    abs_mode = sign == "abs"
+    if mode == "r":
+        R, C, V = O.graph_r(r, N, value, abs_mode=abs_mode, weighted=weighted)
+        return R, C, V, value
+    k = O.sparsity_k(N, value)
+    R, C, V, tau = O.graph_k(r, N, k, abs_mode=abs_mode, weighted=weighted)
+    return R, C, V, tau
+
+
+@pytest.mark.parametrize("precision", ["fp32"])
+@pytest.mark.parametrize("N,T,mode,value,sign", [
+    (700, 200, "r", 0.3, "signed"),
+    (1000, 150, "s", 1.0, "signed"),
+    (1000, 150, "s", 2.0, "abs"),
+    (513, 77, "r", 0.25, "abs"),
+    (129, 64, "s", 0.5, "signed"),
+])
+def test_edge_set_exact(ctx, precision, N, T, mode, value, sign):
+    bold = synth.bold_series(N, T, 10, 1000 + N + T)
+    g, info = ctx.build_graph(bold, mode=mode, value=value, sign=sign, precision=precision)
+    R, C, _ = g.to_csr()
+    Ro, Co, _, tau = _oracle_graph(bold, mode, value, sign)
+    assert np.array_equal(R, Ro)
+    assert np.array_equal(C, Co)
+    if mode == "s":
+        assert info["tau"] == tau
+        assert info["edges"] == O.sparsity_k(N, value)
+
+
+def test_degree_matches_reference_rule(ctx):
+    bold = synth.bold_series(400, 100, 5, 5)
+    g, _ = ctx.build_graph(bold, mode="r", value=0.35, precision="fp32")
+    R, C, _ = g.to_csr()
+    deg, iso = ctx.degree(g)
+    d_or, iso_or = O.degree(R)
+    assert np.array_equal(deg, d_or) and iso == iso_or
