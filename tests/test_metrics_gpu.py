@@ -1,0 +1,166 @@
+"""Graph metrics on the GPU against the oracle restatement."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "ring_chord": G.ring_chord(),
+    "path200": G.path(200),
+    "star50": G.star(50),
+    "islands": G.two_components_with_isolated(),
+    "complete30": G.complete(30),
+    "bold700": G.from_bold(700, 200, 0.3, 11),
+    "bold1500": G.bench_like(),
+}
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request, ctx):
+    R, C, _ = CASES[request.param]
+    return request.param, R, C, ctx.graph(R, C)
+
+
+def test_degree(ctx, case):
+    name, R, C, g = case
+    deg, iso = ctx.degree(g)
+    d_or, iso_or = O.degree(R)
+    assert np.array_equal(deg, d_or) and iso == iso_or
+
+
+def test_weighted_strength_bit_exact(ctx):
+    R, C, V = G.random_weighted(300, 0.05, 3)
+    g = ctx.graph(R, C, V)
+    deg, _ = ctx.degree(g)
+    d_or, _ = O.degree(R, V)
+    assert np.array_equal(deg, d_or)
+
+
+def test_triangles_and_cp(ctx, case):
+    name, R, C, g = case
+    cp, tri, mean = ctx.clustering(g)
+    tri_or, cp_or, mean_or = O.cp_binary(R, C)
+    assert np.array_equal(tri, tri_or)
+    assert np.array_equal(cp, cp_or)           # same FP64 rounding sequence
+    assert mean == pytest.approx(mean_or, rel=1e-12, abs=1e-15)
+
+
+def test_paths(ctx, case):
+    name, R, C, g = case
+    eff, inv, lp, hist, diam = ctx.paths(g, max_hop=256)
+    inv_or, hist_or, lp_or, dmax = O.bfs_paths(R, C, max_hop=256)
+    assert np.array_equal(hist, hist_or)
+    assert diam == dmax
+    np.testing.assert_allclose(inv, inv_or, rtol=1e-12, atol=0)
+    assert lp == pytest.approx(lp_or, rel=1e-12)
+    n = len(R) - 1
+    np.testing.assert_allclose(eff, (inv_or / max(n - 1, 1)).astype(np.float32), rtol=1e-6)
+
+
+def test_bfs_sigma_exact(ctx, case):
+    name, R, C, g = case
+    n = len(R) - 1
+    rng = np.random.default_rng(5)
+    src = rng.integers(0, n, size=min(n, 40)).astype(np.int32)
+    dist, sigma = ctx.bfs_sigma(g, src)
+    for q, s in enumerate(src):
+        d_or, s_or = O.bfs_source(R, C, int(s))
+        assert np.array_equal(dist[q], d_or)
+        assert np.array_equal(sigma[q], s_or)
+
+
+def test_betweenness(ctx, case):
+    name, R, C, g = case
+    bc, bc64, eff, lp = ctx.betweenness(g, with_paths=True)
+    bc_or = O.brandes(R, C)
+    np.testing.assert_allclose(bc64, bc_or, rtol=1e-10, atol=1e-9)
+    inv_or, _, lp_or, _ = O.bfs_paths(R, C)
+    assert lp == pytest.approx(lp_or, rel=1e-12)
+
+
+def test_newman(ctx, case):
+    name, R, C, g = case
+    labels, Q, nm = ctx.newman(g)
+    lab_or, Q_or, nm_or, _ = O.newman(R, C)
+    assert nm == nm_or
+    assert np.array_equal(labels, lab_or)
+    assert Q == pytest.approx(Q_or, rel=1e-9, abs=1e-12)
+
+
+def test_fw_unweighted_equals_hops(ctx):
+    R, C, _ = G.from_bold(300, 100, 0.35, 4)
+    g = ctx.graph(R, C)
+    eff, lp, D = ctx.fw_paths(g, want_dist=True)
+    n = len(R) - 1
+    for s in range(0, n, 37):
+        d_or, _ = O.bfs_source(R, C, s)
+        ref = np.where(d_or < 0, np.inf, d_or).astype(np.float32)
+        assert np.array_equal(D[s], ref)
+
+
+def test_fw_weighted(ctx):
+    R, C, V = G.random_weighted(150, 0.06, 9)
+    g = ctx.graph(R, C, V)
+    eff, lp, D = ctx.fw_paths(g, want_dist=True)
+    n = len(R) - 1
+    Dd = np.full((n, n), np.inf, np.float32)
+    for i in range(n):
+        Dd[i, C[R[i]:R[i + 1]]] = np.float32(1) / V[R[i]:R[i + 1]]
+    np.fill_diagonal(Dd, 0)
+    D_or = O.fw_dense(Dd)
+    fin = np.isfinite(D_or)
+    assert np.array_equal(fin, np.isfinite(D))
+    np.testing.assert_allclose(D[fin], D_or[fin], rtol=1e-6)
+    eff_or, lp_or = O.weighted_paths(R, C, V)
+    np.testing.assert_allclose(eff, eff_or, rtol=1e-5)
+    assert lp == pytest.approx(lp_or, rel=1e-6)
+
+
+def test_onnela(ctx):
+    R, C, V = G.from_bold(400, 300, 0.2, 21, weighted=True)
+    g = ctx.graph(R, C, V)
+    for first_n in (False, True):
+        cp, _, mean = ctx.clustering(g, kind="onnela", vmax_first_n=first_n)
+        cp_or, mean_or = O.onnela(R, C, V, vmax_first_n=first_n)
+        np.testing.assert_allclose(cp, cp_or, rtol=1e-5, atol=1e-7)
+        assert mean == pytest.approx(mean_or, rel=1e-5)
+
+
+def test_fw_batched_with_onnela(ctx):
+    gs, refs = [], []
+    for q, n in enumerate([90, 131, 64, 257]):
+        R, C, V = G.from_bold(n, 400, 0.2, 100 + q, weighted=True)
+        gs.append(ctx.graph(R, C, V))
+        refs.append((R, C, V))
+    out = ctx.fw_batched(gs)
+    for (eff, lp, cp, cpm), (R, C, V) in zip(out, refs):
+        eff_or, lp_or = O.weighted_paths(R, C, V)
+        np.testing.assert_allclose(eff, eff_or, rtol=1e-5)
+        assert lp == pytest.approx(lp_or, rel=1e-6)
+        cp_or, m_or = O.onnela(R, C, V)
+        np.testing.assert_allclose(cp, cp_or, rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_maslov_bit_exact(ctx, weighted):
+    if weighted:
+        R, C, V = G.from_bold(500, 300, 0.2, 31, weighted=True)
+    else:
+        R, C, V = G.from_bold(600, 200, 0.3, 32)
+    g = ctx.graph(R, C, V)
+    attempts = 10 * (len(C) // 2)
+    g2, committed = ctx.maslov(g, 12345, attempts)
+    R2, C2, V2 = g2.to_csr()
+    Ro, Co, Vo, comm_or = O.maslov(R, C, V, 12345, attempts)
+    assert committed == comm_or
+    assert np.array_equal(R2, Ro) and np.array_equal(C2, Co)
+    if weighted:
+        assert np.array_equal(V2, Vo)
+    assert np.array_equal(np.diff(R2), np.diff(R))   # degrees preserved
+    n = len(R) - 1
+    rows = np.repeat(np.arange(n), np.diff(R2))
+    assert not np.any(rows == C2)                    # no self loops
+    assert committed > attempts // 20
