@@ -150,6 +150,7 @@ pg_status pg_graph_alloc(pg_ctx* ctx, int32_t n, int64_t nnz, bool weighted, pg_
     pg_graph* g = new (std::nothrow) pg_graph;
     if (!g) return PG_ERR_NOMEM;
     g->ctx = ctx;
+    g->device = ctx->device;
     g->n = n;
     g->nnz = nnz;
     cudaError_t e = cudaMalloc(&g->R, sizeof(int32_t) * ((size_t)n + 1));
@@ -168,10 +169,9 @@ pg_status pg_graph_alloc(pg_ctx* ctx, int32_t n, int64_t nnz, bool weighted, pg_
 extern "C" pg_status pg_graph_free(pg_graph* g)
 {
     if (!g) return PG_OK;
-    if (g->ctx) {
-        cudaSetDevice(g->ctx->device);
-        cudaStreamSynchronize(g->ctx->stream);
-    }
+    // cudaFree waits for the device work that may still use the arrays; the
+    // graph does not touch its creating context, which may already be gone.
+    cudaSetDevice(g->device);
     cudaFree(g->R);
     cudaFree(g->C);
     cudaFree(g->V);

@@ -26,6 +26,7 @@ namespace cg = cooperative_groups;
 
 namespace {
 constexpr int THREADS = 256;
+constexpr int LCAP = 48;      // levels whose frontier masks are kept for the backward sweep
 
 struct BCArgs {
     const int32_t* R;
@@ -37,6 +38,7 @@ struct BCArgs {
     unsigned long long* sigma;  // [n][32]
     double* coef;             // [n][32]
     unsigned int* front;      // [2][n]
+    unsigned int* fhist;      // [LCAP][n] frontier mask of every level < LCAP
     unsigned int* seen;       // [n]
     int* flags;               // [3] rotating "something changed" flags
     double* bc;               // [n] accumulated FP64 betweenness (null: forward only)
@@ -62,7 +64,7 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
         const unsigned full = ns == 32 ? 0xffffffffu : ((1u << ns) - 1u);
         // ---- init: levels -1, frontier = sources
         for (size_t q = gt; q < (size_t)n * 32; q += gstride) a.dist[q] = -1;
-        for (size_t v = gt; v < (size_t)n; v += gstride) { a.front[v] = 0u; a.seen[v] = 0u; }
+        for (size_t v = gt; v < (size_t)n; v += gstride) { a.front[v] = 0u; a.seen[v] = 0u; a.fhist[v] = 0u; }
         if (gt < 3) a.flags[gt] = 0;
         grid.sync();
         if (gt < (size_t)ns) {
@@ -71,6 +73,7 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
             a.sigma[(size_t)s * 32 + gt] = 1ULL;
             atomicOr(&a.front[s], 1u << gt);
             atomicOr(&a.seen[s], 1u << gt);
+            atomicOr(&a.fhist[s], 1u << gt);
         }
         grid.sync();
         // ---- forward
@@ -120,6 +123,7 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                 if (lane == 0) {
                     nxt[v] = nb;
                     a.seen[v] = sv | nb;
+                    if (d < LCAP) a.fhist[(size_t)d * n + v] = nb;
                 }
             }
             if (found && lane == 0) a.flags[d % 3] = 1;
@@ -140,20 +144,36 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
         if (a.do_backward) {
             for (int lv = maxd; lv >= 1; lv--) {
                 for (int v = gw; v < n; v += nw) {
-                    const int dv = a.dist[(size_t)v * 32 + lane];
-                    const bool mine = dv == lv;
-                    if (!__any_sync(0xffffffffu, mine)) continue;
+                    // sources for which v sits on level lv
+                    unsigned mine_m;
+                    if (lv < LCAP) mine_m = a.fhist[(size_t)lv * n + v];
+                    else mine_m = __ballot_sync(0xffffffffu, a.dist[(size_t)v * 32 + lane] == lv);
+                    if (!mine_m) continue;
+                    const bool mine = (mine_m >> lane) & 1u;
                     double acc = 0.0;
                     if (lv < maxd) {
                         const int32_t s = a.R[v], e = a.R[v + 1];
                         for (int32_t base = s; base < e; base += 32) {
                             int32_t f = base + lane;
-                            int w = f < e ? a.C[f] : -1;
-                            int cnt = min(32, e - base);
-                            for (int j = 0; j < cnt; j++) {
-                                int wj = __shfl_sync(0xffffffffu, w, j);
-                                int dw = a.dist[(size_t)wj * 32 + lane];
-                                if (mine && dw == lv + 1) acc += a.coef[(size_t)wj * 32 + lane];
+                            int w = f < e ? a.C[f] : 0;
+                            if (lv + 1 < LCAP) {
+                                // neighbours one level deeper for some of v's sources
+                                unsigned mw = f < e ? (a.fhist[(size_t)(lv + 1) * n + w] & mine_m) : 0u;
+                                unsigned bm = __ballot_sync(0xffffffffu, mw != 0u);
+                                while (bm) {
+                                    int j = __ffs(bm) - 1;
+                                    bm &= bm - 1;
+                                    int wj = __shfl_sync(0xffffffffu, w, j);
+                                    unsigned mj = __shfl_sync(0xffffffffu, mw, j);
+                                    if ((mj >> lane) & 1u) acc += a.coef[(size_t)wj * 32 + lane];
+                                }
+                            } else {
+                                int cnt = min(32, e - base);
+                                for (int j = 0; j < cnt; j++) {
+                                    int wj = __shfl_sync(0xffffffffu, w, j);
+                                    int dw = a.dist[(size_t)wj * 32 + lane];
+                                    if (mine && dw == lv + 1) acc += a.coef[(size_t)wj * 32 + lane];
+                                }
                             }
                         }
                     }
@@ -205,6 +225,7 @@ pg_status alloc_state(pg_ctx* ctx, int n, BCArgs& a)
     PG_TRY(pg_wst(ctx, "bc.sigma", (size_t)n * 32 + 32, &a.sigma));
     PG_TRY(pg_wst(ctx, "bc.coef", (size_t)n * 32 + 32, &a.coef));
     PG_TRY(pg_wst(ctx, "bc.front", (size_t)2 * n + 2, &a.front));
+    PG_TRY(pg_wst(ctx, "bc.fhist", (size_t)LCAP * n + 2, &a.fhist));
     PG_TRY(pg_wst(ctx, "bc.seen", (size_t)n + 1, &a.seen));
     PG_TRY(pg_wst(ctx, "bc.flags", 4, &a.flags));
     return PG_OK;

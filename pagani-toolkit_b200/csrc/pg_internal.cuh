@@ -28,7 +28,8 @@ struct pg_ctx {
 };
 
 struct pg_graph {
-    pg_ctx* ctx = nullptr;
+    pg_ctx* ctx = nullptr;  // creator; not used after pg_destroy
+    int device = 0;
     int32_t n = 0;
     int64_t nnz = 0;
     int32_t* R = nullptr;   // device

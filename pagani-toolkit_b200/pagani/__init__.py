@@ -124,7 +124,7 @@ class Graph:
     """Device-resident CSR graph owned by a Context."""
 
     def __init__(self, ctx, handle):
-        self.ctx, self.h = ctx, handle
+        self.ctx, self.h = ctx, handle   # the reference keeps the context alive
 
     @property
     def info(self):
