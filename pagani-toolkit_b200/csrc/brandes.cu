@@ -2,22 +2,25 @@
 // BC_GPU_node_pred.cu:6-155; Betweenness_CPU, U/BC/BC_CPU/BC_CPU/BC_CPU.cpp:6-82)
 // with exact 64-bit path counts and FP64 dependencies.
 //
-// 32 sources run together, one warp lane per source: per node the state is
-// a row of 32 entries (level int32, sigma uint64, coefficient double), so a
-// neighbour's state for all sources is one coalesced 128/256-byte read.
-// Source bits of the current frontier are a 32-bit mask per node.
-//   forward level d:  v finds the sources that reach it at d (OR of the
-//                     frontier masks of its neighbours), then sums
-//                     sigma[u][s] over neighbours u on level d-1 of source s;
+// 64 sources run together, two per warp lane (lane l owns sources l and
+// l+32): per node the state is a row of 64 entries (level int32, sigma
+// uint64, coefficient double), so a neighbour's state for all sources is two
+// coalesced 256-byte reads.  Source bits are 64-bit masks per node.
+//   forward level d:  node v sums sigma[u][s] over neighbours u that are in
+//                     the frontier of a source s not yet seen at v; the
+//                     non-zero sums are exactly the sources reaching v at d;
 //   backward level d: v on level d of source s sums
 //                     (1 + delta[w][s]) / sigma[w][s] over neighbours w on
-//                     level d+1 (kept as one coefficient per entry), so
+//                     level d+1 (stored as one coefficient per entry), so
 //                     delta[v][s] = sigma[v][s] * sum; BC[v] += sum_s delta.
+// Neighbours are visited 32 at a time; a ballot over the 32 frontier masks
+// keeps only those that matter for some source, and those are broadcast to
+// the warp one by one.  The frontier mask of every level (< LCAP) is kept so
+// the backward sweep filters neighbours the same way.
 // BC[v] is the sum over ORDERED (source, target) pairs like the reference.
-// The whole sweep over all source batches is one cooperative kernel; levels
-// are separated by grid-wide barriers, so no host round trip happens per
-// level.  The same forward pass yields the hop path length (sum of 1/d per
-// node), which pg_betweenness can return as well.
+// The whole sweep is a cooperative kernel; levels are separated by grid-wide
+// barriers (no host round trip per level).  The forward pass also yields the
+// hop path length (sum of 1/d per node), returned by pg_betweenness on request.
 #include "pg_internal.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
@@ -26,7 +29,9 @@ namespace cg = cooperative_groups;
 
 namespace {
 constexpr int THREADS = 256;
+constexpr int S = 64;         // sources per batch
 constexpr int LCAP = 48;      // levels whose frontier masks are kept for the backward sweep
+typedef unsigned long long u64;
 
 struct BCArgs {
     const int32_t* R;
@@ -34,20 +39,21 @@ struct BCArgs {
     int32_t n;
     const int32_t* sources;   // null: sources 0..n-1
     int32_t nsrc;
-    int32_t* dist;            // [n][32]
-    unsigned long long* sigma;  // [n][32]
-    double* coef;             // [n][32]
-    unsigned int* front;      // [2][n]
-    unsigned int* fhist;      // [LCAP][n] frontier mask of every level < LCAP
-    unsigned int* seen;       // [n]
+    int32_t* dist;            // [n][S]
+    u64* sigma;               // [n][S]
+    double* coef;             // [n][S]
+    u64* front;               // [2][n]
+    u64* fhist;               // [LCAP][n] frontier mask of every level < LCAP
+    u64* seen;                // [n]
     int* flags;               // [3] rotating "something changed" flags
     double* bc;               // [n] accumulated FP64 betweenness (null: forward only)
     double* inv;              // [n] sum of 1/d (null: skip)
     int do_backward;
-    // pg_bfs_sigma output of one batch (null otherwise)
-    int32_t* out_dist;
-    unsigned long long* out_sigma;
+    int32_t* out_dist;        // pg_bfs_sigma output of one batch (null otherwise)
+    u64* out_sigma;
 };
+
+__device__ __forceinline__ u64 shfl64(u64 x, int j) { return __shfl_sync(0xffffffffu, x, j); }
 
 __global__ void __launch_bounds__(THREADS)
 k_brandes(BCArgs a, int batch_first, int batch_last)
@@ -58,67 +64,69 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int n = a.n;
     const size_t gt = (size_t)blockIdx.x * blockDim.x + threadIdx.x, gstride = (size_t)gridDim.x * blockDim.x;
+    const u64 lo_bit = 1ULL << lane, hi_bit = 1ULL << (lane + 32);
     for (int b = batch_first; b < batch_last; b++) {
-        const int s0 = b * 32;
-        const int ns = min(32, a.nsrc - s0);
-        const unsigned full = ns == 32 ? 0xffffffffu : ((1u << ns) - 1u);
+        const int s0 = b * S;
+        const int ns = min(S, a.nsrc - s0);
+        const u64 full = ns == S ? ~0ULL : ((1ULL << ns) - 1ULL);
         // ---- init: levels -1, frontier = sources
-        for (size_t q = gt; q < (size_t)n * 32; q += gstride) a.dist[q] = -1;
-        for (size_t v = gt; v < (size_t)n; v += gstride) { a.front[v] = 0u; a.seen[v] = 0u; a.fhist[v] = 0u; }
+        for (size_t q = gt; q < (size_t)n * S; q += gstride) a.dist[q] = -1;
+        for (size_t v = gt; v < (size_t)n; v += gstride) { a.front[v] = 0ULL; a.seen[v] = 0ULL; a.fhist[v] = 0ULL; }
         if (gt < 3) a.flags[gt] = 0;
         grid.sync();
         if (gt < (size_t)ns) {
             int s = a.sources ? a.sources[s0 + gt] : s0 + (int)gt;
-            a.dist[(size_t)s * 32 + gt] = 0;
-            a.sigma[(size_t)s * 32 + gt] = 1ULL;
-            atomicOr(&a.front[s], 1u << gt);
-            atomicOr(&a.seen[s], 1u << gt);
-            atomicOr(&a.fhist[s], 1u << gt);
+            a.dist[(size_t)s * S + gt] = 0;
+            a.sigma[(size_t)s * S + gt] = 1ULL;
+            atomicOr(&a.front[s], 1ULL << gt);
+            atomicOr(&a.seen[s], 1ULL << gt);
+            atomicOr(&a.fhist[s], 1ULL << gt);
         }
         grid.sync();
         // ---- forward
         int d = 1;
-        unsigned int* cur = a.front;
-        unsigned int* nxt = a.front + n;
+        u64* cur = a.front;
+        u64* nxt = a.front + n;
         for (;; d++) {
             if (gt == 0) a.flags[(d + 1) % 3] = 0;
             int found = 0;
             for (int v = gw; v < n; v += nw) {
-                const unsigned sv = a.seen[v];
-                const unsigned need = full & ~sv;
-                unsigned nb = 0;
-                const int32_t s = a.R[v], e = a.R[v + 1];
+                const u64 sv = a.seen[v];
+                const u64 need = full & ~sv;
+                u64 nb = 0ULL;
                 if (need) {
-                    unsigned acc = 0;
-                    for (int32_t base = s; base < e; base += 32) {
-                        int32_t f = base + lane;
-                        if (f < e) acc |= cur[a.C[f]];
-                        acc = __reduce_or_sync(0xffffffffu, acc);
-                        if ((acc & need) == need) break;
-                    }
-                    nb = acc & need;
-                }
-                if (nb) {
-                    unsigned long long sg = 0;
+                    const int32_t s = a.R[v], e = a.R[v + 1];
+                    u64 sg0 = 0ULL, sg1 = 0ULL;
                     for (int32_t base = s; base < e; base += 32) {
                         int32_t f = base + lane;
                         int u = f < e ? a.C[f] : 0;
-                        unsigned fu = f < e ? (cur[u] & nb) : 0u;
-                        unsigned m = __ballot_sync(0xffffffffu, fu != 0u);
+                        u64 fu = f < e ? (cur[u] & need) : 0ULL;
+                        unsigned m = __ballot_sync(0xffffffffu, fu != 0ULL);
                         while (m) {
                             int j = __ffs(m) - 1;
                             m &= m - 1;
                             int uj = __shfl_sync(0xffffffffu, u, j);
-                            unsigned fj = __shfl_sync(0xffffffffu, fu, j);
-                            if ((fj >> lane) & 1u) sg += a.sigma[(size_t)uj * 32 + lane];
+                            u64 fj = shfl64(fu, j);
+                            const u64* row = a.sigma + (size_t)uj * S;
+                            if (fj & lo_bit) sg0 += row[lane];
+                            if (fj & hi_bit) sg1 += row[lane + 32];
                         }
                     }
-                    if ((nb >> lane) & 1u) {
-                        a.sigma[(size_t)v * 32 + lane] = sg;
-                        a.dist[(size_t)v * 32 + lane] = d;
+                    const unsigned b0 = __ballot_sync(0xffffffffu, sg0 != 0ULL);
+                    const unsigned b1 = __ballot_sync(0xffffffffu, sg1 != 0ULL);
+                    nb = (u64)b0 | ((u64)b1 << 32);
+                    if (sg0) {
+                        a.sigma[(size_t)v * S + lane] = sg0;
+                        a.dist[(size_t)v * S + lane] = d;
                     }
-                    if (lane == 0 && a.inv) a.inv[v] += (double)__popc(nb) / (double)d;
-                    found = 1;
+                    if (sg1) {
+                        a.sigma[(size_t)v * S + lane + 32] = sg1;
+                        a.dist[(size_t)v * S + lane + 32] = d;
+                    }
+                    if (nb) {
+                        if (lane == 0 && a.inv) a.inv[v] += (double)__popcll(nb) / (double)d;
+                        found = 1;
+                    }
                 }
                 if (lane == 0) {
                     nxt[v] = nb;
@@ -129,15 +137,15 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
             if (found && lane == 0) a.flags[d % 3] = 1;
             grid.sync();
             const int any = a.flags[d % 3];
-            unsigned int* t = cur; cur = nxt; nxt = t;
+            u64* t = cur; cur = nxt; nxt = t;
             if (!any) break;
         }
         const int maxd = d - 1;  // deepest level reached
         if (a.out_dist) {
             for (size_t q = gt; q < (size_t)ns * n; q += gstride) {
                 size_t sidx = q / n, v = q % n;
-                a.out_dist[q] = a.dist[v * 32 + sidx];
-                a.out_sigma[q] = a.dist[v * 32 + sidx] >= 0 ? a.sigma[v * 32 + sidx] : 0ULL;
+                a.out_dist[q] = a.dist[v * S + sidx];
+                a.out_sigma[q] = a.dist[v * S + sidx] >= 0 ? a.sigma[v * S + sidx] : 0ULL;
             }
         }
         // ---- backward
@@ -145,12 +153,16 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
             for (int lv = maxd; lv >= 1; lv--) {
                 for (int v = gw; v < n; v += nw) {
                     // sources for which v sits on level lv
-                    unsigned mine_m;
-                    if (lv < LCAP) mine_m = a.fhist[(size_t)lv * n + v];
-                    else mine_m = __ballot_sync(0xffffffffu, a.dist[(size_t)v * 32 + lane] == lv);
+                    u64 mine_m;
+                    if (lv < LCAP) {
+                        mine_m = a.fhist[(size_t)lv * n + v];
+                    } else {
+                        unsigned x0 = __ballot_sync(0xffffffffu, a.dist[(size_t)v * S + lane] == lv);
+                        unsigned x1 = __ballot_sync(0xffffffffu, a.dist[(size_t)v * S + lane + 32] == lv);
+                        mine_m = (u64)x0 | ((u64)x1 << 32);
+                    }
                     if (!mine_m) continue;
-                    const bool mine = (mine_m >> lane) & 1u;
-                    double acc = 0.0;
+                    double acc0 = 0.0, acc1 = 0.0;
                     if (lv < maxd) {
                         const int32_t s = a.R[v], e = a.R[v + 1];
                         for (int32_t base = s; base < e; base += 32) {
@@ -158,34 +170,44 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                             int w = f < e ? a.C[f] : 0;
                             if (lv + 1 < LCAP) {
                                 // neighbours one level deeper for some of v's sources
-                                unsigned mw = f < e ? (a.fhist[(size_t)(lv + 1) * n + w] & mine_m) : 0u;
-                                unsigned bm = __ballot_sync(0xffffffffu, mw != 0u);
+                                u64 mw = f < e ? (a.fhist[(size_t)(lv + 1) * n + w] & mine_m) : 0ULL;
+                                unsigned bm = __ballot_sync(0xffffffffu, mw != 0ULL);
                                 while (bm) {
                                     int j = __ffs(bm) - 1;
                                     bm &= bm - 1;
                                     int wj = __shfl_sync(0xffffffffu, w, j);
-                                    unsigned mj = __shfl_sync(0xffffffffu, mw, j);
-                                    if ((mj >> lane) & 1u) acc += a.coef[(size_t)wj * 32 + lane];
+                                    u64 mj = shfl64(mw, j);
+                                    const double* row = a.coef + (size_t)wj * S;
+                                    if (mj & lo_bit) acc0 += row[lane];
+                                    if (mj & hi_bit) acc1 += row[lane + 32];
                                 }
                             } else {
                                 int cnt = min(32, e - base);
                                 for (int j = 0; j < cnt; j++) {
                                     int wj = __shfl_sync(0xffffffffu, w, j);
-                                    int dw = a.dist[(size_t)wj * 32 + lane];
-                                    if (mine && dw == lv + 1) acc += a.coef[(size_t)wj * 32 + lane];
+                                    const int32_t* dw = a.dist + (size_t)wj * S;
+                                    const double* row = a.coef + (size_t)wj * S;
+                                    if ((mine_m & lo_bit) && dw[lane] == lv + 1) acc0 += row[lane];
+                                    if ((mine_m & hi_bit) && dw[lane + 32] == lv + 1) acc1 += row[lane + 32];
                                 }
                             }
                         }
                     }
                     double delta = 0.0;
-                    if (mine) {
-                        double sg = __ull2double_rn(a.sigma[(size_t)v * 32 + lane]);
-                        delta = sg * acc;
-                        a.coef[(size_t)v * 32 + lane] = (1.0 + delta) / sg;
+                    if (mine_m & lo_bit) {
+                        double sg = __ull2double_rn(a.sigma[(size_t)v * S + lane]);
+                        double dl = sg * acc0;
+                        a.coef[(size_t)v * S + lane] = (1.0 + dl) / sg;
+                        delta += dl;
                     }
-                    double tot = delta;
-                    for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-                    if (lane == 0 && a.bc) a.bc[v] += tot;
+                    if (mine_m & hi_bit) {
+                        double sg = __ull2double_rn(a.sigma[(size_t)v * S + lane + 32]);
+                        double dl = sg * acc1;
+                        a.coef[(size_t)v * S + lane + 32] = (1.0 + dl) / sg;
+                        delta += dl;
+                    }
+                    for (int o = 16; o; o >>= 1) delta += __shfl_xor_sync(0xffffffffu, delta, o);
+                    if (lane == 0 && a.bc) a.bc[v] += delta;
                 }
                 grid.sync();
             }
@@ -221,9 +243,9 @@ __global__ void k_sum_inv(const double* __restrict__ x, int32_t n, double* __res
 
 pg_status alloc_state(pg_ctx* ctx, int n, BCArgs& a)
 {
-    PG_TRY(pg_wst(ctx, "bc.dist", (size_t)n * 32 + 32, &a.dist));
-    PG_TRY(pg_wst(ctx, "bc.sigma", (size_t)n * 32 + 32, &a.sigma));
-    PG_TRY(pg_wst(ctx, "bc.coef", (size_t)n * 32 + 32, &a.coef));
+    PG_TRY(pg_wst(ctx, "bc.dist", (size_t)n * S + S, &a.dist));
+    PG_TRY(pg_wst(ctx, "bc.sigma", (size_t)n * S + S, &a.sigma));
+    PG_TRY(pg_wst(ctx, "bc.coef", (size_t)n * S + S, &a.coef));
     PG_TRY(pg_wst(ctx, "bc.front", (size_t)2 * n + 2, &a.front));
     PG_TRY(pg_wst(ctx, "bc.fhist", (size_t)LCAP * n + 2, &a.fhist));
     PG_TRY(pg_wst(ctx, "bc.seen", (size_t)n + 1, &a.seen));
@@ -262,9 +284,9 @@ extern "C" pg_status pg_betweenness(pg_ctx* ctx, const pg_graph* g, float* bc, d
         PG_TRY(pg_wst(ctx, "bc.inv", (size_t)n + 1, &a.inv));
         PG_CUDA(ctx, cudaMemsetAsync(a.inv, 0, sizeof(double) * (n + 1), ctx->stream));
     }
-    const int nb = (n + 31) / 32;
-    // a few batches per launch keeps every launch short
-    const int per_launch = 64;
+    const int nb = (n + S - 1) / S;
+    // a bounded number of batches per launch keeps every launch short
+    const int per_launch = 32;
     for (int b = 0; b < nb; b += per_launch) PG_TRY(launch_brandes(ctx, a, b, std::min(nb, b + per_launch)));
     float *dbc, *deff = nullptr;
     PG_TRY(pg_wst(ctx, "bc.bcf", (size_t)n + 1, &dbc));
@@ -305,13 +327,13 @@ extern "C" pg_status pg_bfs_sigma(pg_ctx* ctx, const pg_graph* g, const int32_t*
     PG_TRY(pg_wst(ctx, "bc.src", (size_t)ns + 1, &dsrc));
     PG_CUDA(ctx, cudaMemcpyAsync(dsrc, sources, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream));
     a.sources = dsrc;
-    PG_TRY(pg_wst(ctx, "bc.odist", (size_t)32 * n, &a.out_dist));
-    PG_TRY(pg_wst(ctx, "bc.osigma", (size_t)32 * n, &a.out_sigma));
-    for (int b = 0; b < (ns + 31) / 32; b++) {
+    PG_TRY(pg_wst(ctx, "bc.odist", (size_t)S * n, &a.out_dist));
+    PG_TRY(pg_wst(ctx, "bc.osigma", (size_t)S * n, &a.out_sigma));
+    for (int b = 0; b < (ns + S - 1) / S; b++) {
         PG_TRY(launch_brandes(ctx, a, b, b + 1));
-        int cnt = std::min(32, ns - b * 32);
-        PG_TRY(pg_d2h(ctx, dist + (size_t)b * 32 * n, a.out_dist, sizeof(int32_t) * (size_t)cnt * n));
-        PG_TRY(pg_d2h(ctx, sigma + (size_t)b * 32 * n, a.out_sigma, sizeof(int64_t) * (size_t)cnt * n));
+        int cnt = std::min(S, ns - b * S);
+        PG_TRY(pg_d2h(ctx, dist + (size_t)b * S * n, a.out_dist, sizeof(int32_t) * (size_t)cnt * n));
+        PG_TRY(pg_d2h(ctx, sigma + (size_t)b * S * n, a.out_sigma, sizeof(int64_t) * (size_t)cnt * n));
     }
     return PG_OK;
 }
