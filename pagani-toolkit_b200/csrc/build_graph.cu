@@ -308,34 +308,48 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
     inf.zero_variance = nzero;
     PG_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
 
-    // ---- histogram pass
+    // ---- histogram pass(es): only keys >= kmin are binned, the rest counted
     EpiParams p;
     memset(&p, 0, sizeof p);
     p.N = N;
     p.abs_mode = o.sign == PG_ABS;
     p.weighted = o.weighted != 0;
-    p.kmin = p.abs_mode ? 0.0f : -1.0f;
-    p.scale = (float)HIST_BINS / (p.abs_mode ? 1.0f : 2.0f);
+    p.tile_stride = 1;
+    const double g = o.guard;
+    const float key_lo = p.abs_mode ? 0.0f : -1.0f;
+    const float edge_band = (float)(1.0 - g);
+    p.edge_band = (g == 0.0 && o.mode == PG_THRESH_R) ? INFINITY : edge_band;
     unsigned int* hist;
+    unsigned long long* below;
     PG_TRY(pg_wst(ctx, "b.hist", HIST_BINS, &hist));
-    PG_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(unsigned int) * HIST_BINS, ctx->stream));
+    PG_TRY(pg_wst(ctx, "b.below", 4, &below));
     p.hist = hist;
-    if (M1 > 0) PG_TRY(run_gram(ctx, z, o.precision, EPI_HIST, p));
+    p.below = below;
     std::vector<unsigned int> h(HIST_BINS);
-    PG_TRY(pg_d2h(ctx, h.data(), hist, sizeof(unsigned int) * HIST_BINS));
-    PG_CUDA(ctx, cudaEventRecord(ev[2], ctx->stream));
-    long long hsum = 0;
-    for (int b = 0; b < HIST_BINS; b++) hsum += h[b];
-    if (hsum != M1) return pg_fail(ctx, PG_ERR_INTERNAL, "histogram holds %lld pairs, expected %lld", hsum, M1);
-
-    // bin edges as floats exactly as the kernel maps keys (monotone)
+    unsigned long long hbelow[2] = {0, 0};
+    auto hist_pass = [&](float kmin, int stride) -> pg_status {
+        p.kmin = kmin;
+        p.scale = (float)HIST_BINS / (1.0f - kmin);
+        p.tile_stride = stride;
+        PG_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(unsigned int) * HIST_BINS, ctx->stream));
+        PG_CUDA(ctx, cudaMemsetAsync(below, 0, 2 * sizeof(unsigned long long), ctx->stream));
+        if (M1 > 0) PG_TRY(run_gram(ctx, z, o.precision, EPI_HIST, p));
+        PG_TRY(pg_d2h(ctx, h.data(), hist, sizeof(unsigned int) * HIST_BINS));
+        PG_TRY(pg_d2h(ctx, hbelow, below, 2 * sizeof(unsigned long long)));
+        p.tile_stride = 1;
+        return PG_OK;
+    };
     auto bin_of = [&](float key) {
         float x = (key - p.kmin) * p.scale;
         int b = (int)x;
         if (!(x >= 0.0f)) b = 0;
         return std::min(b, HIST_BINS - 1);
     };
-    const double g = o.guard;
+    auto hist_total = [&]() {
+        long long s = 0;
+        for (int b = 0; b < HIST_BINS; b++) s += h[b];
+        return s;
+    };
     long long k_edges = -1;  // sparsity: wanted edges
     float lo_cut, hi_cut;
     if (o.mode == PG_THRESH_SPARSITY) {
@@ -343,38 +357,62 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
             return pg_fail(ctx, PG_ERR_INVALID, "sparsity %g%% out of range", o.value);
         k_edges = pg_sparsity_edges(N, (float)o.value);
         if (k_edges > M1) k_edges = M1;
+        // floor for the binned range: from a sampled pass over every 8th tile
+        // when the problem is large, with room for twice the wanted edges
+        float floor_key = key_lo;
+        const long long ntiles = (long long)(z.Np / 128) * (z.Np / 128 + 1) / 2;
+        if (k_edges > 0 && ntiles >= 64LL * ctx->sm_count) {
+            PG_TRY(hist_pass(key_lo, 8));
+            const long long ps = hist_total();
+            const double f = M1 > 0 ? (double)ps / (double)M1 : 1.0;
+            const double want = 2.0 * (double)k_edges * f + 1024.0;
+            long long acc = 0;
+            int bf = 0;
+            for (int b = HIST_BINS - 1; b >= 0; b--) {
+                acc += h[b];
+                if ((double)acc >= want) { bf = b; break; }
+            }
+            floor_key = (float)std::max((double)key_lo, p.kmin + (double)bf / p.scale - g - 4.0 / p.scale);
+        }
+        PG_TRY(hist_pass(floor_key, 1));
+        if (floor_key > key_lo && hist_total() < k_edges) PG_TRY(hist_pass(key_lo, 1));  // sample misled us
         if (k_edges <= 0) {
             lo_cut = hi_cut = INFINITY;
         } else {
-            // bin holding the k-th largest key
             long long acc = 0;
-            int bk = HIST_BINS - 1;
+            int bk = 0;
             for (int b = HIST_BINS - 1; b >= 0; b--) {
                 acc += h[b];
                 if (acc >= k_edges) { bk = b; break; }
             }
-            double lo_b = p.kmin + (double)bk / p.scale, hi_b = p.kmin + (double)(bk + 1) / p.scale;
+            const double lo_b = p.kmin + (double)bk / p.scale, hi_b = p.kmin + (double)(bk + 1) / p.scale;
             lo_cut = (float)(lo_b - g - 1.0 / p.scale);
             hi_cut = (float)(hi_b + g + 1.0 / p.scale);
         }
     } else {
         lo_cut = (float)(o.value - g);
         hi_cut = (float)(o.value + g);
-        if (g == 0.0) lo_cut = hi_cut = (float)o.value;  // no recheck: decided by the tile alone
+        if (g == 0.0) lo_cut = hi_cut = nextafterf((float)o.value, INFINITY);  // tile decides alone: key > value
+        PG_TRY(hist_pass(std::max(key_lo, std::min(lo_cut, edge_band) - 1e-3f), 1));
     }
-    if (lo_cut < p.kmin) lo_cut = p.kmin;
-    // capacities from the histogram (upper bounds, the mapping is monotone)
-    const float edge_band = (float)(1.0 - g);
+    PG_CUDA(ctx, cudaEventRecord(ev[2], ctx->stream));
+    if (hist_total() + (long long)hbelow[0] != M1)
+        return pg_fail(ctx, PG_ERR_INTERNAL, "histogram holds %lld pairs, expected %lld",
+                       hist_total() + (long long)hbelow[0], M1);
+    if (lo_cut < key_lo) lo_cut = key_lo;
+    // capacities from the histogram (upper bounds: the bin mapping is monotone)
     long long cap_pairs = 0, cap_band = 0;
     {
         int bh = std::isfinite(hi_cut) ? bin_of(hi_cut) : HIST_BINS;
         int bl = std::isfinite(lo_cut) ? bin_of(lo_cut) : HIST_BINS;
         int be = bin_of(edge_band);
-        int bneg = p.abs_mode ? HIST_BINS : bin_of(-edge_band);
         for (int b = 0; b < HIST_BINS; b++) {
             if (b >= bh) cap_pairs += h[b];
-            if (b >= bl || b >= be || b <= bneg) cap_band += h[b];
+            if (b >= bl || b >= be) cap_band += h[b];
         }
+        if (lo_cut < p.kmin) cap_band += (long long)hbelow[0];   // band reaches below the binned range
+        if (hi_cut < p.kmin) cap_pairs += (long long)hbelow[0];
+        cap_band += (long long)hbelow[1];                         // r <= -(1 - guard), signed keys
         if (g == 0.0 && o.mode == PG_THRESH_R) cap_band = 0;
     }
     if (cap_pairs > (long long)INT32_MAX) return pg_fail(ctx, PG_ERR_TOO_LARGE, "too many edges");
@@ -390,7 +428,6 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
     PG_CUDA(ctx, cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), ctx->stream));
     p.lo_cut = lo_cut;
     p.hi_cut = hi_cut;
-    p.edge_band = (g == 0.0 && o.mode == PG_THRESH_R) ? INFINITY : edge_band;
     p.pairs = pairs;
     p.pair_w = pw;
     p.n_pairs = counters;

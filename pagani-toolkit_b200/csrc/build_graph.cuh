@@ -27,9 +27,12 @@ struct EpiParams {
     int N;
     int abs_mode;
     int weighted;
-    // HIST: bin = clamp((key - kmin) * scale)
+    int tile_stride;               // HIST: visit every tile_stride-th tile only (sampling)
+    // HIST: keys below kmin are only counted; the rest go to
+    // bin = clamp((key - kmin) * scale)
     float kmin, scale;
     unsigned int* hist;            // HIST_BINS global counters
+    unsigned long long* below;     // [0] keys < kmin, [1] pairs with r <= -edge_band
     // EMIT: key >= hi_cut -> decided edge; key >= lo_cut -> FP64 band;
     // |r| >= edge_band -> band (range rule near +-1).
     float lo_cut, hi_cut, edge_band;
@@ -63,16 +66,74 @@ __device__ __forceinline__ int epi_class(float r, const EpiParams& p)
     return 0;
 }
 
-// Appends for one (i, j, r) candidate; all lanes of the warp must call it.
-__device__ __forceinline__ void epi_emit(int cls, int i, int j, float r, const EpiParams& p)
+// HIST for one valid pair: count below the floor in registers, bin the rest
+// in the shared-memory histogram.
+__device__ __forceinline__ void epi_hist(float r, const EpiParams& p, unsigned int* sh_hist,
+                                         unsigned int& below, unsigned int& neg)
 {
-    long long s = warp_append(p.n_pairs, cls == 1);
-    if (s >= 0 && s < p.cap_pairs) {
-        p.pairs[s] = make_int2(i, j);
-        if (p.weighted) p.pair_w[s] = epi_key(r, p.abs_mode);
+    float k = epi_key(r, p.abs_mode);
+    neg += (!p.abs_mode && r <= -p.edge_band);
+    if (k < p.kmin) below++;
+    else atomicAdd(&sh_hist[epi_bin(k, p)], 1u);
+}
+
+// Flush the per-thread HIST counters: one atomic per warp.
+__device__ __forceinline__ void epi_hist_flush(unsigned int below, unsigned int neg, const EpiParams& p)
+{
+    unsigned int b = __reduce_add_sync(0xffffffffu, below);
+    unsigned int n = __reduce_add_sync(0xffffffffu, neg);
+    if ((threadIdx.x & 31) == 0) {
+        if (b) atomicAdd(&p.below[0], (unsigned long long)b);
+        if (n) atomicAdd(&p.below[1], (unsigned long long)n);
     }
-    long long b = warp_append(p.n_band, cls == 2);
-    if (b >= 0 && b < p.cap_band) p.band[b] = make_int2(i, j);
+}
+
+// Reserve c slots per lane in a global list with one atomic per warp; returns
+// this lane's first slot.
+__device__ __forceinline__ long long warp_reserve(unsigned long long* counter, unsigned int c)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned int x = c;
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    unsigned int total = __shfl_sync(0xffffffffu, x, 31);
+    unsigned long long base = 0;
+    if (lane == 31 && total) base = atomicAdd(counter, (unsigned long long)total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    return (long long)(base + (x - c));
+}
+
+// EMIT for a run of up to 32 candidates per lane.  m1/m2 flag "decided edge"
+// / "band" per candidate slot; (i, j, r) of slot q come from `at(q, i, j, r)`.
+// The slot loop is unrolled so that `at` may index register arrays.
+template <class At>
+__device__ __forceinline__ void epi_emit_masks(unsigned int m1, unsigned int m2, const EpiParams& p, At at)
+{
+    if (!__any_sync(0xffffffffu, (m1 | m2) != 0u)) return;
+    long long s1 = warp_reserve(p.n_pairs, __popc(m1));
+    long long s2 = warp_reserve(p.n_band, __popc(m2));
+    if (!(m1 | m2)) return;
+#pragma unroll
+    for (int q = 0; q < 32; q++) {
+        const bool e1 = (m1 >> q) & 1u, e2 = (m2 >> q) & 1u;
+        if (e1 | e2) {
+            int i, j;
+            float r;
+            at(q, i, j, r);
+            if (e1) {
+                if (s1 < p.cap_pairs) {
+                    p.pairs[s1] = make_int2(i, j);
+                    if (p.weighted) p.pair_w[s1] = epi_key(r, p.abs_mode);
+                }
+                s1++;
+            } else {
+                if (s2 < p.cap_band) p.band[s2] = make_int2(i, j);
+                s2++;
+            }
+        }
+    }
 }
 
 // Upper-triangle tile enumeration: linear index L in [0, nb(nb+1)/2) ->

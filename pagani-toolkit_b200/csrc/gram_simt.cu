@@ -30,7 +30,9 @@ k_gram_simt(const float* __restrict__ Z, int Tp, int nb, EpiParams p)
     }
     const long long nt = (long long)nb * (nb + 1) / 2;
     const int nk = Tp / BK;
-    for (long long L = blockIdx.x; L < nt; L += gridDim.x) {
+    unsigned int below = 0u, neg = 0u;
+    const long long stride = MODE == EPI_HIST ? (long long)p.tile_stride : 1LL;
+    for (long long L = blockIdx.x * stride; L < nt; L += (long long)gridDim.x * stride) {
         int bi, bj;
         tri_tile(L, nb, bi, bj);
         const float* Ag = Z + (size_t)bi * BM * Tp;
@@ -93,30 +95,32 @@ k_gram_simt(const float* __restrict__ Z, int Tp, int nb, EpiParams p)
 #pragma unroll
                 for (int y = 0; y < 8; y++) {
                     int i = i0 + x, j = j0 + y;
-                    if (i < j && j < p.N) atomicAdd(&sh_hist[epi_bin(epi_key(acc[x][y], p.abs_mode), p)], 1u);
+                    if (i < j && j < p.N) epi_hist(acc[x][y], p, sh_hist, below, neg);
                 }
         } else {
-            bool any = false;
 #pragma unroll
-            for (int x = 0; x < 8; x++)
+            for (int h = 0; h < 2; h++) {
+                unsigned int m1 = 0u, m2 = 0u;
 #pragma unroll
-                for (int y = 0; y < 8; y++) {
-                    int i = i0 + x, j = j0 + y;
-                    any |= (i < j && j < p.N && epi_class(acc[x][y], p) != 0);
-                }
-            if (__any_sync(0xffffffffu, any)) {
-#pragma unroll
-                for (int x = 0; x < 8; x++)
+                for (int x = 0; x < 4; x++)
 #pragma unroll
                     for (int y = 0; y < 8; y++) {
-                        int i = i0 + x, j = j0 + y;
-                        int cls = (i < j && j < p.N) ? epi_class(acc[x][y], p) : 0;
-                        epi_emit(cls, i, j, acc[x][y], p);
+                        int i = i0 + 4 * h + x, j = j0 + y;
+                        int cls = (i < j && j < p.N) ? epi_class(acc[4 * h + x][y], p) : 0;
+                        m1 |= (unsigned)(cls == 1) << (x * 8 + y);
+                        m2 |= (unsigned)(cls == 2) << (x * 8 + y);
                     }
+                epi_emit_masks(m1, m2, p, [&](int q, int& i, int& j, float& r) {
+                    int x = q >> 3, y = q & 7;
+                    i = i0 + 4 * h + x;
+                    j = j0 + y;
+                    r = acc[4 * h + x][y];
+                });
             }
         }
     }
     if (MODE == EPI_HIST) {
+        epi_hist_flush(below, neg, p);
         __syncthreads();
         for (int b = t; b < HIST_BINS; b += THREADS)
             if (sh_hist[b]) atomicAdd(&p.hist[b], sh_hist[b]);

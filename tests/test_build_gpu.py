@@ -21,7 +21,7 @@ def _oracle_graph(bold, mode, value, sign="signed", weighted=False):
     return R, C, V, tau
 
 
-@pytest.mark.parametrize("precision", ["fp32"])
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
 @pytest.mark.parametrize("N,T,mode,value,sign", [
     (700, 200, "r", 0.3, "signed"),
     (1000, 150, "s", 1.0, "signed"),
