@@ -44,6 +44,13 @@ WORKLOAD = "subject-58k: N=58000 voxels, T=240, 20 latent signals, top 1% |r| ->
 
 
 # --------------------------------------------------------------- helpers
+def set_voxels(n):
+    global N_VOX, WORKLOAD
+    if n != N_VOX:
+        WORKLOAD = WORKLOAD.replace(f"N={N_VOX}", f"N={n}").replace("subject-58k", f"subject-{n}")
+        N_VOX = n
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -103,6 +110,21 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def reduce_max_ms(t_ms, device):
+    """Step time of a multi-rank run: the maximum over ranks (replicas)."""
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([t_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def rank_subject_seed(rank):
+    """Every replica processes its own subject stream."""
+    from pagani import synth
+    return synth.subject_seed(2, rank)
 
 
 # ----------------------------------------------------- reference CPU arm
@@ -209,7 +231,10 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-leg", action="store_true")
+    ap.add_argument("--voxels", type=int, default=N_VOX,
+                    help="profiling aid: a smaller subject for ncu captures (the metric is quoted at 58000)")
     args = ap.parse_args()
+    set_voxels(args.voxels)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -229,7 +254,7 @@ def main():
     ctx = pagani.Context(local)
     stream = torch.cuda.ExternalStream(pagani.lib().pg_stream(ctx.h))
 
-    bold = synth.bold_series(N_VOX, T_LEN, N_SIG, synth.subject_seed(2, rank))
+    bold = synth.bold_series(N_VOX, T_LEN, N_SIG, rank_subject_seed(rank))
     bold_dev = torch.from_numpy(bold).to(f"cuda:{local}")
     bold_pin = torch.from_numpy(bold).pin_memory()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -273,9 +298,7 @@ def main():
             torch.cuda.synchronize()
             t = e0.elapsed_time(e1)
             if world > 1:
-                tt = torch.tensor([t], device=f"cuda:{local}")
-                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-                t = float(tt.item())
+                t = reduce_max_ms(t, f"cuda:{local}")
             ms.append(t)
         return float(np.mean(ms)), ms
 

@@ -1,0 +1,133 @@
+"""The reference-compatible CLI tools end to end on the GPU: NIfTI in,
+.csr/.nm/.modu/.txt out with the reference's names, contents checked against
+the oracle."""
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pagani import synth
+from tests.nifti import volume_from_series, write_nifti
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "pagani-toolkit_b200", "bin")
+
+
+def run(*args, cwd=None):
+    p = subprocess.run([os.path.join(BIN, args[0]), *map(str, args[1:])], capture_output=True, text=True,
+                       timeout=600, cwd=cwd)
+    assert p.returncode == 0, p.stdout + p.stderr
+    return p.stdout
+
+
+def read_csr(path):
+    raw = np.fromfile(path, np.int32)
+    rl = raw[0]
+    R = raw[1:1 + rl]
+    cl = raw[1 + rl]
+    C = raw[2 + rl:2 + rl + cl]
+    V = raw[3 + rl + cl:].view(np.float32) if len(raw) > 2 + rl + cl else None
+    return R, C, V
+
+
+def read_nm(path):
+    raw = np.fromfile(path, np.int32)
+    return raw[1:].view(np.float32)
+
+
+@pytest.fixture(scope="module")
+def subject_dir(tmp_path_factory):
+    d = tmp_path_factory.mktemp("bold")
+    N, T, shape = 600, 150, (10, 10, 7)
+    mask = np.zeros(shape, np.uint8)
+    flat = np.zeros(np.prod(shape), np.uint8)
+    flat[:N] = 1
+    mask[:] = flat.reshape(shape[2], shape[1], shape[0]).transpose(2, 1, 0)
+    write_nifti(d / "mask.nii", mask, 2)
+    bold = synth.bold_series(N, T, 10, 777)
+    write_nifti(d / "subj01.nii", volume_from_series(bold, shape), 16)
+    return d, bold
+
+
+def test_cucormat_r_and_s(subject_dir):
+    d, bold = subject_dir
+    run("CUCorMat", d, 0.5, "n", "y", "r", 0.3)
+    run("CUCorMat", d, 0.5, "n", "n", "s", 2)
+    N = bold.shape[1]
+    z, _ = O.zscore(bold)
+    r = O.corr_packed(z)
+    Ro, Co, _ = O.graph_r(r, N, np.float32(0.3))
+    s_r = 100.0 * len(Co) / (N * (N - 1) // 2) / 2
+    f_r = d / f"subj01_{N}_spa{np.float32(s_r):.3f}%_cor0.300.csr"
+    R, C, V = read_csr(f_r)
+    assert np.array_equal(R, Ro) and np.array_equal(C, Co) and V is None
+    cm = np.fromfile(d / f"subj01_{N}.cormat", np.float32)[1:]
+    assert np.max(np.abs(cm - r)) < 1e-6
+    k = O.sparsity_k(N, 2.0)
+    Rk, Ck, _, tau = O.graph_k(r, N, k)
+    f_s = glob.glob(str(d / f"subj01_{N}_spa2.000%_cor*.csr"))
+    assert len(f_s) == 1
+    R, C, _ = read_csr(f_s[0])
+    assert np.array_equal(R, Rk) and np.array_equal(C, Ck)
+
+
+def test_metric_tools(subject_dir, tmp_path):
+    d, bold = subject_dir
+    N = bold.shape[1]
+    z, _ = O.zscore(bold)
+    R, C, _ = O.graph_r(O.corr_packed(z), N, 0.3)
+    g = tmp_path / "g"
+    g.mkdir()
+    raw = np.concatenate([[len(R)], R, [len(C)], C]).astype(np.int32)
+    raw.tofile(g / "net.csr")
+    run("Degree", g)
+    assert np.array_equal(read_nm(g / "net_deg.nm"), O.degree(R)[0])
+    run("Cp", g, 2, "gnk")
+    assert np.array_equal(read_nm(g / "net_cp.nm"), O.cp_binary(R, C)[1])
+    assert len(open(g / "net_cp.txt").read().split()) == 3 and (g / "net_gamma.txt").exists()
+    run("BFS_MulCPU", g, 1, "b")
+    inv, _, lp, _ = O.bfs_paths(R, C)
+    np.testing.assert_allclose(read_nm(g / "net_eff.nm"), inv / (N - 1), rtol=1e-6)
+    assert float(open(g / "net_Lp.txt").read().split()[0]) == pytest.approx(lp, rel=1e-5)
+    run("CUBC", g)
+    np.testing.assert_allclose(read_nm(g / "net_bc.nm"), O.brandes(R, C), rtol=1e-6, atol=1e-3)
+    run("Newman_Modularity", g, 0)
+    lab = np.fromfile(g / "net.modu", np.int32)[1:]
+    assert np.array_equal(lab, O.newman(R, C)[0])
+    assert "Round:" in open(g / "net_modu.txt").read()
+    run("Maslov", g / "net.csr")
+    R2, C2, _ = read_csr(g / "net_Maslov.csr")
+    assert np.array_equal(np.diff(R2), np.diff(R))
+
+
+def test_weighted_tools_and_smallworld(subject_dir, tmp_path):
+    d, bold = subject_dir
+    w = tmp_path / "w"
+    w.mkdir()
+    for f in ("mask.nii", "subj01.nii"):
+        os.symlink(d / f, w / f)
+    run("CUCorMat_weighted", w, 0.5, "n", "n", "r", 0.25)
+    files = glob.glob(str(w / "*_weighted.csr"))
+    assert len(files) == 1
+    R, C, V = read_csr(files[0])
+    N = bold.shape[1]
+    z, _ = O.zscore(bold)
+    r = O.corr_packed(z, weighted=True)
+    Ro, Co, Vo = O.graph_r(r, N, O.weighted_r_threshold(np.float32(0.25)), weighted=True)
+    assert np.array_equal(R, Ro) and np.array_equal(C, Co)
+    assert np.array_equal(V, Vo)                   # V = float(FP64 r) for every edge
+    gdir = tmp_path / "wg"
+    gdir.mkdir()
+    os.symlink(files[0], gdir / os.path.basename(files[0]))
+    run("CUBFW_Lp", gdir, 2, "gnl")
+    run("Cp", gdir, 2, "2", "gnk")
+    run("SmallWorldProperty", gdir)
+    sw = glob.glob(str(gdir / "*_smallWorld.txt"))
+    assert len(sw) == 1
+    lam = float(open(glob.glob(str(gdir / "*_lambda.txt"))[0]).read())
+    gam = float(open(glob.glob(str(gdir / "*_gamma.txt"))[0]).read())
+    assert float(open(sw[0]).read()) == pytest.approx(gam / lam, rel=1e-5)

@@ -1,0 +1,55 @@
+"""The oracle restatement against the reference's own CPU functions run live
+(oracle/_ref, built from the reference sources where they are present) on
+fresh seeded inputs.  CPU only; skipped when the reference build is absent."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pagani import synth
+from tests import graphs as G
+
+pytestmark = pytest.mark.skipif(not O.Ref.available(), reason="oracle/_ref not built")
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return O.Ref()
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_graph_and_metrics(ref, seed):
+    N, T = 240, 80
+    bold = synth.bold_series(N, T, 6, 900 + seed)
+    z, _ = O.zscore(bold)
+    r = O.corr_packed(z)
+    cm = ref.cormat_cpu(bold)
+    assert np.max(np.abs(r - cm)) < 1e-6
+    R, C, _ = O.graph_r(r, N, 0.25)
+    Rr, Cr = ref.graph_r(cm, N, np.float32(0.25))
+    near = np.abs(r - 0.25) < 1e-6
+    if not near.any():
+        assert np.array_equal(R, Rr) and np.array_equal(C, Cr)
+    tri, cp, mean = O.cp_binary(R, C)
+    cpr, meanr = ref.cp(R, C)
+    assert np.array_equal(cp, cpr)
+    np.testing.assert_allclose(O.brandes(R, C), ref.betweenness(R, C), rtol=1e-4, atol=1e-3)
+    assert np.array_equal(O.newman(R, C)[0], ref.partition(R, C))
+
+
+@pytest.mark.parametrize("mk", [G.ring_chord, lambda: G.path(40), lambda: G.star(30), G.two_components_with_isolated])
+def test_small_graphs(ref, mk):
+    R, C, _ = mk()
+    np.testing.assert_allclose(O.brandes(R, C), ref.betweenness(R, C), rtol=1e-5, atol=1e-5)
+    _, cp, _ = O.cp_binary(R, C)
+    assert np.array_equal(cp, ref.cp(R, C)[0])
+    inv, _, lp, _ = O.bfs_paths(R, C)
+    li, lpr = ref.apsp_bfs(R, C)
+    np.testing.assert_allclose(inv / (len(R) - 2), li, rtol=1e-6, atol=1e-7)
+
+
+def test_ring_chord_betweenness_is_twice_the_undirected_value(ref):
+    # an 8-ring with one chord: the reference counts ordered source/target pairs
+    R, C, _ = G.ring_chord(8)
+    bc = ref.betweenness(R, C)
+    assert np.allclose(bc, [15, 5, 2, 5, 15, 5, 2, 5])
+    assert np.allclose(O.brandes(R, C), bc)
