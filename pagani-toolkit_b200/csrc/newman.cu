@@ -23,6 +23,7 @@
 #include "pg_internal.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <string>
 
@@ -500,7 +501,17 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     int Round = 0, Max_Result = 0, Module_Num = 1, Index = 1;
     char line[512];
     std::vector<int32_t> hAD(n), hgidx(n);
+    // wall time per kind of power-iteration launch, reported in the log
+    double t_small = 0, t_medium = 0, t_large = 0, t_setup = 0;
+    long long it_small = 0, it_medium = 0, it_large = 0;
+    int generations = 0;
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto ms_since = [&](std::chrono::steady_clock::time_point t0) {
+        return std::chrono::duration<double, std::milli>(now() - t0).count();
+    };
     while (Round <= Max_Result) {
+        generations++;
+        auto t_gen = now();
         // ---- pending groups of this generation: labels Round..Max_Result
         const int lo = Round, hi = Max_Result, G = hi - lo + 1;
         PG_TRY(pg_d2h(ctx, hl.data(), label, sizeof(int32_t) * n));
@@ -540,6 +551,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         PG_LAUNCHED(ctx);
         std::vector<long long> hsoff(P + 1);
         PG_TRY(pg_d2h(ctx, hsoff.data(), soff, sizeof(long long) * (P + 1)));
+        t_setup += ms_since(t_gen);
         // ---- power iterations
         std::vector<int> small, medium, large;
         for (int q = 0; q < G; q++) {
@@ -557,9 +569,12 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
             PG_CUDA(ctx, cudaMemcpyAsync(glist, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice,
                                          ctx->stream));
             if (!small.empty()) {
+                auto t0 = now();
                 k_nm_cluster<<<(int)small.size(), THREADS, 0, ctx->stream>>>(glist, goff, AD, sR, sC, kdeg, sumBG, v,
                                                                              v0, vv, M, gpu_rule_above, out);
                 PG_LAUNCHED(ctx);
+                PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+                t_small += ms_since(t0);
             }
             if (!medium.empty()) {
                 cudaLaunchConfig_t cfg = {};
@@ -574,13 +589,19 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                 cfg.attrs = attr;
                 cfg.numAttrs = 1;
                 const int* mlist = glist + small.size();
+                auto t0 = now();
                 PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_cluster, mlist, (const long long*)goff, (const int32_t*)AD,
                                                 (const int32_t*)sR, (const int32_t*)sC, (const double*)kdeg,
                                                 (const double*)sumBG, v, v0, vv, M, (int)gpu_rule_above, out));
                 PG_LAUNCHED(ctx);
+                PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+                t_medium += ms_since(t0);
             }
             PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * 8));
+            for (int q : small) it_small += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
+            for (int q : medium) it_medium += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
         }
+        auto t_l = now();
         for (int q : large) {
             const long long p0 = hgoff[q];
             LVArgs a;
@@ -610,7 +631,9 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
             o[5] = shifted ? r[1][3] : r[0][3];
             o[6] = shifted ? r[1][4] : r[0][4];
             o[7] = shifted;
+            it_large += (long long)(o[1] + o[3]);
         }
+        t_large += ms_since(t_l);
         // ---- decisions in round order (labels exactly as the sequential reference)
         std::vector<int> hbase(G, -1);
         std::vector<double> hcoef(G, 0.0);
@@ -670,6 +693,11 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     if (n_modules) *n_modules = Module_Num;
     if (log) {
         snprintf(line, sizeof line, "Number of Modules: %d,\tQ=%.6g", Module_Num, q);
+        log(line, user);
+        snprintf(line, sizeof line,
+                 "Timing (ms): generations %d, setup %.1f, one-CTA groups %.1f (%lld iterations), "
+                 "cluster groups %.1f (%lld), cooperative groups %.1f (%lld)",
+                 generations, t_setup, t_small, it_small, t_medium, it_medium, t_large, it_large);
         log(line, user);
     }
     return PG_OK;
