@@ -51,7 +51,28 @@ struct BCArgs {
     int do_backward;
     int32_t* out_dist;        // pg_bfs_sigma output of one batch (null otherwise)
     u64* out_sigma;
+    const int32_t* order;     // nodes by decreasing degree (largest work first)
+    int* work;                // [WORK_SLOTS] per-level work counters
 };
+
+constexpr int WORK_SLOTS = 4096;   // forward + backward levels per batch with dynamic scheduling
+
+// Next node for this warp: nodes are handed out in order of decreasing
+// degree through one atomic counter per level, so hubs start first and no
+// warp idles at the level barrier while another still holds a long list.
+// Levels beyond the counter array fall back to a static interleave.
+__device__ __forceinline__ int next_node(const BCArgs& a, int slot, int& k, int gw, int nw)
+{
+    if (slot >= WORK_SLOTS) {
+        int v = gw + k * nw;
+        k++;
+        return v < a.n ? v : a.n;
+    }
+    int idx = 0;
+    if ((threadIdx.x & 31) == 0) idx = atomicAdd(&a.work[slot], 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    return idx < a.n ? a.order[idx] : a.n;
+}
 
 __device__ __forceinline__ u64 shfl64(u64 x, int j) { return __shfl_sync(0xffffffffu, x, j); }
 
@@ -72,6 +93,7 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
         // ---- init: levels -1, frontier = sources
         for (size_t q = gt; q < (size_t)n * S; q += gstride) a.dist[q] = -1;
         for (size_t v = gt; v < (size_t)n; v += gstride) { a.front[v] = 0ULL; a.seen[v] = 0ULL; a.fhist[v] = 0ULL; }
+        for (size_t q = gt; q < (size_t)WORK_SLOTS; q += gstride) a.work[q] = 0;
         if (gt < 3) a.flags[gt] = 0;
         grid.sync();
         if (gt < (size_t)ns) {
@@ -90,7 +112,9 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
         for (;; d++) {
             if (gt == 0) a.flags[(d + 1) % 3] = 0;
             int found = 0;
-            for (int v = gw; v < n; v += nw) {
+            int kk = 0;
+            const int fslot = d < WORK_SLOTS / 2 ? d : WORK_SLOTS;
+            for (int v = next_node(a, fslot, kk, gw, nw); v < n; v = next_node(a, fslot, kk, gw, nw)) {
                 const u64 sv = a.seen[v];
                 const u64 need = full & ~sv;
                 u64 nb = 0ULL;
@@ -151,7 +175,10 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
         // ---- backward
         if (a.do_backward) {
             for (int lv = maxd; lv >= 1; lv--) {
-                for (int v = gw; v < n; v += nw) {
+                // backward levels use the upper half of the counters
+                const int bslot = lv < WORK_SLOTS / 2 ? WORK_SLOTS / 2 + lv : WORK_SLOTS;
+                int kk = 0;
+                for (int v = next_node(a, bslot, kk, gw, nw); v < n; v = next_node(a, bslot, kk, gw, nw)) {
                     // sources for which v sits on level lv
                     u64 mine_m;
                     if (lv < LCAP) {
@@ -250,6 +277,16 @@ pg_status alloc_state(pg_ctx* ctx, int n, BCArgs& a)
     PG_TRY(pg_wst(ctx, "bc.fhist", (size_t)LCAP * n + 2, &a.fhist));
     PG_TRY(pg_wst(ctx, "bc.seen", (size_t)n + 1, &a.seen));
     PG_TRY(pg_wst(ctx, "bc.flags", 4, &a.flags));
+    PG_TRY(pg_wst(ctx, "bc.work", (size_t)WORK_SLOTS, &a.work));
+    // nodes by decreasing degree (stable), for the dynamic level schedule
+    std::vector<int32_t> hR((size_t)n + 1), ord(n);
+    PG_TRY(pg_d2h(ctx, hR.data(), a.R, sizeof(int32_t) * (n + 1)));
+    for (int i = 0; i < n; i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return hR[x + 1] - hR[x] > hR[y + 1] - hR[y]; });
+    int32_t* dord;
+    PG_TRY(pg_wst(ctx, "bc.order", (size_t)n + 1, &dord));
+    PG_TRY(pg_h2d(ctx, dord, ord.data(), sizeof(int32_t) * n));
+    a.order = dord;
     return PG_OK;
 }
 
