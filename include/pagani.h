@@ -129,6 +129,24 @@ pg_status pg_degree(pg_ctx* ctx, const pg_graph* g, float* deg, int32_t* isolate
 pg_status pg_clustering(pg_ctx* ctx, const pg_graph* g, int32_t kind, int32_t flags,
                         float* cp, int64_t* triangles, double* mean);
 
+/* Allocation-free binary clustering (no counterpart in the reference).  For
+ * callers that cannot allocate device memory -- a host whose GPU memory is
+ * owned by another component (a framework's caching allocator, a plugin host
+ * that reserves the device at start-up) or a latency-critical pipeline that
+ * forbids cudaMalloc after initialisation because it can synchronise the
+ * device.  R/C (the CSR, n+1 and R[n] entries), cp (float[n]) and
+ * triangles (int64[n], may be NULL) are DEVICE pointers owned by the caller;
+ * work is issued on `stream` (a cudaStream_t, NULL = legacy default stream)
+ * and is not waited for.  Scratch is a 16 MiB static device array inside the
+ * library: n is limited to pg_clustering_noalloc_max_nodes() (larger n returns
+ * PG_ERR_TOO_LARGE), every GPU that loads the library holds the array until
+ * exit, and calls that overlap on the GPU race on it.  The first call on a
+ * device resolves the array's device address (with that device current);
+ * make that first call before any stream capture.  No cudaMalloc/cudaFree. */
+pg_status pg_clustering_noalloc(const int32_t* R, const int32_t* C, int32_t n, float* cp, int64_t* triangles,
+                                void* stream);
+int64_t   pg_clustering_noalloc_max_nodes(void);
+
 /* Hop path length and nodal efficiency: APSP_BFS (U/BFS_MulCPU/BFS_MulCPU/
  * APSP_BFS.cpp:27-147).  eff[i] = sum_j 1/d_ij / (n-1) (float, optional),
  * inv_sum[i] = sum_j 1/d_ij (double, optional), lp = n(n-1)/sum_ij 1/d_ij,

@@ -306,3 +306,59 @@ extern "C" pg_status pg_clustering(pg_ctx* ctx, const pg_graph* g, int32_t kind,
     if (mean) PG_TRY(pg_d2h(ctx, mean, dmean, sizeof(double)));
     return PG_OK;
 }
+
+// ------------------------------------------------ allocation-free variant
+// Binary clustering for callers that cannot allocate device memory: host
+// processes whose device memory is owned by someone else (a framework's
+// caching allocator or a plugin host that reserves the GPU up front), and
+// latency-critical pipelines that forbid cudaMalloc after start-up because
+// it can synchronise the device.  The per-node triangle counters live in
+// this file-scope device array instead of a workspace allocation.  Every
+// call shares it and it keeps the last call's contents, so it is cleared at
+// the start of each call, and calls that overlap on the GPU (other streams,
+// other host threads) race on it.
+namespace {
+constexpr int64_t NOALLOC_SCRATCH_WORDS = (16LL << 20) / 8;   // 16 MiB: n + 2 counters
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static unsigned long long* g_noalloc_ptr[NOALLOC_MAX_DEVICES];   // device address, per device
+
+__global__ void k_noalloc_clear(unsigned long long* __restrict__ w, int64_t count)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x)
+        w[q] = 0ULL;
+}
+}  // namespace
+
+extern "C" int64_t pg_clustering_noalloc_max_nodes(void) { return NOALLOC_SCRATCH_WORDS - 2; }
+
+extern "C" pg_status pg_clustering_noalloc(const int32_t* R, const int32_t* C, int32_t n, float* cp, int64_t* triangles,
+                                           void* stream)
+{
+    if (!R || !cp || n < 0) return PG_ERR_INVALID;
+    if ((int64_t)n > pg_clustering_noalloc_max_nodes()) return PG_ERR_TOO_LARGE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PG_ERR_NO_DEVICE;
+    // First call on this device: resolve the array's device address with the
+    // device current (the host-side symbol is not a device address).
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PG_ERR_CUDA;
+        g_noalloc_ptr[dev] = (unsigned long long*)p;
+    }
+    if (n == 0) return PG_OK;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return PG_ERR_CUDA;
+    size_t smem = (size_t)((n + 31) / 32) * 4;
+    if (smem > prop.sharedMemPerBlockOptin - 4096) return PG_ERR_TOO_LARGE;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_triangles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return PG_ERR_CUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long* tri2 = g_noalloc_ptr[dev];
+    int* next_node = (int*)(tri2 + (n + 1));
+    k_noalloc_clear<<<prop.multiProcessorCount, 256, 0, st>>>(tri2, (int64_t)n + 2);
+    k_triangles<<<prop.multiProcessorCount * 4, THREADS, smem, st>>>(R, C, n, tri2, next_node);
+    k_cp_binary<<<prop.multiProcessorCount * 4, 256, 0, st>>>(R, n, tri2, cp, (long long*)triangles);
+    return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_CUDA;
+}

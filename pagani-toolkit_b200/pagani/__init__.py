@@ -29,6 +29,7 @@ EXPORTS = [
     "pg_build_opts_default", "pg_build_graph", "pg_sparsity_edges", "pg_correlation_packed",
     "pg_degree", "pg_clustering", "pg_paths", "pg_betweenness", "pg_bfs_sigma", "pg_fw_paths",
     "pg_fw_batched", "pg_newman", "pg_maslov", "pg_maslov_round_size", "pg_smallworld",
+    "pg_clustering_noalloc", "pg_clustering_noalloc_max_nodes",
 ]
 
 
@@ -104,6 +105,9 @@ def lib():
         L.pg_maslov_round_size.argtypes = [i64]
         L.pg_maslov_round_size.restype = i64
         L.pg_smallworld.argtypes = [dbl, vp, i32, dbl, vp, i32, P(dbl), P(dbl), P(dbl)]
+        L.pg_clustering_noalloc.argtypes = [vp, vp, i32, vp, vp, vp]
+        L.pg_clustering_noalloc_max_nodes.argtypes = []
+        L.pg_clustering_noalloc_max_nodes.restype = i64
         _lib = L
     return _lib
 
