@@ -12,14 +12,20 @@
 // All groups that exist when a round sweep starts are independent, and the
 // reference hands out new labels in round order, so processing every pending
 // group of a "generation" together and assigning labels in round order
-// afterwards gives exactly the reference's labelling.  Per generation:
-//   - induced sub-graphs of all groups at once (columns keep original ids,
-//     as the reference's NewCol);
-//   - groups with few edges: one CTA per group runs the whole power
-//     iteration (block barriers only), all such groups in one launch;
-//   - large groups: one cooperative kernel per group, the three reductions
-//     per iteration separated by grid-wide barriers.
-// Reductions are FP64 in a fixed order: results are deterministic.
+// afterwards gives exactly the reference's labelling.  Per generation the
+// induced sub-graphs of all groups are built at once, with columns renumbered
+// to positions inside the group, so the power iteration reads the group's own
+// contiguous vector.  Then, by size:
+//   - small groups: one CTA each; CSR and vectors are staged in shared
+//     memory for the whole power iteration, and the two reductions per step
+//     are block barriers only;
+//   - medium groups: one 16-CTA thread-block cluster each, reductions through
+//     distributed shared memory and cluster barriers;
+//   - large groups: the whole GPU as one cooperative grid, one fat block per
+//     SM so the grid barrier stays short.
+// Each step needs only two reductions: |y| for y = B v, then |v' -+ v| and
+// v'.k for the next step together.  Reductions are FP64 in a fixed order, so
+// results are deterministic.
 #include "pg_internal.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
@@ -31,12 +37,19 @@ namespace cg = cooperative_groups;
 
 namespace {
 constexpr int THREADS = 256;
+constexpr int COOP_THREADS = 512;
 constexpr int MAX_ITER = 10000;
 constexpr double EPSILON = 1e-6;
 constexpr double LAMBDA = 0.01;
-constexpr long long SMALL_EDGES = 1LL << 15;   // at most this many edges: one CTA per group
+constexpr size_t SMEM_CAP = 200 * 1024;        // shared-memory budget of the one-CTA path
 constexpr long long MEDIUM_EDGES = 1LL << 22;  // at most this many edges: one cluster per group
 constexpr int CLUSTER = 16;                    // CTAs per cluster for medium groups
+
+size_t small_bytes(long long n, long long e)
+{
+    // sR (n+1 ints), sC (e ints), kdeg, sumBG, v, v0 (n doubles each), 16-byte aligned parts
+    return ((size_t)(n + 1) * 4 + 15) / 16 * 16 + ((size_t)e * 4 + 15) / 16 * 16 + (size_t)n * 32;
+}
 
 // In-group degree of every member (label of neighbour == label of node).
 __global__ void k_nm_gdeg(const int32_t* __restrict__ R, const int32_t* __restrict__ C,
@@ -54,26 +67,32 @@ __global__ void k_nm_gdeg(const int32_t* __restrict__ R, const int32_t* __restri
     }
 }
 
-// Induced CSR rows (columns keep original node ids and CSR order).
+// Induced CSR rows in CSR order, columns renumbered to the position of the
+// neighbour inside its group (the reference keeps original ids and a
+// node-indexed scatter array, which is the same arithmetic).  Group g's n+1
+// row offsets (relative to its first edge) sit at sR[goff[g] + g ...].
 __global__ void k_nm_gfill(const int32_t* __restrict__ R, const int32_t* __restrict__ C,
-                           const int32_t* __restrict__ label, const int32_t* __restrict__ AD, int32_t P,
-                           const long long* __restrict__ soff, int32_t* __restrict__ sR, int32_t* __restrict__ sC)
+                           const int32_t* __restrict__ label, const int32_t* __restrict__ pos,
+                           const int32_t* __restrict__ AD, int32_t P, const long long* __restrict__ soff,
+                           const long long* __restrict__ goff, const long long* __restrict__ eoff,
+                           const int32_t* __restrict__ gidx, int32_t* __restrict__ sR, int32_t* __restrict__ sC)
 {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     for (int p = gw; p < P; p += nw) {
-        int i = AD[p], li = label[i];
-        long long pos = soff[p];
+        const int i = AD[p], li = label[i], q = gidx[p];
+        const long long e0 = eoff[q];
+        long long w = soff[p];
         if (lane == 0) {
-            sR[p] = (int32_t)pos;
-            if (p == P - 1) sR[P] = (int32_t)soff[P];
+            sR[p + q] = (int32_t)(w - e0);
+            if (p + 1 == goff[q + 1]) sR[p + q + 1] = (int32_t)(soff[p + 1] - e0);
         }
         for (int32_t base = R[i]; base < R[i + 1]; base += 32) {
-            int32_t q = base + lane;
-            bool in = q < R[i + 1] && label[C[q]] == li;
+            int32_t e = base + lane;
+            bool in = e < R[i + 1] && label[C[e]] == li;
             unsigned m = __ballot_sync(0xffffffffu, in);
-            if (in) sC[pos + __popc(m & ((1u << lane) - 1u))] = C[q];
-            pos += __popc(m);
+            if (in) sC[w + __popc(m & ((1u << lane) - 1u))] = pos[C[e]];
+            w += __popc(m);
         }
     }
 }
@@ -95,129 +114,104 @@ __global__ void k_nm_gsumbg(const int32_t* __restrict__ R, const int32_t* __rest
     }
 }
 
-// Sum over the block, result returned to every thread.
-__device__ double block_allsum(double x, double* sh)
-{
-    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    __syncthreads();
-    if (lane == 0) sh[w] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int q = 0; q < nw; q++) t += sh[q];
-        sh[32] = t;
-    }
-    __syncthreads();
-    return sh[32];
-}
-
+// One group: rows are the group's members in ascending node id; sR holds
+// n+1 offsets into sC, sC holds positions inside the group.
 struct Group {
     const int32_t* AD;
-    const int32_t* sR;      // row offsets into sC (global positions)
+    const int32_t* sR;
     const int32_t* sC;
     const double* kdeg;
     const double* sumBG;
-    double* v;
-    double* v0;
+    double* v;      // current vector (the reference's v0 entering a step)
+    double* v0;     // previous vector; holds y inside a step
     int ng;
 };
 
-// Reduction across the CTAs of a thread-block cluster through distributed
-// shared memory: every CTA publishes its block sum in slot[par][k], the
-// cluster barrier orders it, and each CTA adds the published values in rank
-// order (the same order everywhere, so every CTA holds the same total).
-struct ClusterReduce {
-    double slot[2][4];
-    double bcast[4];
-};
-
-__device__ void cluster_sums(cg::cluster_group& cl, ClusterReduce* cr, int par, const double* x, int k, double* out,
-                             double* sh)
+// The reference's Lead_Vector (Modularity_CPU.cpp:224-298) with two
+// reductions per step; `Red` supplies barrier + sum over the threads that own
+// the group.
+template <class Red>
+__device__ double lead_vector(const Group& g, int M, double beta, int* iters, double* resid, Red& red, int tid,
+                              int nthr, int lane, int wid, int nwarp)
 {
-    for (int q = 0; q < k; q++) {
-        double t = block_allsum(x[q], sh);
-        if (threadIdx.x == 0) cr->slot[par][q] = t;
+    double x[3];
+    double vk = 0.0;
+    for (int p = tid; p < g.ng; p += nthr) {
+        double vp = (double)g.AD[p];
+        g.v[p] = vp;
+        vk += vp * g.kdeg[p];
     }
-    __threadfence();
-    cl.sync();
-    if (threadIdx.x == 0) {
-        const int nb = (int)cl.num_blocks();
-        for (int q = 0; q < k; q++) {
-            double t = 0.0;
-            for (int r = 0; r < nb; r++) t += cl.map_shared_rank(cr, r)->slot[par][q];
-            cr->bcast[q] = t;
-        }
-    }
-    __syncthreads();
-    for (int q = 0; q < k; q++) out[q] = cr->bcast[q];
-    __syncthreads();
-}
-
-// Lead_Vector on one cluster (a cluster of one CTA is a single block);
-// returns lambda and fills iterations / residual.
-__device__ double lead_vector_cluster(const Group& g, double* vv, int M, double beta, int* iters, double* resid,
-                                      double* sh, ClusterReduce* cr, int& par)
-{
-    cg::cluster_group cl = cg::this_cluster();
-    const int B = blockDim.x;
-    const int ct = (int)cl.block_rank() * B + threadIdx.x, cth = (int)cl.num_blocks() * B;
-    const int lane = threadIdx.x & 31, cw = ct >> 5, cnw = cth >> 5;
-    for (int p = ct; p < g.ng; p += cth) g.v[p] = (double)g.AD[p];
-    __threadfence();
-    cl.sync();
+    x[0] = vk;
+    red.sum(x, 1);
+    vk = x[0];
     double err1 = 1.0, err2 = 1.0, vnorm = 0.0;
     int iter = 0;
-    double in[2], out[2];
     while (err1 > EPSILON && err2 > EPSILON && iter < MAX_ITER) {
-        double x = 0.0;
-        for (int p = ct; p < g.ng; p += cth) {
-            double vp = g.v[p];
-            g.v0[p] = vp;
-            vv[g.AD[p]] = vp;
-            x += vp * g.kdeg[p];
-        }
-        in[0] = x;
-        cluster_sums(cl, cr, par, in, 1, out, sh);
-        par ^= 1;
-        const double c = out[0] / 2.0 / (double)M;
+        const double c = vk / 2.0 / (double)M;
         double y2 = 0.0;
-        for (int p = cw; p < g.ng; p += cnw) {
+        for (int p = wid; p < g.ng; p += nwarp) {
             double s = 0.0;
-            for (int32_t q = g.sR[p] + lane; q < g.sR[p + 1]; q += 32) s += vv[g.sC[q]];
+            for (int32_t q = g.sR[p] + lane; q < g.sR[p + 1]; q += 32) s += g.v[g.sC[q]];
             for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) {
-                s -= c * g.kdeg[p] + (g.sumBG[p] - beta) * g.v0[p];
-                g.v[p] = s;
+                s -= c * g.kdeg[p] + (g.sumBG[p] - beta) * g.v[p];
+                g.v0[p] = s;
                 y2 += s * s;
             }
         }
-        in[0] = y2;
-        cluster_sums(cl, cr, par, in, 1, out, sh);
-        par ^= 1;
-        vnorm = sqrt(out[0]);
+        x[0] = y2;
+        red.sum(x, 1);
+        vnorm = sqrt(x[0]);
         double e1 = 0.0, e2 = 0.0;
-        for (int p = ct; p < g.ng; p += cth) {
-            double vp = g.v[p] / vnorm;
-            g.v[p] = vp;
-            double d1 = vp - g.v0[p], d2 = vp + g.v0[p];
+        vk = 0.0;
+        for (int p = tid; p < g.ng; p += nthr) {
+            const double vold = g.v[p];
+            const double vp = g.v0[p] / vnorm;
+            const double d1 = vp - vold, d2 = vp + vold;
             e1 += d1 * d1;
             e2 += d2 * d2;
+            vk += vp * g.kdeg[p];
+            g.v0[p] = vold;
+            g.v[p] = vp;
         }
-        in[0] = e1;
-        in[1] = e2;
-        cluster_sums(cl, cr, par, in, 2, out, sh);
-        par ^= 1;
-        err1 = sqrt(out[0]);
-        err2 = sqrt(out[1]);
+        x[0] = e1;
+        x[1] = e2;
+        x[2] = vk;
+        red.sum(x, 3);
+        err1 = sqrt(x[0]);
+        err2 = sqrt(x[1]);
+        vk = x[2];
         iter++;
     }
-    // first entry of largest magnitude decides the sign (Modularity_CPU.cpp:291-296):
-    // per CTA (value, index), then the CTAs in rank order.
-    double best = -1.0;
-    int bi = 0x7fffffff;
-    for (int p = ct; p < g.ng; p += cth) {
-        double m = fabs(g.v[p]);
+    *iters = iter;
+    *resid = fmin(err1, err2);
+    // first entry of largest magnitude decides the sign (Modularity_CPU.cpp:291-296)
+    const int mx = red.argmax_abs(g.v, g.ng, tid, nthr);
+    double lam = 0.0;
+    if (g.ng > 0) lam = (g.v[mx] * g.v0[mx] > 0) ? vnorm : -vnorm;
+    red.sync();
+    return lam;
+}
+
+struct WarpSlots {
+    double warp[32][4];
+    double bcast[4];
+    int par;
+};
+
+__device__ __forceinline__ void warp_reduce(double* x, int k)
+{
+    for (int q = 0; q < k; q++)
+        for (int o = 16; o; o >>= 1) x[q] += __shfl_xor_sync(0xffffffffu, x[q], o);
+}
+
+// per-warp (|v|max, first index) over a strided range
+__device__ __forceinline__ void local_argmax(const double* v, int n, int tid, int nthr, double& best, int& bi)
+{
+    best = -1.0;
+    bi = 0x7fffffff;
+    for (int p = tid; p < n; p += nthr) {
+        double m = fabs(v[p]);
         if (m > best) { best = m; bi = p; }
     }
     for (int o = 16; o; o >>= 1) {
@@ -225,199 +219,324 @@ __device__ double lead_vector_cluster(const Group& g, double* vv, int M, double 
         int oi = __shfl_xor_sync(0xffffffffu, bi, o);
         if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
     }
-    __shared__ double sb[32];
-    __shared__ int si[32];
-    __syncthreads();
-    if (lane == 0) { sb[threadIdx.x >> 5] = best; si[threadIdx.x >> 5] = bi; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double b = -1.0;
-        int ix = 0x7fffffff;
-        for (int q = 0; q < (B >> 5); q++)
-            if (sb[q] > b || (sb[q] == b && si[q] < ix)) { b = sb[q]; ix = si[q]; }
-        cr->slot[par][0] = b;
-        cr->slot[par][1] = (double)ix;
-    }
-    __threadfence();
-    cl.sync();
-    if (threadIdx.x == 0) {
-        double b = -1.0;
-        int ix = 0x7fffffff;
-        for (int r = 0; r < (int)cl.num_blocks(); r++) {
-            const ClusterReduce* o = cl.map_shared_rank(cr, r);
-            double ob = o->slot[par][0];
-            int oi = (int)o->slot[par][1];
-            if (ob > b || (ob == b && oi < ix)) { b = ob; ix = oi; }
-        }
-        si[0] = ix;
-    }
-    par ^= 1;
-    __syncthreads();
-    const int mx = si[0];
-    *iters = iter;
-    *resid = fmin(err1, err2);
-    double lam = 0.0;
-    if (g.ng > 0) lam = (g.v[mx] * g.v0[mx] > 0) ? vnorm : -vnorm;
-    __syncthreads();
-    return lam;
 }
 
-// One group per cluster (cluster size 1 for small groups, up to 16 CTAs for
-// medium ones).  out per group: lambda, it0, res0, it1, res1, subP, subN, shifted.
-__global__ void __launch_bounds__(THREADS)
-k_nm_cluster(const int* __restrict__ glist, const long long* __restrict__ goff, const int32_t* __restrict__ AD,
-             const int32_t* __restrict__ sR, const int32_t* __restrict__ sC, const double* __restrict__ kdeg,
-             const double* __restrict__ sumBG, double* __restrict__ v, double* __restrict__ v0,
-             double* __restrict__ vv, int M, int gpu_rule_above, double* __restrict__ out)
+// block-level (value, index) of the warp results, in warp order (thread 0)
+__device__ __forceinline__ void block_argmax(const WarpSlots& s, int nw, double& b, int& ix)
 {
-    __shared__ double sh[40];
-    __shared__ ClusterReduce cr;
-    cg::cluster_group cl = cg::this_cluster();
-    const int gi = glist[blockIdx.x / cl.num_blocks()];
-    const long long p0 = goff[gi];
+    b = -1.0;
+    ix = 0x7fffffff;
+    for (int ww = 0; ww < nw; ww++)
+        if (s.warp[ww][0] > b || (s.warp[ww][0] == b && (int)s.warp[ww][1] < ix)) {
+            b = s.warp[ww][0];
+            ix = (int)s.warp[ww][1];
+        }
+}
+
+// ---- one CTA owns the group: block barriers only
+struct BlockRed {
+    WarpSlots s;
+    __device__ void sync() { __syncthreads(); }
+    __device__ void sum(double* x, int k)
+    {
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        warp_reduce(x, k);
+        if (lane == 0)
+            for (int q = 0; q < k; q++) s.warp[w][q] = x[q];
+        __syncthreads();
+        if (threadIdx.x < k) {
+            double t = 0.0;
+            for (int ww = 0; ww < nw; ww++) t += s.warp[ww][threadIdx.x];
+            s.bcast[threadIdx.x] = t;
+        }
+        __syncthreads();
+        for (int q = 0; q < k; q++) x[q] = s.bcast[q];
+        __syncthreads();
+    }
+    __device__ int argmax_abs(const double* v, int n, int tid, int nthr)
+    {
+        double best;
+        int bi;
+        local_argmax(v, n, tid, nthr, best, bi);
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        if (lane == 0) { s.warp[w][0] = best; s.warp[w][1] = (double)bi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b;
+            int ix;
+            block_argmax(s, nw, b, ix);
+            s.bcast[0] = (double)(ix == 0x7fffffff ? 0 : ix);
+        }
+        __syncthreads();
+        const int r = (int)s.bcast[0];
+        __syncthreads();
+        return r;
+    }
+};
+
+// ---- a thread-block cluster owns the group: DSMEM partials, cluster barrier
+struct ClusterRed {
+    WarpSlots s;
+    double slot[2][4];
+    __device__ void init()
+    {
+        if (threadIdx.x == 0) s.par = 0;
+        __syncthreads();
+    }
+    __device__ void sync()
+    {
+        __threadfence();
+        cg::this_cluster().sync();
+    }
+    __device__ void sum(double* x, int k)
+    {
+        cg::cluster_group cl = cg::this_cluster();
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        warp_reduce(x, k);
+        if (lane == 0)
+            for (int q = 0; q < k; q++) s.warp[w][q] = x[q];
+        __syncthreads();
+        const int pr = s.par;
+        if (threadIdx.x < k) {
+            double t = 0.0;
+            for (int ww = 0; ww < nw; ww++) t += s.warp[ww][threadIdx.x];
+            slot[pr][threadIdx.x] = t;
+        }
+        // the other slot half is written next; this one again only after
+        // another cluster barrier, when every CTA has read it
+        __threadfence();
+        cl.sync();
+        if (threadIdx.x < k) {
+            double t = 0.0;
+            for (int r = 0; r < (int)cl.num_blocks(); r++) t += cl.map_shared_rank(this, r)->slot[pr][threadIdx.x];
+            s.bcast[threadIdx.x] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s.par = pr ^ 1;
+        for (int q = 0; q < k; q++) x[q] = s.bcast[q];
+        __syncthreads();
+    }
+    __device__ int argmax_abs(const double* v, int n, int tid, int nthr)
+    {
+        cg::cluster_group cl = cg::this_cluster();
+        double best;
+        int bi;
+        local_argmax(v, n, tid, nthr, best, bi);
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        if (lane == 0) { s.warp[w][0] = best; s.warp[w][1] = (double)bi; }
+        __syncthreads();
+        const int pr = s.par;
+        if (threadIdx.x == 0) {
+            double b;
+            int ix;
+            block_argmax(s, nw, b, ix);
+            slot[pr][0] = b;
+            slot[pr][1] = (double)ix;
+        }
+        __threadfence();
+        cl.sync();
+        if (threadIdx.x == 0) {
+            double b = -1.0;
+            int ix = 0x7fffffff;
+            for (int r = 0; r < (int)cl.num_blocks(); r++) {
+                const ClusterRed* o = cl.map_shared_rank(this, r);
+                double ob = o->slot[pr][0];
+                int oi = (int)o->slot[pr][1];
+                if (ob > b || (ob == b && oi < ix)) { b = ob; ix = oi; }
+            }
+            s.bcast[0] = (double)(ix == 0x7fffffff ? 0 : ix);
+            s.par = pr ^ 1;
+        }
+        __syncthreads();
+        const int r = (int)s.bcast[0];
+        __syncthreads();
+        return r;
+    }
+};
+
+// ---- the whole cooperative grid owns the group
+struct GridRed {
+    WarpSlots s;
+    double* part;   // [2][gridDim.x][4], alternate halves per reduction
+    __device__ void init(double* p)
+    {
+        if (threadIdx.x == 0) { part = p; s.par = 0; }
+        __syncthreads();
+    }
+    __device__ void sync() { cg::this_grid().sync(); }
+    __device__ void sum(double* x, int k)
+    {
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        warp_reduce(x, k);
+        if (lane == 0)
+            for (int q = 0; q < k; q++) s.warp[w][q] = x[q];
+        __syncthreads();
+        const int pr = s.par;
+        double* pp = part + (size_t)pr * gridDim.x * 4;
+        if (threadIdx.x < k) {
+            double t = 0.0;
+            for (int ww = 0; ww < nw; ww++) t += s.warp[ww][threadIdx.x];
+            pp[blockIdx.x * 4 + threadIdx.x] = t;
+        }
+        // one grid barrier per reduction: the other half of `part` is written
+        // next, and this half again only after another barrier
+        cg::this_grid().sync();
+        if (threadIdx.x < k) {
+            double t = 0.0;
+            for (int b = 0; b < (int)gridDim.x; b++) t += pp[b * 4 + threadIdx.x];
+            s.bcast[threadIdx.x] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s.par = pr ^ 1;
+        for (int q = 0; q < k; q++) x[q] = s.bcast[q];
+        __syncthreads();
+    }
+    __device__ int argmax_abs(const double* v, int n, int tid, int nthr)
+    {
+        double best;
+        int bi;
+        local_argmax(v, n, tid, nthr, best, bi);
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        if (lane == 0) { s.warp[w][0] = best; s.warp[w][1] = (double)bi; }
+        __syncthreads();
+        const int pr = s.par;
+        double* pp = part + (size_t)pr * gridDim.x * 4;
+        if (threadIdx.x == 0) {
+            double b;
+            int ix;
+            block_argmax(s, nw, b, ix);
+            pp[blockIdx.x * 4 + 0] = b;
+            pp[blockIdx.x * 4 + 1] = (double)ix;
+        }
+        cg::this_grid().sync();
+        if (threadIdx.x == 0) {
+            double b = -1.0;
+            int ix = 0x7fffffff;
+            for (int r = 0; r < (int)gridDim.x; r++) {
+                double ob = pp[r * 4 + 0];
+                int oi = (int)pp[r * 4 + 1];
+                if (ob > b || (ob == b && oi < ix)) { b = ob; ix = oi; }
+            }
+            s.bcast[0] = (double)(ix == 0x7fffffff ? 0 : ix);
+            s.par = pr ^ 1;
+        }
+        __syncthreads();
+        const int r = (int)s.bcast[0];
+        __syncthreads();
+        return r;
+    }
+};
+
+struct Inputs {
+    const long long* goff;   // group start in member order (G+1)
+    const long long* eoff;   // group start in edge order (G+1)
+    const int32_t* AD;
+    const int32_t* sR;       // group g's n+1 row offsets start at goff[g] + g
+    const int32_t* sC;
+    const double* kdeg;
+    const double* sumBG;
+    double* v;
+    double* v0;
+    int M;
+    int gpu_rule_above;
+    double* out;             // per group: lambda, it0, res0, it1, res1, subP, subN, shifted
+};
+
+__device__ __forceinline__ Group global_group(const Inputs& in, int gi)
+{
+    const long long p0 = in.goff[gi];
     Group g;
-    g.ng = (int)(goff[gi + 1] - p0);
-    g.AD = AD + p0; g.sR = sR + p0; g.sC = sC; g.kdeg = kdeg + p0; g.sumBG = sumBG + p0;
-    g.v = v + p0; g.v0 = v0 + p0;
-    int par = 0;
+    g.ng = (int)(in.goff[gi + 1] - p0);
+    g.AD = in.AD + p0;
+    g.sR = in.sR + p0 + gi;
+    g.sC = in.sC + in.eoff[gi];
+    g.kdeg = in.kdeg + p0;
+    g.sumBG = in.sumBG + p0;
+    g.v = in.v + p0;
+    g.v0 = in.v0 + p0;
+    return g;
+}
+
+// Both passes of Sub_Partition for one group.
+template <class Red>
+__device__ void sub_partition(const Group& g, const Inputs& in, int gi, Red& red, int tid, int nthr, int lane,
+                              int wid, int nwarp, bool writer)
+{
     int it0, it1 = 0;
     double r0, r1 = 0.0;
-    double lam = lead_vector_cluster(g, vv, M, 0.0, &it0, &r0, sh, &cr, par);
-    const double below = g.ng > gpu_rule_above ? -LAMBDA : 0.0;
+    double lam = lead_vector(g, in.M, 0.0, &it0, &r0, red, tid, nthr, lane, wid, nwarp);
+    const double below = g.ng > in.gpu_rule_above ? -LAMBDA : 0.0;
     const bool shifted = lam < below;
-    if (shifted) lam += lead_vector_cluster(g, vv, M, -lam, &it1, &r1, sh, &cr, par);
+    if (shifted) lam += lead_vector(g, in.M, -lam, &it1, &r1, red, tid, nthr, lane, wid, nwarp);
+    double x[3] = {0.0, 0.0, 0.0};
+    for (int p = tid; p < g.ng; p += nthr) {
+        x[0] += g.v[p] > 0.0;
+        x[1] += g.v[p] <= 0.0;
+    }
+    red.sum(x, 2);
+    if (writer) {
+        double* o = in.out + (size_t)gi * 8;
+        o[0] = lam; o[1] = it0; o[2] = r0; o[3] = it1; o[4] = r1; o[5] = x[0]; o[6] = x[1]; o[7] = shifted;
+    }
+}
+
+// small groups: one CTA per group, everything in shared memory
+__global__ void __launch_bounds__(THREADS)
+k_nm_block(const int* __restrict__ glist, Inputs in)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ BlockRed red;
+    const int gi = glist[blockIdx.x];
+    const Group gg = global_group(in, gi);
+    const int n = gg.ng;
+    const long long ne = in.eoff[gi + 1] - in.eoff[gi];
+    int32_t* sR = (int32_t*)sm;
+    int32_t* sC = (int32_t*)(sm + ((size_t)(n + 1) * 4 + 15) / 16 * 16);
+    double* dv = (double*)((unsigned char*)sC + ((size_t)ne * 4 + 15) / 16 * 16);
+    for (int p = threadIdx.x; p <= n; p += blockDim.x) sR[p] = gg.sR[p];
+    for (int p = threadIdx.x; p < n; p += blockDim.x) {
+        dv[p] = gg.kdeg[p];
+        dv[n + p] = gg.sumBG[p];
+    }
+    for (long long q = threadIdx.x; q < ne; q += blockDim.x) sC[q] = gg.sC[q];
+    __syncthreads();
+    Group g = gg;
+    g.sR = sR;
+    g.sC = sC;
+    g.kdeg = dv;
+    g.sumBG = dv + n;
+    g.v = dv + 2 * n;
+    g.v0 = dv + 3 * n;
+    sub_partition(g, in, gi, red, threadIdx.x, blockDim.x, threadIdx.x & 31, threadIdx.x >> 5, blockDim.x >> 5,
+                  threadIdx.x == 0);
+    for (int p = threadIdx.x; p < n; p += blockDim.x) gg.v[p] = g.v[p];   // the labels are assigned from v
+}
+
+// medium groups: one cluster per group, global memory
+__global__ void __launch_bounds__(THREADS)
+k_nm_cluster(const int* __restrict__ glist, Inputs in)
+{
+    __shared__ ClusterRed red;
+    cg::cluster_group cl = cg::this_cluster();
+    red.init();
+    cl.sync();
+    const int gi = glist[blockIdx.x / cl.num_blocks()];
+    Group g = global_group(in, gi);
     const int ct = (int)cl.block_rank() * blockDim.x + threadIdx.x, cth = (int)cl.num_blocks() * blockDim.x;
-    double in[2] = {0.0, 0.0}, res[2];
-    for (int p = ct; p < g.ng; p += cth) {
-        in[0] += g.v[p] > 0.0;
-        in[1] += g.v[p] <= 0.0;
-    }
-    cluster_sums(cl, &cr, par, in, 2, res, sh);
-    if (cl.block_rank() == 0 && threadIdx.x == 0) {
-        double* o = out + (size_t)gi * 8;
-        o[0] = lam; o[1] = it0; o[2] = r0; o[3] = it1; o[4] = r1; o[5] = res[0]; o[6] = res[1]; o[7] = shifted;
-    }
+    sub_partition(g, in, gi, red, ct, cth, threadIdx.x & 31, ct >> 5, cth >> 5, ct == 0);
     // no CTA may exit while another still reads its shared memory
     cl.sync();
 }
 
-// ---- large groups: cooperative kernel, one group, one pass (beta given)
-struct LVArgs {
-    Group g;
-    int M;
-    double beta;
-    double* vv;
-    double* part;   // [grid][4]
-    double* out;    // lambda, iterations, residual, subP, subN
-};
-
-__device__ double grid_total(const double* part, int col, double* sh)
+// large groups: the whole cooperative grid, one group per launch
+__global__ void __launch_bounds__(COOP_THREADS)
+k_nm_coop(int gi, Inputs in, double* __restrict__ part)
 {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int b = 0; b < (int)gridDim.x; b++) t += part[b * 4 + col];
-        sh[33] = t;
-    }
-    __syncthreads();
-    return sh[33];
-}
-
-__device__ double block_sum0(double x, double* sh)
-{
-    return block_allsum(x, sh);
-}
-
-__global__ void __launch_bounds__(THREADS) k_nm_coop(LVArgs a)
-{
-    cg::grid_group grid = cg::this_grid();
-    __shared__ double sh[40];
-    const Group& g = a.g;
+    __shared__ GridRed red;
+    red.init(part);
+    Group g = global_group(in, gi);
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    const int gw = tid >> 5, nw = nthr >> 5;
-    for (int p = tid; p < g.ng; p += nthr) g.v[p] = (double)g.AD[p];
-    grid.sync();
-    double err1 = 1.0, err2 = 1.0, vnorm = 0.0;
-    int iter = 0;
-    while (err1 > EPSILON && err2 > EPSILON && iter < MAX_ITER) {
-        double x = 0.0;
-        for (int p = tid; p < g.ng; p += nthr) {
-            double vp = g.v[p];
-            g.v0[p] = vp;
-            a.vv[g.AD[p]] = vp;
-            x += vp * g.kdeg[p];
-        }
-        double bs = block_sum0(x, sh);
-        if (threadIdx.x == 0) a.part[blockIdx.x * 4 + 0] = bs;
-        grid.sync();
-        const double c = grid_total(a.part, 0, sh) / 2.0 / (double)a.M;
-        double y2 = 0.0;
-        for (int p = gw; p < g.ng; p += nw) {
-            double s = 0.0;
-            for (int32_t q = g.sR[p] + lane; q < g.sR[p + 1]; q += 32) s += a.vv[g.sC[q]];
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) {
-                s -= c * g.kdeg[p] + (g.sumBG[p] - a.beta) * g.v0[p];
-                g.v[p] = s;
-                y2 += s * s;
-            }
-        }
-        bs = block_sum0(y2, sh);
-        if (threadIdx.x == 0) a.part[blockIdx.x * 4 + 1] = bs;
-        grid.sync();
-        vnorm = sqrt(grid_total(a.part, 1, sh));
-        double e1 = 0.0, e2 = 0.0;
-        for (int p = tid; p < g.ng; p += nthr) {
-            double vp = g.v[p] / vnorm;
-            g.v[p] = vp;
-            double d1 = vp - g.v0[p], d2 = vp + g.v0[p];
-            e1 += d1 * d1;
-            e2 += d2 * d2;
-        }
-        bs = block_sum0(e1, sh);
-        if (threadIdx.x == 0) a.part[blockIdx.x * 4 + 2] = bs;
-        bs = block_sum0(e2, sh);
-        if (threadIdx.x == 0) a.part[blockIdx.x * 4 + 3] = bs;
-        grid.sync();
-        err1 = sqrt(grid_total(a.part, 2, sh));
-        err2 = sqrt(grid_total(a.part, 3, sh));
-        iter++;
-        grid.sync();
-    }
-    if (blockIdx.x == 0) {
-        double best = -1.0;
-        int bi = 0x7fffffff;
-        double sp = 0.0, sn = 0.0;
-        for (int p = threadIdx.x; p < g.ng; p += blockDim.x) {
-            double m = fabs(g.v[p]);
-            if (m > best) { best = m; bi = p; }
-            sp += g.v[p] > 0.0;
-            sn += g.v[p] <= 0.0;
-        }
-        for (int o = 16; o; o >>= 1) {
-            double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-        }
-        __shared__ double sb[32];
-        __shared__ int si[32];
-        const int w = threadIdx.x >> 5, nwb = blockDim.x >> 5;
-        if (lane == 0) { sb[w] = best; si[w] = bi; }
-        sp = block_allsum(sp, sh);
-        sn = block_allsum(sn, sh);
-        if (threadIdx.x == 0) {
-            double b = -1.0;
-            int ix = 0;
-            for (int q = 0; q < nwb; q++)
-                if (sb[q] > b || (sb[q] == b && si[q] < ix)) { b = sb[q]; ix = si[q]; }
-            a.out[0] = g.ng > 0 ? ((g.v[ix] * g.v0[ix] > 0) ? vnorm : -vnorm) : 0.0;
-            a.out[1] = iter;
-            a.out[2] = fmin(err1, err2);
-            a.out[3] = sp;
-            a.out[4] = sn;
-        }
-    }
+    sub_partition(g, in, gi, red, tid, nthr, threadIdx.x & 31, tid >> 5, nthr >> 5, tid == 0);
 }
 
 __global__ void k_nm_gassign(const int32_t* __restrict__ AD, const int32_t* __restrict__ gidx,
@@ -463,36 +582,35 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         if (n_modules) *n_modules = 1;
         return PG_OK;
     }
-    int32_t *label, *AD, *gidx, *kg, *sR, *sC, *dbase, *glist;
-    long long *soff, *goff, *innerM;
-    double *v, *v0, *vv, *sumBG, *kdeg, *part, *out, *dcoef;
+    int32_t *label, *AD, *gidx, *kg, *sR, *sC, *dbase, *glist, *pos;
+    long long *soff, *goff, *eoff, *innerM;
+    double *v, *v0, *sumBG, *kdeg, *part, *out, *dcoef;
     unsigned long long* acc;
     PG_TRY(pg_wst(ctx, "nm.label", (size_t)n + 1, &label));
     PG_TRY(pg_wst(ctx, "nm.AD", (size_t)n + 1, &AD));
+    PG_TRY(pg_wst(ctx, "nm.pos", (size_t)n + 1, &pos));
     PG_TRY(pg_wst(ctx, "nm.gidx", (size_t)n + 1, &gidx));
     PG_TRY(pg_wst(ctx, "nm.kg", (size_t)n + 1, &kg));
     PG_TRY(pg_wst(ctx, "nm.soff", (size_t)n + 2, &soff));
-    PG_TRY(pg_wst(ctx, "nm.sR", (size_t)n + 2, &sR));
     PG_TRY(pg_wst(ctx, "nm.sC", (size_t)nnz + 1, &sC));
     PG_TRY(pg_wst(ctx, "nm.v", (size_t)n + 1, &v));
     PG_TRY(pg_wst(ctx, "nm.v0", (size_t)n + 1, &v0));
-    PG_TRY(pg_wst(ctx, "nm.vv", (size_t)n + 1, &vv));
     PG_TRY(pg_wst(ctx, "nm.sumBG", (size_t)n + 1, &sumBG));
     PG_TRY(pg_wst(ctx, "nm.kdeg", (size_t)n + 1, &kdeg));
     PG_TRY(pg_wst(ctx, "nm.acc", 4, &acc));
     int per_sm = 0;
-    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nm_coop, THREADS, 0));
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nm_coop, COOP_THREADS, 0));
     if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "power iteration kernel cannot be resident");
-    const int coop_grid = per_sm * ctx->sm_count;
-    // widest cluster the device accepts for the medium-group kernel (16 needs the non-portable opt-in)
-    int cluster = CLUSTER;
+    const int coop_grid = ctx->sm_count;   // one fat block per SM keeps the grid barrier short
+    PG_TRY(pg_wst(ctx, "nm.part", (size_t)coop_grid * 8 + 8, &part));
+    int cluster = CLUSTER;  // 16 needs the non-portable opt-in
     if (cudaFuncSetAttribute(k_nm_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
         cluster = 8;
     }
-    PG_TRY(pg_wst(ctx, "nm.part", (size_t)coop_grid * 4 + 4, &part));
+    const size_t smem_cap = std::min(SMEM_CAP, (size_t)ctx->smem_optin - 8192);
+    PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     PG_CUDA(ctx, cudaMemsetAsync(label, 0, sizeof(int32_t) * (n + 1), ctx->stream));
-    PG_CUDA(ctx, cudaMemsetAsync(vv, 0, sizeof(double) * (n + 1), ctx->stream));
 
     std::vector<int32_t> hR(n + 1), hl(n);
     PG_TRY(pg_d2h(ctx, hR.data(), g->R, sizeof(int32_t) * (n + 1)));
@@ -500,7 +618,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     std::vector<int32_t> adjust((size_t)n + 2, 0);
     int Round = 0, Max_Result = 0, Module_Num = 1, Index = 1;
     char line[512];
-    std::vector<int32_t> hAD(n), hgidx(n);
+    std::vector<int32_t> hAD(n), hgidx(n), hpos(n, 0);
     // wall time per kind of power-iteration launch, reported in the log
     double t_small = 0, t_medium = 0, t_large = 0, t_setup = 0;
     long long it_small = 0, it_medium = 0, it_large = 0;
@@ -527,12 +645,15 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                     int q = hl[i] - lo;
                     hAD[cur[q]] = i;
                     hgidx[cur[q]] = q;
+                    hpos[i] = (int32_t)(cur[q] - hgoff[q]);
                     cur[q]++;
                     hinner[q] += hR[i + 1] - hR[i];
                 }
         }
         if (P == 0) { Round = hi + 1; continue; }
+        PG_TRY(pg_wst(ctx, "nm.sR", (size_t)P + G + 2, &sR));   // n+1 offsets per group
         PG_TRY(pg_wst(ctx, "nm.goff", (size_t)G + 1, &goff));
+        PG_TRY(pg_wst(ctx, "nm.eoff", (size_t)G + 1, &eoff));
         PG_TRY(pg_wst(ctx, "nm.inner", (size_t)G, &innerM));
         PG_TRY(pg_wst(ctx, "nm.out", (size_t)G * 8, &out));
         PG_TRY(pg_wst(ctx, "nm.glist", (size_t)G, &glist));
@@ -540,100 +661,89 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         PG_TRY(pg_wst(ctx, "nm.coef", (size_t)G, &dcoef));
         PG_CUDA(ctx, cudaMemcpyAsync(AD, hAD.data(), sizeof(int32_t) * P, cudaMemcpyHostToDevice, ctx->stream));
         PG_CUDA(ctx, cudaMemcpyAsync(gidx, hgidx.data(), sizeof(int32_t) * P, cudaMemcpyHostToDevice, ctx->stream));
-        PG_CUDA(ctx, cudaMemcpyAsync(goff, hgoff.data(), sizeof(long long) * (G + 1), cudaMemcpyHostToDevice, ctx->stream));
-        PG_CUDA(ctx, cudaMemcpyAsync(innerM, hinner.data(), sizeof(long long) * G, cudaMemcpyHostToDevice, ctx->stream));
+        PG_CUDA(ctx, cudaMemcpyAsync(pos, hpos.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+        PG_CUDA(ctx, cudaMemcpyAsync(goff, hgoff.data(), sizeof(long long) * (G + 1), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        PG_CUDA(ctx, cudaMemcpyAsync(innerM, hinner.data(), sizeof(long long) * G, cudaMemcpyHostToDevice,
+                                     ctx->stream));
         k_nm_gdeg<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, label, AD, P, kg);
         PG_LAUNCHED(ctx);
         PG_TRY(pg_scan_counts(ctx, kg, (int64_t*)soff, P));
-        k_nm_gfill<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, label, AD, P, soff, sR, sC);
+        std::vector<long long> hsoff(P + 1), heoff(G + 1);
+        PG_TRY(pg_d2h(ctx, hsoff.data(), soff, sizeof(long long) * (P + 1)));
+        for (int q = 0; q <= G; q++) heoff[q] = hsoff[hgoff[q]];
+        PG_CUDA(ctx, cudaMemcpyAsync(eoff, heoff.data(), sizeof(long long) * (G + 1), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        k_nm_gfill<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, label, pos, AD, P, soff, goff, eoff, gidx, sR, sC);
         PG_LAUNCHED(ctx);
         k_nm_gsumbg<<<grid, 256, 0, ctx->stream>>>(g->R, AD, kg, gidx, innerM, P, M, sumBG, kdeg);
         PG_LAUNCHED(ctx);
-        std::vector<long long> hsoff(P + 1);
-        PG_TRY(pg_d2h(ctx, hsoff.data(), soff, sizeof(long long) * (P + 1)));
         t_setup += ms_since(t_gen);
-        // ---- power iterations
+        // ---- power iterations, groups by size
+        Inputs in;
+        in.goff = goff; in.eoff = eoff; in.AD = AD; in.sR = sR; in.sC = sC; in.kdeg = kdeg; in.sumBG = sumBG;
+        in.v = v; in.v0 = v0; in.M = M; in.gpu_rule_above = gpu_rule_above; in.out = out;
         std::vector<int> small, medium, large;
+        size_t smem_small = 16;
         for (int q = 0; q < G; q++) {
-            long long ng = hgoff[q + 1] - hgoff[q];
+            const long long ng = hgoff[q + 1] - hgoff[q];
             if (ng == 0) continue;
-            long long edges = hsoff[hgoff[q + 1]] - hsoff[hgoff[q]];
-            if (edges <= SMALL_EDGES) small.push_back(q);
-            else if (edges <= MEDIUM_EDGES && cluster > 1) medium.push_back(q);
-            else large.push_back(q);
+            const long long edges = heoff[q + 1] - heoff[q];
+            const size_t b = small_bytes(ng, edges);
+            if (b <= smem_cap) {
+                small.push_back(q);
+                smem_small = std::max(smem_small, b);
+            } else if (edges <= MEDIUM_EDGES && cluster > 1) {
+                medium.push_back(q);
+            } else {
+                large.push_back(q);
+            }
         }
         std::vector<double> hout((size_t)G * 8, 0.0);
-        if (!small.empty() || !medium.empty()) {
-            std::vector<int> lists(small);
-            lists.insert(lists.end(), medium.begin(), medium.end());
+        std::vector<int> lists(small);
+        lists.insert(lists.end(), medium.begin(), medium.end());
+        if (!lists.empty())
             PG_CUDA(ctx, cudaMemcpyAsync(glist, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice,
                                          ctx->stream));
-            if (!small.empty()) {
-                auto t0 = now();
-                k_nm_cluster<<<(int)small.size(), THREADS, 0, ctx->stream>>>(glist, goff, AD, sR, sC, kdeg, sumBG, v,
-                                                                             v0, vv, M, gpu_rule_above, out);
-                PG_LAUNCHED(ctx);
-                PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-                t_small += ms_since(t0);
-            }
-            if (!medium.empty()) {
-                cudaLaunchConfig_t cfg = {};
-                cudaLaunchAttribute attr[1];
-                attr[0].id = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = cluster;
-                attr[0].val.clusterDim.y = 1;
-                attr[0].val.clusterDim.z = 1;
-                cfg.gridDim = dim3((unsigned)(medium.size() * cluster));
-                cfg.blockDim = dim3(THREADS);
-                cfg.stream = ctx->stream;
-                cfg.attrs = attr;
-                cfg.numAttrs = 1;
-                const int* mlist = glist + small.size();
-                auto t0 = now();
-                PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_cluster, mlist, (const long long*)goff, (const int32_t*)AD,
-                                                (const int32_t*)sR, (const int32_t*)sC, (const double*)kdeg,
-                                                (const double*)sumBG, v, v0, vv, M, (int)gpu_rule_above, out));
-                PG_LAUNCHED(ctx);
-                PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-                t_medium += ms_since(t0);
-            }
-            PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * 8));
-            for (int q : small) it_small += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
-            for (int q : medium) it_medium += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
+        auto t0 = now();
+        if (!small.empty()) {
+            k_nm_block<<<(int)small.size(), THREADS, smem_small, ctx->stream>>>(glist, in);
+            PG_LAUNCHED(ctx);
+            PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         }
-        auto t_l = now();
+        t_small += ms_since(t0);
+        t0 = now();
+        if (!medium.empty()) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = cluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3((unsigned)(medium.size() * cluster));
+            cfg.blockDim = dim3(THREADS);
+            cfg.stream = ctx->stream;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            const int* mlist = glist + small.size();
+            PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_cluster, mlist, in));
+            PG_LAUNCHED(ctx);
+            PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+        t_medium += ms_since(t0);
+        t0 = now();
         for (int q : large) {
-            const long long p0 = hgoff[q];
-            LVArgs a;
-            a.g.ng = (int)(hgoff[q + 1] - p0);
-            a.g.AD = AD + p0; a.g.sR = sR + p0; a.g.sC = sC; a.g.kdeg = kdeg + p0; a.g.sumBG = sumBG + p0;
-            a.g.v = v + p0; a.g.v0 = v0 + p0;
-            a.M = M; a.beta = 0.0; a.vv = vv; a.part = part; a.out = out + (size_t)q * 8;
-            double r[2][5];
-            bool shifted = false;
-            for (int pass = 0; pass < 2; pass++) {
-                void* args[] = {(void*)&a};
-                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_nm_coop, dim3(coop_grid), dim3(THREADS), args, 0,
-                                                         ctx->stream));
-                PG_LAUNCHED(ctx);
-                PG_TRY(pg_d2h(ctx, r[pass], a.out, sizeof(double) * 5));
-                if (pass == 0) {
-                    const double below = a.g.ng > gpu_rule_above ? -LAMBDA : 0.0;
-                    if (!(r[0][0] < below)) break;
-                    shifted = true;
-                    a.beta = -r[0][0];
-                }
-            }
-            double* o = &hout[(size_t)q * 8];
-            o[0] = shifted ? r[0][0] + r[1][0] : r[0][0];
-            o[1] = r[0][1]; o[2] = r[0][2];
-            o[3] = shifted ? r[1][1] : 0; o[4] = shifted ? r[1][2] : 0;
-            o[5] = shifted ? r[1][3] : r[0][3];
-            o[6] = shifted ? r[1][4] : r[0][4];
-            o[7] = shifted;
-            it_large += (long long)(o[1] + o[3]);
+            int qq = q;
+            void* args[] = {(void*)&qq, (void*)&in, (void*)&part};
+            PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_nm_coop, dim3(coop_grid), dim3(COOP_THREADS), args, 0,
+                                                     ctx->stream));
+            PG_LAUNCHED(ctx);
         }
-        t_large += ms_since(t_l);
+        PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * 8));
+        t_large += ms_since(t0);
+        for (int q : small) it_small += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
+        for (int q : medium) it_medium += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
+        for (int q : large) it_large += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
         // ---- decisions in round order (labels exactly as the sequential reference)
         std::vector<int> hbase(G, -1);
         std::vector<double> hcoef(G, 0.0);

@@ -48,3 +48,59 @@ def test_degree_matches_reference_rule(ctx):
     deg, iso = ctx.degree(g)
     d_or, iso_or = O.degree(R)
     assert np.array_equal(deg, d_or) and iso == iso_or
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+@pytest.mark.parametrize("mode,value,sign", [("r", 0.3, "signed"), ("s", 1.0, "abs")])
+def test_edge_set_exact_with_tight_band(ctx, precision, mode, value, sign):
+    # a 1e-4 recheck band still reproduces the FP64 edge set: the tile error of
+    # both Gram paths is far below half of it
+    N, T = 1200, 240
+    bold = synth.bold_series(N, T, 20, 31337)
+    g, info = ctx.build_graph(bold, mode=mode, value=value, sign=sign, precision=precision, guard=1e-4)
+    R, C, _ = g.to_csr()
+    Ro, Co, _, tau = _oracle_graph(bold, mode, value, sign)
+    assert np.array_equal(R, Ro) and np.array_equal(C, Co)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_zero_variance_and_duplicate_voxels(ctx, precision):
+    # flat series give r = 0 (the reference's NaN -> 0 rule); duplicated
+    # series give r at +-1 and go through the range rule in FP64
+    bold = synth.bold_series(300, 64, 5, 99)
+    bold[:, 5] = 3.0
+    bold[:, 17] = bold[:, 3]
+    bold[:, 18] = -bold[:, 3]
+    for mode, value in (("r", 0.3), ("s", 3.0), ("r", -0.5)):
+        g, info = ctx.build_graph(bold, mode=mode, value=value, precision=precision)
+        R, C, _ = g.to_csr()
+        Ro, Co, _, _ = _oracle_graph(bold, mode, value)
+        assert info["zero_variance"] == 1
+        assert np.array_equal(R, Ro) and np.array_equal(C, Co)
+
+
+def test_weighted_values_exact(ctx):
+    bold = synth.bold_series(500, 200, 8, 7)
+    thr = O.weighted_r_threshold(np.float32(0.2))
+    g, _ = ctx.build_graph(bold, mode="r", value=thr, weighted=True, precision="bf16x3")
+    R, C, V = g.to_csr()
+    z, _ = O.zscore(bold)
+    Ro, Co, Vo = O.graph_r(O.corr_packed(z, weighted=True), 500, thr, weighted=True)
+    assert np.array_equal(R, Ro) and np.array_equal(C, Co) and np.array_equal(V, Vo)
+
+
+def test_correlation_packed(ctx):
+    bold = synth.bold_series(200, 50, 4, 3)
+    r = ctx.correlation_packed(bold)
+    z, _ = O.zscore(bold)
+    assert np.array_equal(r, O.corr_packed(z).astype(np.float32))
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 127, 128, 129, 257])
+def test_tiny_and_ragged_sizes(ctx, N):
+    bold = synth.bold_series(N, 70, 3, 5 + N)
+    for precision in ("fp32", "bf16x3"):
+        g, info = ctx.build_graph(bold, mode="s", value=10.0, precision=precision)
+        R, C, _ = g.to_csr()
+        Ro, Co, _, _ = _oracle_graph(bold, "s", 10.0)
+        assert np.array_equal(R, Ro) and np.array_equal(C, Co)
