@@ -126,14 +126,29 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                         int u = f < e ? a.C[f] : 0;
                         u64 fu = f < e ? (cur[u] & need) : 0ULL;
                         unsigned m = __ballot_sync(0xffffffffu, fu != 0ULL);
+                        // up to four active neighbours per step, loads issued together
                         while (m) {
-                            int j = __ffs(m) - 1;
-                            m &= m - 1;
-                            int uj = __shfl_sync(0xffffffffu, u, j);
-                            u64 fj = shfl64(fu, j);
-                            const u64* row = a.sigma + (size_t)uj * S;
-                            if (fj & lo_bit) sg0 += row[lane];
-                            if (fj & hi_bit) sg1 += row[lane + 32];
+                            int j[4];
+#pragma unroll
+                            for (int t = 0; t < 4; t++) {
+                                j[t] = m ? __ffs(m) - 1 : -1;
+                                m &= m ? m - 1 : 0u;
+                            }
+                            u64 x0[4], x1[4];
+#pragma unroll
+                            for (int t = 0; t < 4; t++) {
+                                const int jj = j[t] < 0 ? j[0] : j[t];
+                                const int uj = __shfl_sync(0xffffffffu, u, jj);
+                                const u64 fj = j[t] < 0 ? 0ULL : shfl64(fu, jj);
+                                const u64* row = a.sigma + (size_t)uj * S;
+                                x0[t] = (fj & lo_bit) ? row[lane] : 0ULL;
+                                x1[t] = (fj & hi_bit) ? row[lane + 32] : 0ULL;
+                            }
+#pragma unroll
+                            for (int t = 0; t < 4; t++) {
+                                sg0 += x0[t];
+                                sg1 += x1[t];
+                            }
                         }
                     }
                     const unsigned b0 = __ballot_sync(0xffffffffu, sg0 != 0ULL);
@@ -200,13 +215,27 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                                 u64 mw = f < e ? (a.fhist[(size_t)(lv + 1) * n + w] & mine_m) : 0ULL;
                                 unsigned bm = __ballot_sync(0xffffffffu, mw != 0ULL);
                                 while (bm) {
-                                    int j = __ffs(bm) - 1;
-                                    bm &= bm - 1;
-                                    int wj = __shfl_sync(0xffffffffu, w, j);
-                                    u64 mj = shfl64(mw, j);
-                                    const double* row = a.coef + (size_t)wj * S;
-                                    if (mj & lo_bit) acc0 += row[lane];
-                                    if (mj & hi_bit) acc1 += row[lane + 32];
+                                    int j[4];
+#pragma unroll
+                                    for (int t = 0; t < 4; t++) {
+                                        j[t] = bm ? __ffs(bm) - 1 : -1;
+                                        bm &= bm ? bm - 1 : 0u;
+                                    }
+                                    double y0[4], y1[4];
+#pragma unroll
+                                    for (int t = 0; t < 4; t++) {
+                                        const int jj = j[t] < 0 ? j[0] : j[t];
+                                        const int wj = __shfl_sync(0xffffffffu, w, jj);
+                                        const u64 mj = j[t] < 0 ? 0ULL : shfl64(mw, jj);
+                                        const double* row = a.coef + (size_t)wj * S;
+                                        y0[t] = (mj & lo_bit) ? row[lane] : 0.0;
+                                        y1[t] = (mj & hi_bit) ? row[lane + 32] : 0.0;
+                                    }
+#pragma unroll
+                                    for (int t = 0; t < 4; t++) {
+                                        acc0 += y0[t];
+                                        acc1 += y1[t];
+                                    }
                                 }
                             } else {
                                 int cnt = min(32, e - base);

@@ -283,11 +283,9 @@ struct ClusterRed {
         if (threadIdx.x == 0) s.par = 0;
         __syncthreads();
     }
-    __device__ void sync()
-    {
-        __threadfence();
-        cg::this_cluster().sync();
-    }
+    // cluster barriers release/acquire at cluster scope, which orders the
+    // global-memory vector writes of one CTA before the reads of another
+    __device__ void sync() { cg::this_cluster().sync(); }
     __device__ void sum(double* x, int k)
     {
         cg::cluster_group cl = cg::this_cluster();
@@ -304,7 +302,6 @@ struct ClusterRed {
         }
         // the other slot half is written next; this one again only after
         // another cluster barrier, when every CTA has read it
-        __threadfence();
         cl.sync();
         if (threadIdx.x < k) {
             double t = 0.0;
@@ -333,7 +330,6 @@ struct ClusterRed {
             slot[pr][0] = b;
             slot[pr][1] = (double)ix;
         }
-        __threadfence();
         cl.sync();
         if (threadIdx.x == 0) {
             double b = -1.0;
