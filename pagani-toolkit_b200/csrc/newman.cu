@@ -36,8 +36,8 @@
 namespace cg = cooperative_groups;
 
 namespace {
-constexpr int THREADS = 256;
-constexpr int COOP_THREADS = 512;
+constexpr int GROUP_THREADS = 1024; // one-CTA and cluster power iterations
+constexpr int COOP_THREADS = 1024;
 constexpr int MAX_ITER = 10000;
 constexpr double EPSILON = 1e-6;
 constexpr double LAMBDA = 0.01;
@@ -477,7 +477,7 @@ __device__ void sub_partition(const Group& g, const Inputs& in, int gi, Red& red
 }
 
 // small groups: one CTA per group, everything in shared memory
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(GROUP_THREADS)
 k_nm_block(const int* __restrict__ glist, Inputs in)
 {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -509,7 +509,7 @@ k_nm_block(const int* __restrict__ glist, Inputs in)
 }
 
 // medium groups: one cluster per group, global memory
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(GROUP_THREADS)
 k_nm_cluster(const int* __restrict__ glist, Inputs in)
 {
     __shared__ ClusterRed red;
@@ -703,7 +703,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                                          ctx->stream));
         auto t0 = now();
         if (!small.empty()) {
-            k_nm_block<<<(int)small.size(), THREADS, smem_small, ctx->stream>>>(glist, in);
+            k_nm_block<<<(int)small.size(), GROUP_THREADS, smem_small, ctx->stream>>>(glist, in);
             PG_LAUNCHED(ctx);
             PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         }
@@ -717,7 +717,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
             attr[0].val.clusterDim.y = 1;
             attr[0].val.clusterDim.z = 1;
             cfg.gridDim = dim3((unsigned)(medium.size() * cluster));
-            cfg.blockDim = dim3(THREADS);
+            cfg.blockDim = dim3(GROUP_THREADS);
             cfg.stream = ctx->stream;
             cfg.attrs = attr;
             cfg.numAttrs = 1;
