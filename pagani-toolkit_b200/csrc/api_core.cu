@@ -76,6 +76,8 @@ extern "C" pg_status pg_destroy(pg_ctx* ctx)
     for (auto& kv : ctx->ws) cudaFree(kv.second.p);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (auto& e : ctx->ev) cudaEventDestroy(e);
+    for (auto& st : ctx->side)
+        if (st) cudaStreamDestroy(st);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return PG_OK;

@@ -36,20 +36,15 @@
 namespace cg = cooperative_groups;
 
 namespace {
-constexpr int GROUP_THREADS = 1024; // one-CTA and cluster power iterations
+constexpr int TEAM_THREADS = 512;   // team power iterations
 constexpr int COOP_THREADS = 1024;
 constexpr int MAX_ITER = 10000;
 constexpr double EPSILON = 1e-6;
 constexpr double LAMBDA = 0.01;
-constexpr size_t SMEM_CAP = 200 * 1024;        // shared-memory budget of the one-CTA path
-constexpr long long MEDIUM_EDGES = 1LL << 22;  // at most this many edges: one cluster per group
-constexpr int CLUSTER = 16;                    // CTAs per cluster for medium groups
-
-size_t small_bytes(long long n, long long e)
-{
-    // sR (n+1 ints), sC (e ints), kdeg, sumBG, v, v0 (n doubles each), 16-byte aligned parts
-    return ((size_t)(n + 1) * 4 + 15) / 16 * 16 + ((size_t)e * 4 + 15) / 16 * 16 + (size_t)n * 32;
-}
+constexpr size_t SMEM_CAP = 200 * 1024;        // dynamic shared memory of a team CTA
+constexpr long long MEDIUM_EDGES = 1LL << 22;  // at most this many edges: one team per group
+constexpr int CLUSTER = 16;                    // largest team (CTAs of one cluster)
+constexpr long long MIN_CTA_EDGES = 16384;     // a team CTA keeps at least this many edges
 
 // In-group degree of every member (label of neighbour == label of node).
 __global__ void k_nm_gdeg(const int32_t* __restrict__ R, const int32_t* __restrict__ C,
@@ -127,12 +122,72 @@ struct Group {
     int ng;
 };
 
+// Rows of y = B v for the rows this warp owns, L lanes per row.  Each lane
+// keeps four independent gathers in flight; the L partial sums meet in a
+// shuffle tree.  Returns this lane's share of |y|^2.
+template <int L>
+__device__ __forceinline__ double spmv_rows(const Group& g, double c, double beta, int lane, int wid, int nwarp)
+{
+    constexpr int RPW = 32 / L;
+    const int sub = lane & (L - 1);
+    double y2 = 0.0;
+    for (int base = wid * RPW; base < g.ng; base += nwarp * RPW) {
+        const int p = base + lane / L;
+        const bool act = p < g.ng;
+        int q = 0, q1 = 0;
+        if (act) {
+            q = g.sR[p] + sub;
+            q1 = g.sR[p + 1];
+        }
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (; q + 3 * L < q1; q += 4 * L) {
+            const int c0 = g.sC[q], c1 = g.sC[q + L], c2 = g.sC[q + 2 * L], c3 = g.sC[q + 3 * L];
+            s0 += g.v[c0];
+            s1 += g.v[c1];
+            s2 += g.v[c2];
+            s3 += g.v[c3];
+        }
+        for (; q < q1; q += L) s0 += g.v[g.sC[q]];
+        double s = (s0 + s1) + (s2 + s3);
+        for (int o = L / 2; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (act && sub == 0) {
+            s -= c * g.kdeg[p] + (g.sumBG[p] - beta) * g.v[p];
+            g.v0[p] = s;
+            y2 += s * s;
+        }
+    }
+    return y2;
+}
+
+// Lanes per row: about 8-16 edges per lane, widened while rows alone would
+// leave threads idle.  Every thread of a group computes the same value.
+__device__ __forceinline__ int lanes_per_row(int ng, long long edges, int nthr)
+{
+    const long long avg = ng > 0 ? edges / ng : 0;
+    int L = 1;
+    while (L < 32 && (long long)L * 16 <= avg) L <<= 1;
+    while (L < 32 && (long long)ng * L < nthr && 2LL * L <= avg) L <<= 1;
+    return L;
+}
+
+__device__ __forceinline__ double spmv(int L, const Group& g, double c, double beta, int lane, int wid, int nwarp)
+{
+    switch (L) {
+    case 1: return spmv_rows<1>(g, c, beta, lane, wid, nwarp);
+    case 2: return spmv_rows<2>(g, c, beta, lane, wid, nwarp);
+    case 4: return spmv_rows<4>(g, c, beta, lane, wid, nwarp);
+    case 8: return spmv_rows<8>(g, c, beta, lane, wid, nwarp);
+    case 16: return spmv_rows<16>(g, c, beta, lane, wid, nwarp);
+    default: return spmv_rows<32>(g, c, beta, lane, wid, nwarp);
+    }
+}
+
 // The reference's Lead_Vector (Modularity_CPU.cpp:224-298) with two
 // reductions per step; `Red` supplies barrier + sum over the threads that own
-// the group.
+// the group.  `ph` alternates the reduction buffers.
 template <class Red>
-__device__ double lead_vector(const Group& g, int M, double beta, int* iters, double* resid, Red& red, int tid,
-                              int nthr, int lane, int wid, int nwarp)
+__device__ double lead_vector(const Group& g, int M, double beta, double err_sq, int* iters, double* resid, Red& red,
+                              int tid, int nthr, int lane, int wid, int nwarp, int& ph)
 {
     double x[3];
     double vk = 0.0;
@@ -142,25 +197,16 @@ __device__ double lead_vector(const Group& g, int M, double beta, int* iters, do
         vk += vp * g.kdeg[p];
     }
     x[0] = vk;
-    red.sum(x, 1);
+    red.sum(x, 1, ph);
     vk = x[0];
-    double err1 = 1.0, err2 = 1.0, vnorm = 0.0;
+    const int L = lanes_per_row(g.ng, g.ng > 0 ? (long long)g.sR[g.ng] - g.sR[0] : 0, nthr);
+    // |v' - v|^2 and |v' + v|^2; sqrt(e) > EPSILON exactly when e > err_sq
+    double s1 = 1.0, s2 = 1.0, vnorm = 0.0;
     int iter = 0;
-    while (err1 > EPSILON && err2 > EPSILON && iter < MAX_ITER) {
-        const double c = vk / 2.0 / (double)M;
-        double y2 = 0.0;
-        for (int p = wid; p < g.ng; p += nwarp) {
-            double s = 0.0;
-            for (int32_t q = g.sR[p] + lane; q < g.sR[p + 1]; q += 32) s += g.v[g.sC[q]];
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) {
-                s -= c * g.kdeg[p] + (g.sumBG[p] - beta) * g.v[p];
-                g.v0[p] = s;
-                y2 += s * s;
-            }
-        }
-        x[0] = y2;
-        red.sum(x, 1);
+    while (s1 > err_sq && s2 > err_sq && iter < MAX_ITER) {
+        const double c = vk * 0.5 / (double)M;   // vk / 2 / M, the same double
+        x[0] = spmv(L, g, c, beta, lane, wid, nwarp);
+        red.sum(x, 1, ph);
         vnorm = sqrt(x[0]);
         double e1 = 0.0, e2 = 0.0;
         vk = 0.0;
@@ -177,32 +223,37 @@ __device__ double lead_vector(const Group& g, int M, double beta, int* iters, do
         x[0] = e1;
         x[1] = e2;
         x[2] = vk;
-        red.sum(x, 3);
-        err1 = sqrt(x[0]);
-        err2 = sqrt(x[1]);
+        red.sum(x, 3, ph);
+        s1 = x[0];
+        s2 = x[1];
         vk = x[2];
         iter++;
     }
     *iters = iter;
-    *resid = fmin(err1, err2);
+    *resid = fmin(sqrt(s1), sqrt(s2));
     // first entry of largest magnitude decides the sign (Modularity_CPU.cpp:291-296)
-    const int mx = red.argmax_abs(g.v, g.ng, tid, nthr);
+    const int mx = red.argmax_abs(g.v, g.ng, tid, nthr, ph);
     double lam = 0.0;
     if (g.ng > 0) lam = (g.v[mx] * g.v0[mx] > 0) ? vnorm : -vnorm;
     red.sync();
     return lam;
 }
 
-struct WarpSlots {
-    double warp[32][4];
-    double bcast[4];
-    int par;
-};
-
 __device__ __forceinline__ void warp_reduce(double* x, int k)
 {
     for (int q = 0; q < k; q++)
         for (int o = 16; o; o >>= 1) x[q] += __shfl_xor_sync(0xffffffffu, x[q], o);
+}
+
+// (value, index) maximum over the lanes, lowest index on ties; all lanes end
+// with the result
+__device__ __forceinline__ void warp_argmax(double& best, int& bi)
+{
+    for (int o = 16; o; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
 }
 
 // per-warp (|v|max, first index) over a strided range
@@ -214,211 +265,104 @@ __device__ __forceinline__ void local_argmax(const double* v, int n, int tid, in
         double m = fabs(v[p]);
         if (m > best) { best = m; bi = p; }
     }
-    for (int o = 16; o; o >>= 1) {
-        double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-    }
+    warp_argmax(best, bi);
 }
 
-// block-level (value, index) of the warp results, in warp order (thread 0)
-__device__ __forceinline__ void block_argmax(const WarpSlots& s, int nw, double& b, int& ix)
+// Per-warp partials of up to four sums, two buffers used alternately: a
+// buffer is written again only after another barrier that every warp reaches
+// once it has read the buffer.
+struct Partials {
+    double warp[2][32][4];
+};
+
+// Sums of K values over one CTA: every warp folds the warp partials itself in
+// the same fixed order, so all threads hold bit-identical sums after a single
+// block barrier.
+template <int K>
+__device__ __forceinline__ void block_sum(Partials& s, double (&x)[K], int& ph)
 {
-    b = -1.0;
-    ix = 0x7fffffff;
-    for (int ww = 0; ww < nw; ww++)
-        if (s.warp[ww][0] > b || (s.warp[ww][0] == b && (int)s.warp[ww][1] < ix)) {
-            b = s.warp[ww][0];
-            ix = (int)s.warp[ww][1];
-        }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    warp_reduce(x, K);
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < K; q++) s.warp[ph][w][q] = x[q];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; q++) x[q] = lane < nw ? s.warp[ph][lane][q] : 0.0;
+    warp_reduce(x, K);
+    ph ^= 1;
 }
 
-// ---- one CTA owns the group: block barriers only
-struct BlockRed {
-    WarpSlots s;
-    __device__ void sync() { __syncthreads(); }
-    __device__ void sum(double* x, int k)
-    {
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        warp_reduce(x, k);
-        if (lane == 0)
-            for (int q = 0; q < k; q++) s.warp[w][q] = x[q];
-        __syncthreads();
-        if (threadIdx.x < k) {
-            double t = 0.0;
-            for (int ww = 0; ww < nw; ww++) t += s.warp[ww][threadIdx.x];
-            s.bcast[threadIdx.x] = t;
-        }
-        __syncthreads();
-        for (int q = 0; q < k; q++) x[q] = s.bcast[q];
-        __syncthreads();
-    }
-    __device__ int argmax_abs(const double* v, int n, int tid, int nthr)
-    {
-        double best;
-        int bi;
-        local_argmax(v, n, tid, nthr, best, bi);
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        if (lane == 0) { s.warp[w][0] = best; s.warp[w][1] = (double)bi; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double b;
-            int ix;
-            block_argmax(s, nw, b, ix);
-            s.bcast[0] = (double)(ix == 0x7fffffff ? 0 : ix);
-        }
-        __syncthreads();
-        const int r = (int)s.bcast[0];
-        __syncthreads();
-        return r;
-    }
-};
-
-// ---- a thread-block cluster owns the group: DSMEM partials, cluster barrier
-struct ClusterRed {
-    WarpSlots s;
-    double slot[2][4];
-    __device__ void init()
-    {
-        if (threadIdx.x == 0) s.par = 0;
-        __syncthreads();
-    }
-    // cluster barriers release/acquire at cluster scope, which orders the
-    // global-memory vector writes of one CTA before the reads of another
-    __device__ void sync() { cg::this_cluster().sync(); }
-    __device__ void sum(double* x, int k)
-    {
-        cg::cluster_group cl = cg::this_cluster();
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        warp_reduce(x, k);
-        if (lane == 0)
-            for (int q = 0; q < k; q++) s.warp[w][q] = x[q];
-        __syncthreads();
-        const int pr = s.par;
-        if (threadIdx.x < k) {
-            double t = 0.0;
-            for (int ww = 0; ww < nw; ww++) t += s.warp[ww][threadIdx.x];
-            slot[pr][threadIdx.x] = t;
-        }
-        // the other slot half is written next; this one again only after
-        // another cluster barrier, when every CTA has read it
-        cl.sync();
-        if (threadIdx.x < k) {
-            double t = 0.0;
-            for (int r = 0; r < (int)cl.num_blocks(); r++) t += cl.map_shared_rank(this, r)->slot[pr][threadIdx.x];
-            s.bcast[threadIdx.x] = t;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) s.par = pr ^ 1;
-        for (int q = 0; q < k; q++) x[q] = s.bcast[q];
-        __syncthreads();
-    }
-    __device__ int argmax_abs(const double* v, int n, int tid, int nthr)
-    {
-        cg::cluster_group cl = cg::this_cluster();
-        double best;
-        int bi;
-        local_argmax(v, n, tid, nthr, best, bi);
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        if (lane == 0) { s.warp[w][0] = best; s.warp[w][1] = (double)bi; }
-        __syncthreads();
-        const int pr = s.par;
-        if (threadIdx.x == 0) {
-            double b;
-            int ix;
-            block_argmax(s, nw, b, ix);
-            slot[pr][0] = b;
-            slot[pr][1] = (double)ix;
-        }
-        cl.sync();
-        if (threadIdx.x == 0) {
-            double b = -1.0;
-            int ix = 0x7fffffff;
-            for (int r = 0; r < (int)cl.num_blocks(); r++) {
-                const ClusterRed* o = cl.map_shared_rank(this, r);
-                double ob = o->slot[pr][0];
-                int oi = (int)o->slot[pr][1];
-                if (ob > b || (ob == b && oi < ix)) { b = ob; ix = oi; }
-            }
-            s.bcast[0] = (double)(ix == 0x7fffffff ? 0 : ix);
-            s.par = pr ^ 1;
-        }
-        __syncthreads();
-        const int r = (int)s.bcast[0];
-        __syncthreads();
-        return r;
-    }
-};
-
-// ---- the whole cooperative grid owns the group
+// ---- the whole cooperative grid owns the group: one value per block in
+// global memory, a grid barrier, then warp 0 of every block folds the block
+// values in the same order and broadcasts through shared memory.
 struct GridRed {
-    WarpSlots s;
-    double* part;   // [2][gridDim.x][4], alternate halves per reduction
+    Partials s;
+    double bc[2][4];
+    double* part;   // [2][gridDim.x][4]
     __device__ void init(double* p)
     {
-        if (threadIdx.x == 0) { part = p; s.par = 0; }
+        if (threadIdx.x == 0) part = p;
         __syncthreads();
     }
     __device__ void sync() { cg::this_grid().sync(); }
-    __device__ void sum(double* x, int k)
+    __device__ void sum(double* x, int k, int& ph)
     {
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
         warp_reduce(x, k);
         if (lane == 0)
-            for (int q = 0; q < k; q++) s.warp[w][q] = x[q];
+            for (int q = 0; q < k; q++) s.warp[ph][w][q] = x[q];
         __syncthreads();
-        const int pr = s.par;
-        double* pp = part + (size_t)pr * gridDim.x * 4;
-        if (threadIdx.x < k) {
-            double t = 0.0;
-            for (int ww = 0; ww < nw; ww++) t += s.warp[ww][threadIdx.x];
-            pp[blockIdx.x * 4 + threadIdx.x] = t;
+        double* pp = part + (size_t)ph * gridDim.x * 4;
+        if (w == 0) {
+            for (int q = 0; q < k; q++) x[q] = lane < nw ? s.warp[ph][lane][q] : 0.0;
+            warp_reduce(x, k);
+            if (lane < k) pp[blockIdx.x * 4 + lane] = lane == 0 ? x[0] : lane == 1 ? x[1] : x[2];
         }
-        // one grid barrier per reduction: the other half of `part` is written
-        // next, and this half again only after another barrier
+        // the other half of `part` is written next, and this one again only
+        // after another grid barrier
         cg::this_grid().sync();
-        if (threadIdx.x < k) {
-            double t = 0.0;
-            for (int b = 0; b < (int)gridDim.x; b++) t += pp[b * 4 + threadIdx.x];
-            s.bcast[threadIdx.x] = t;
+        if (w == 0) {
+            for (int q = 0; q < k; q++) x[q] = 0.0;
+            for (int b = lane; b < (int)gridDim.x; b += 32)
+                for (int q = 0; q < k; q++) x[q] += pp[b * 4 + q];
+            warp_reduce(x, k);
+            if (lane < k) bc[ph][lane] = lane == 0 ? x[0] : lane == 1 ? x[1] : x[2];
         }
         __syncthreads();
-        if (threadIdx.x == 0) s.par = pr ^ 1;
-        for (int q = 0; q < k; q++) x[q] = s.bcast[q];
-        __syncthreads();
+        for (int q = 0; q < k; q++) x[q] = bc[ph][q];
+        ph ^= 1;
     }
-    __device__ int argmax_abs(const double* v, int n, int tid, int nthr)
+    __device__ int argmax_abs(const double* v, int n, int tid, int nthr, int& ph)
     {
         double best;
         int bi;
         local_argmax(v, n, tid, nthr, best, bi);
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        if (lane == 0) { s.warp[w][0] = best; s.warp[w][1] = (double)bi; }
+        if (lane == 0) { s.warp[ph][w][0] = best; s.warp[ph][w][1] = (double)bi; }
         __syncthreads();
-        const int pr = s.par;
-        double* pp = part + (size_t)pr * gridDim.x * 4;
-        if (threadIdx.x == 0) {
-            double b;
-            int ix;
-            block_argmax(s, nw, b, ix);
-            pp[blockIdx.x * 4 + 0] = b;
-            pp[blockIdx.x * 4 + 1] = (double)ix;
+        double* pp = part + (size_t)ph * gridDim.x * 4;
+        if (w == 0) {
+            best = lane < nw ? s.warp[ph][lane][0] : -1.0;
+            bi = lane < nw ? (int)s.warp[ph][lane][1] : 0x7fffffff;
+            warp_argmax(best, bi);
+            if (lane == 0) { pp[blockIdx.x * 4 + 0] = best; pp[blockIdx.x * 4 + 1] = (double)bi; }
         }
         cg::this_grid().sync();
-        if (threadIdx.x == 0) {
-            double b = -1.0;
-            int ix = 0x7fffffff;
-            for (int r = 0; r < (int)gridDim.x; r++) {
-                double ob = pp[r * 4 + 0];
-                int oi = (int)pp[r * 4 + 1];
-                if (ob > b || (ob == b && oi < ix)) { b = ob; ix = oi; }
+        if (w == 0) {
+            best = -1.0;
+            bi = 0x7fffffff;
+            for (int b = lane; b < (int)gridDim.x; b += 32) {
+                const double ob = pp[b * 4 + 0];
+                const int oi = (int)pp[b * 4 + 1];
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
             }
-            s.bcast[0] = (double)(ix == 0x7fffffff ? 0 : ix);
-            s.par = pr ^ 1;
+            warp_argmax(best, bi);
+            if (lane == 0) bc[ph][0] = (double)(bi == 0x7fffffff ? 0 : bi);
         }
         __syncthreads();
-        const int r = (int)s.bcast[0];
-        __syncthreads();
+        const int r = (int)bc[ph][0];
+        ph ^= 1;
         return r;
     }
 };
@@ -435,6 +379,7 @@ struct Inputs {
     double* v0;
     int M;
     int gpu_rule_above;
+    double err_sq;           // largest double whose square root is at most EPSILON
     double* out;             // per group: lambda, it0, res0, it1, res1, subP, subN, shifted
 };
 
@@ -458,70 +403,442 @@ template <class Red>
 __device__ void sub_partition(const Group& g, const Inputs& in, int gi, Red& red, int tid, int nthr, int lane,
                               int wid, int nwarp, bool writer)
 {
-    int it0, it1 = 0;
+    int it0, it1 = 0, ph = 0;
     double r0, r1 = 0.0;
-    double lam = lead_vector(g, in.M, 0.0, &it0, &r0, red, tid, nthr, lane, wid, nwarp);
+    double lam = lead_vector(g, in.M, 0.0, in.err_sq, &it0, &r0, red, tid, nthr, lane, wid, nwarp, ph);
     const double below = g.ng > in.gpu_rule_above ? -LAMBDA : 0.0;
     const bool shifted = lam < below;
-    if (shifted) lam += lead_vector(g, in.M, -lam, &it1, &r1, red, tid, nthr, lane, wid, nwarp);
+    if (shifted) lam += lead_vector(g, in.M, -lam, in.err_sq, &it1, &r1, red, tid, nthr, lane, wid, nwarp, ph);
     double x[3] = {0.0, 0.0, 0.0};
     for (int p = tid; p < g.ng; p += nthr) {
         x[0] += g.v[p] > 0.0;
         x[1] += g.v[p] <= 0.0;
     }
-    red.sum(x, 2);
+    red.sum(x, 2, ph);
     if (writer) {
         double* o = in.out + (size_t)gi * 8;
         o[0] = lam; o[1] = it0; o[2] = r0; o[3] = it1; o[4] = r1; o[5] = x[0]; o[6] = x[1]; o[7] = shifted;
     }
 }
 
-// small groups: one CTA per group, everything in shared memory
-__global__ void __launch_bounds__(GROUP_THREADS)
-k_nm_block(const int* __restrict__ glist, Inputs in)
+// ---------------------------------------------------------------- teams
+// A team is one CTA, or a thread-block cluster of up to 16 CTAs, that owns
+// one group.  Every CTA keeps the whole vector of the group in shared memory
+// (plus a zero sentinel at index n) and computes y = B v for an
+// edge-balanced range of own rows.  A cluster CTA publishes its rows of y in
+// global memory (two buffers used alternately) and, after one cluster barrier
+// per step, reads all of y back; then every CTA normalises the whole vector
+// and forms |y|, |v' -+ v| and v'.k itself, over all rows in one fixed order.
+// All CTAs of a team therefore hold bit-identical vectors and sums and take
+// the same decisions, with no reduction across CTAs.
+//
+// The own rows are stored as a sorted sliced ELL matrix in shared memory:
+// rows sorted by length (longest first), slices of 32 / L rows with L lanes
+// per row, and per slice the 16-bit columns interleaved so that one warp-wide
+// load reads element j of every lane; short rows are padded with the
+// sentinel column.  A gather of the vector then costs the bank-conflict time
+// of one warp-wide shared-memory access per 32 edges, which bounds a step; L
+// is chosen per CTA from the sorted lengths.  When the slices do not fit, the
+// CTA reads its rows' CSR from global memory instead.
+
+struct SoloTeam {       // one CTA: y stays in shared memory
+    static constexpr bool kCluster = false;
+    __device__ static void barrier() { __syncthreads(); }
+};
+struct ClusterTeam {    // a cluster: rows of y meet in global memory
+    static constexpr bool kCluster = true;
+    // release/acquire at cluster scope orders the global y stores of every
+    // CTA before the loads of every other CTA
+    __device__ static void barrier() { cg::this_cluster().sync(); }
+};
+
+constexpr int TEAM_MAX_ROWS = 12288;   // rows of a team group (its vector fits shared memory)
+
+// First local row whose edge offset reaches rank * E / nb.
+__host__ __device__ inline int team_split(const int32_t* R, int n, int rank, int nb)
 {
-    extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ BlockRed red;
-    const int gi = glist[blockIdx.x];
-    const Group gg = global_group(in, gi);
-    const int n = gg.ng;
-    const long long ne = in.eoff[gi + 1] - in.eoff[gi];
-    int32_t* sR = (int32_t*)sm;
-    int32_t* sC = (int32_t*)(sm + ((size_t)(n + 1) * 4 + 15) / 16 * 16);
-    double* dv = (double*)((unsigned char*)sC + ((size_t)ne * 4 + 15) / 16 * 16);
-    for (int p = threadIdx.x; p <= n; p += blockDim.x) sR[p] = gg.sR[p];
-    for (int p = threadIdx.x; p < n; p += blockDim.x) {
-        dv[p] = gg.kdeg[p];
-        dv[n + p] = gg.sumBG[p];
+    if (rank <= 0) return 0;
+    if (rank >= nb) return n;
+    const long long target = (long long)R[n] * rank / nb;
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (R[mid] >= target) hi = mid;
+        else lo = mid + 1;
     }
-    for (long long q = threadIdx.x; q < ne; q += blockDim.x) sC[q] = gg.sC[q];
-    __syncthreads();
-    Group g = gg;
-    g.sR = sR;
-    g.sC = sC;
-    g.kdeg = dv;
-    g.sumBG = dv + n;
-    g.v = dv + 2 * n;
-    g.v0 = dv + 3 * n;
-    sub_partition(g, in, gi, red, threadIdx.x, blockDim.x, threadIdx.x & 31, threadIdx.x >> 5, blockDim.x >> 5,
-                  threadIdx.x == 0);
-    for (int p = threadIdx.x; p < n; p += blockDim.x) gg.v[p] = g.v[p];   // the labels are assigned from v
+    return lo;
 }
 
-// medium groups: one cluster per group, global memory
-__global__ void __launch_bounds__(GROUP_THREADS)
-k_nm_cluster(const int* __restrict__ glist, Inputs in)
+__host__ __device__ inline int pow2_at_least(int x)
 {
-    __shared__ ClusterRed red;
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// Byte offsets of the shared-memory parts of one team CTA; the slices take
+// what is left.
+struct TeamLayout {
+    size_t rep, kd, oy, oprev, obg, oR, key, soff, cols, need_min;
+};
+
+__host__ __device__ inline size_t team_take(size_t& at, size_t bytes)
+{
+    const size_t o = at;
+    at += (bytes + 15) / 16 * 16;
+    return o;
+}
+
+__host__ __device__ inline TeamLayout team_layout(int n, int nown)
+{
+    TeamLayout t;
+    size_t at = 0;
+    t.rep = team_take(at, (size_t)(n + 1) * 8);
+    t.kd = team_take(at, (size_t)n * 4);                       // degrees, exact as float
+    t.oy = team_take(at, (size_t)nown * 8);
+    t.oprev = team_take(at, (size_t)nown * 8);
+    t.obg = team_take(at, (size_t)nown * 8);
+    t.oR = team_take(at, (size_t)(nown + 1) * 4);
+    t.key = team_take(at, (size_t)pow2_at_least(nown) * 4);   // sort keys, then the row order
+    t.soff = team_take(at, (size_t)(nown + 1) * 4);            // slice offsets (entries)
+    t.cols = at;
+    t.need_min = at;
+    return t;
+}
+
+struct Team {
+    double* rep;          // the group's vector, n entries and a zero at n
+    const float* kd;      // degree of every row
+    double* oy;           // own rows: y (one-CTA teams)
+    double* oprev;        // own rows: vector entering the step
+    double* obg;          // own rows: sumBG
+    int32_t* oR;          // own rows: offsets into the own edge range
+    const uint32_t* perm; // sliced rows: own row of each slot (sorted)
+    const int32_t* soff;  // slice s: entries [soff[s], soff[s+1]) of cols
+    const uint16_t* cols; // sliced columns
+    const int32_t* gcols; // own edges in global memory (unsliced CTAs)
+    int L;                // lanes per row
+    int nslices;          // 0: unsliced
+    int n, r0, nown;
+};
+
+// own rows of y = B v from the sliced matrix, written to ydst[own row]
+template <int L>
+__device__ __forceinline__ void team_slices(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
+                                            int nwarp)
+{
+    constexpr int RPS = 32 / L;
+    const double* __restrict__ rep = tm.rep;
+    const int sub = lane & (L - 1);
+    for (int s = wid; s < tm.nslices; s += nwarp) {
+        const int b = tm.soff[s], it = (tm.soff[s + 1] - b) >> 5;
+        const uint16_t* __restrict__ cs = tm.cols + b + lane;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int j = 0;
+        for (; j + 3 < it; j += 4) {
+            const int c0 = cs[32 * j], c1 = cs[32 * j + 32], c2 = cs[32 * j + 64], c3 = cs[32 * j + 96];
+            a0 += rep[c0];
+            a1 += rep[c1];
+            a2 += rep[c2];
+            a3 += rep[c3];
+        }
+        for (; j < it; j++) a0 += rep[cs[32 * j]];
+        double y = (a0 + a1) + (a2 + a3);
+        for (int o = L / 2; o; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        const int slot = s * RPS + lane / L;
+        if (sub == 0 && slot < tm.nown) {
+            const int lp = (int)tm.perm[slot], p = tm.r0 + lp;
+            ydst[lp] = y - (c * (double)tm.kd[p] + (tm.obg[lp] - beta) * rep[p]);
+        }
+    }
+}
+
+// own rows of y = B v from the CSR in global memory, L lanes per row
+template <int L>
+__device__ __forceinline__ void team_rows(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
+                                          int nwarp)
+{
+    constexpr int RPW = 32 / L;
+    const double* __restrict__ rep = tm.rep;
+    const int32_t* __restrict__ cols = tm.gcols;
+    const int sub = lane & (L - 1);
+    for (int base = wid * RPW; base < tm.nown; base += nwarp * RPW) {
+        const int lp = base + lane / L;
+        const bool act = lp < tm.nown;
+        int q = 0, q1 = 0;
+        if (act) {
+            q = tm.oR[lp] + sub;
+            q1 = tm.oR[lp + 1];
+        }
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (; q + 3 * L < q1; q += 4 * L) {
+            const int c0 = cols[q], c1 = cols[q + L], c2 = cols[q + 2 * L], c3 = cols[q + 3 * L];
+            s0 += rep[c0];
+            s1 += rep[c1];
+            s2 += rep[c2];
+            s3 += rep[c3];
+        }
+        for (; q < q1; q += L) s0 += rep[cols[q]];
+        double y = (s0 + s1) + (s2 + s3);
+        for (int o = L / 2; o; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        if (act && sub == 0) {
+            const int p = tm.r0 + lp;
+            ydst[lp] = y - (c * (double)tm.kd[p] + (tm.obg[lp] - beta) * rep[p]);
+        }
+    }
+}
+
+__device__ __forceinline__ void team_spmv(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
+                                          int nwarp)
+{
+    if (tm.nslices > 0) {
+        switch (tm.L) {
+        case 1: team_slices<1>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 2: team_slices<2>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 4: team_slices<4>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 8: team_slices<8>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 16: team_slices<16>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        default: team_slices<32>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        }
+    }
+    switch (tm.L) {
+    case 1: team_rows<1>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 2: team_rows<2>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 4: team_rows<4>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 8: team_rows<8>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 16: team_rows<16>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    default: team_rows<32>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    }
+}
+
+// first index of the largest |v| over the whole copy, computed by one CTA
+__device__ __forceinline__ int block_argmax_abs(Partials& s, const double* v, int n, int& ph)
+{
+    double best;
+    int bi;
+    local_argmax(v, n, threadIdx.x, blockDim.x, best, bi);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) { s.warp[ph][w][0] = best; s.warp[ph][w][1] = (double)bi; }
+    __syncthreads();
+    best = lane < nw ? s.warp[ph][lane][0] : -1.0;
+    bi = lane < nw ? (int)s.warp[ph][lane][1] : 0x7fffffff;
+    warp_argmax(best, bi);
+    ph ^= 1;
+    return bi == 0x7fffffff ? 0 : bi;
+}
+
+// Lead_Vector (Modularity_CPU.cpp:224-298) for a team: the reference's
+// per-entry arithmetic, sums in a fixed order over all rows.
+template <class Kind>
+__device__ double team_lead_vector(const Team& tm, const Group& gg, int M, double beta, double err_sq, int* iters,
+                                   double* resid, Partials& ps, int& ph)
+{
+    const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, wid = tid >> 5, nwarp = nthr >> 5;
+    const int n = tm.n;
+    double x1[1] = {0.0};
+    for (int p = tid; p < n; p += nthr) {
+        const double vp = (double)gg.AD[p];
+        tm.rep[p] = vp;
+        x1[0] += vp * (double)tm.kd[p];
+    }
+    block_sum(ps, x1, ph);
+    double vk = x1[0];
+    // |v' - v|^2 and |v' + v|^2; sqrt(e) > EPSILON exactly when e > err_sq
+    double s1 = 1.0, s2 = 1.0, vnorm = 0.0;
+    int iter = 0, yb = 0;
+    while (s1 > err_sq && s2 > err_sq && iter < MAX_ITER) {
+        const double c = vk * 0.5 / (double)M;   // vk / 2 / M, the same double
+        double* ybuf = Kind::kCluster ? (yb ? gg.v0 : gg.v) : tm.oy;
+        team_spmv(tm, Kind::kCluster ? ybuf + tm.r0 : ybuf, c, beta, lane, wid, nwarp);
+        Kind::barrier();
+        x1[0] = 0.0;
+        for (int p = tid; p < n; p += nthr) {
+            const double y = ybuf[p];
+            x1[0] += y * y;
+        }
+        block_sum(ps, x1, ph);
+        vnorm = sqrt(x1[0]);
+        double x3[3] = {0.0, 0.0, 0.0};
+        for (int p = tid; p < n; p += nthr) {
+            const double vold = tm.rep[p];
+            const double vp = ybuf[p] / vnorm;
+            const double d1 = vp - vold, d2 = vp + vold;
+            x3[0] += d1 * d1;
+            x3[1] += d2 * d2;
+            x3[2] += vp * (double)tm.kd[p];
+            if ((unsigned)(p - tm.r0) < (unsigned)tm.nown) tm.oprev[p - tm.r0] = vold;
+            tm.rep[p] = vp;
+        }
+        block_sum(ps, x3, ph);
+        s1 = x3[0];
+        s2 = x3[1];
+        vk = x3[2];
+        yb ^= 1;
+        iter++;
+    }
+    *iters = iter;
+    *resid = fmin(sqrt(s1), sqrt(s2));
+    // the labels are assigned from v; the sign test below reads v0 of any row
+    Kind::barrier();   // the y buffers are free again
+    for (int lp = tid; lp < tm.nown; lp += nthr) {
+        gg.v[tm.r0 + lp] = tm.rep[tm.r0 + lp];
+        gg.v0[tm.r0 + lp] = tm.oprev[lp];
+    }
+    Kind::barrier();
+    // first entry of largest magnitude decides the sign (Modularity_CPU.cpp:291-296)
+    const int mx = block_argmax_abs(ps, tm.rep, n, ph);
+    const double lam = (tm.rep[mx] * gg.v0[mx] > 0) ? vnorm : -vnorm;
+    Kind::barrier();   // every read of the copy and of v0 is done before they change
+    return lam;
+}
+
+// Sliced layout of the own rows: sort, choose L, fill.  Returns the number of
+// slices, 0 when they do not fit in `space` bytes.
+__device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int32_t* soff, uint16_t* cols,
+                          size_t space, int* sL)
+{
+    const int tid = threadIdx.x, nthr = blockDim.x, nown = tm.nown;
+    const int P2 = pow2_at_least(nown);
+    // keys: (65535 - length) << 16 | row, so ascending order is longest
+    // first with rows in order on ties
+    for (int i = tid; i < P2; i += nthr) {
+        uint32_t k = 0xffffffffu;
+        if (i < nown) {
+            const int len = min(tm.oR[i + 1] - tm.oR[i], 65535);
+            k = ((uint32_t)(65535 - len) << 16) | (uint32_t)i;
+        }
+        key[i] = k;
+    }
+    __syncthreads();
+    for (int k = 2; k <= P2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < P2; i += nthr) {
+                const int o = i ^ j;
+                if (o > i) {
+                    const uint32_t a = key[i], b = key[o];
+                    if ((a > b) == ((i & k) == 0)) {
+                        key[i] = b;
+                        key[o] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = tid; i < nown; i += nthr) key[i] &= 0xffffu;   // now the row order
+    __syncthreads();
+    // cost of lanes-per-row L = 2^t: warp 0 takes the first slice of every
+    // round, the longest, so its total bounds the step
+    __shared__ long long cost[6], size[6];
+    if (tid < 6) {
+        const int L = 1 << tid, RPS = 32 / L, ns = (nown + RPS - 1) / RPS, nw = nthr >> 5;
+        long long c = 0, sz = 0;
+        for (int s = 0; s < ns; s++) {
+            const int first = (int)key[s * RPS];
+            const int it = (tm.oR[first + 1] - tm.oR[first] + L - 1) / L;
+            sz += 32LL * it;
+            if (s % nw == 0) c += it + 3 + tid;
+        }
+        cost[tid] = c;
+        size[tid] = sz;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int best = -1;
+        for (int t = 0; t < 6; t++)
+            if ((size_t)size[t] * 2 <= space && (best < 0 || cost[t] < cost[best])) best = t;
+        *sL = best < 0 ? 0 : 1 << best;
+        if (best >= 0) {
+            const int L = 1 << best, RPS = 32 / L, ns = (nown + RPS - 1) / RPS;
+            int at = 0;
+            for (int s = 0; s < ns; s++) {
+                soff[s] = at;
+                const int first = (int)key[s * RPS];
+                at += 32 * ((tm.oR[first + 1] - tm.oR[first] + L - 1) / L);
+            }
+            soff[ns] = at;
+        }
+    }
+    __syncthreads();
+    const int L = *sL;
+    if (L == 0) return 0;
+    const int RPS = 32 / L, ns = (nown + RPS - 1) / RPS;
+    const int lane = tid & 31, sub = lane & (L - 1);
+    for (int s = tid >> 5; s < ns; s += nthr >> 5) {
+        const int slot = s * RPS + lane / L;
+        int q0 = 0, len = 0;
+        if (slot < nown) {
+            const int r = (int)key[slot];
+            q0 = tm.oR[r];
+            len = tm.oR[r + 1] - q0;
+        }
+        const int it = (soff[s + 1] - soff[s]) >> 5;
+        for (int j = 0; j < it; j++) {
+            const int k = j * L + sub;
+            cols[soff[s] + 32 * j + lane] = (uint16_t)(k < len ? gg.sC[e0 + q0 + k] : tm.n);
+        }
+    }
+    __syncthreads();
+    return ns;
+}
+
+// One team per group of `glist`; the cluster size is set at launch.
+template <class Kind>
+__global__ void __launch_bounds__(TEAM_THREADS)
+k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ Partials ps;
+    __shared__ int sL;
     cg::cluster_group cl = cg::this_cluster();
-    red.init();
-    cl.sync();
-    const int gi = glist[blockIdx.x / cl.num_blocks()];
-    Group g = global_group(in, gi);
-    const int ct = (int)cl.block_rank() * blockDim.x + threadIdx.x, cth = (int)cl.num_blocks() * blockDim.x;
-    sub_partition(g, in, gi, red, ct, cth, threadIdx.x & 31, ct >> 5, cth >> 5, ct == 0);
-    // no CTA may exit while another still reads its shared memory
-    cl.sync();
+    const int nb = Kind::kCluster ? (int)cl.num_blocks() : 1, rank = Kind::kCluster ? (int)cl.block_rank() : 0;
+    const int gi = glist[blockIdx.x / nb];
+    const Group gg = global_group(in, gi);
+    Team tm;
+    tm.n = gg.ng;
+    tm.r0 = team_split(gg.sR, tm.n, rank, nb);
+    const int r1 = team_split(gg.sR, tm.n, rank + 1, nb);
+    tm.nown = r1 - tm.r0;
+    const int e0 = gg.sR[tm.r0];
+    const TeamLayout t = team_layout(tm.n, tm.nown);
+    tm.rep = (double*)(sm + t.rep);
+    float* kd = (float*)(sm + t.kd);
+    tm.kd = kd;
+    tm.oy = (double*)(sm + t.oy);
+    tm.oprev = (double*)(sm + t.oprev);
+    tm.obg = (double*)(sm + t.obg);
+    tm.oR = (int32_t*)(sm + t.oR);
+    for (int p = threadIdx.x; p < tm.n; p += blockDim.x) kd[p] = (float)gg.kdeg[p];
+    for (int lp = threadIdx.x; lp < tm.nown; lp += blockDim.x) tm.obg[lp] = gg.sumBG[tm.r0 + lp];
+    for (int lp = threadIdx.x; lp <= tm.nown; lp += blockDim.x) tm.oR[lp] = gg.sR[tm.r0 + lp] - e0;
+    if (threadIdx.x == 0) tm.rep[tm.n] = 0.0;   // the padding column
+    __syncthreads();
+    uint32_t* key = (uint32_t*)(sm + t.key);
+    int32_t* soff = (int32_t*)(sm + t.soff);
+    uint16_t* cols = (uint16_t*)(sm + t.cols);
+    const size_t space = (size_t)smem_bytes > t.cols ? (size_t)smem_bytes - t.cols : 0;
+    tm.nslices = tm.n < 65535 ? team_slice(tm, gg, e0, key, soff, cols, space, &sL) : 0;
+    tm.perm = key;
+    tm.soff = soff;
+    tm.cols = cols;
+    tm.gcols = gg.sC + e0;
+    tm.L = tm.nslices > 0 ? sL : lanes_per_row(tm.nown, tm.nown > 0 ? (long long)tm.oR[tm.nown] : 0, blockDim.x);
+    // both passes of Sub_Partition
+    int it0, it1 = 0, ph = 0;
+    double res0, res1 = 0.0;
+    double lam = team_lead_vector<Kind>(tm, gg, in.M, 0.0, in.err_sq, &it0, &res0, ps, ph);
+    const double below = gg.ng > in.gpu_rule_above ? -LAMBDA : 0.0;
+    const bool shifted = lam < below;
+    if (shifted) lam += team_lead_vector<Kind>(tm, gg, in.M, -lam, in.err_sq, &it1, &res1, ps, ph);
+    double x2[2] = {0.0, 0.0};
+    for (int p = threadIdx.x; p < tm.n; p += blockDim.x) {
+        x2[0] += tm.rep[p] > 0.0;
+        x2[1] += tm.rep[p] <= 0.0;
+    }
+    block_sum(ps, x2, ph);
+    if (rank == 0 && threadIdx.x == 0) {
+        double* o = in.out + (size_t)gi * 8;
+        o[0] = lam; o[1] = it0; o[2] = res0; o[3] = it1; o[4] = res1; o[5] = x2[0]; o[6] = x2[1]; o[7] = shifted;
+    }
 }
 
 // large groups: the whole cooperative grid, one group per launch
@@ -599,25 +916,35 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "power iteration kernel cannot be resident");
     const int coop_grid = ctx->sm_count;   // one fat block per SM keeps the grid barrier short
     PG_TRY(pg_wst(ctx, "nm.part", (size_t)coop_grid * 8 + 8, &part));
-    int cluster = CLUSTER;  // 16 needs the non-portable opt-in
-    if (cudaFuncSetAttribute(k_nm_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    int max_cluster = CLUSTER;  // 16 needs the non-portable opt-in
+    if (cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+        cudaSuccess) {
         cudaGetLastError();
-        cluster = 8;
+        max_cluster = 8;
     }
+    for (auto& st : ctx->side)
+        if (!st) PG_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     const size_t smem_cap = std::min(SMEM_CAP, (size_t)ctx->smem_optin - 8192);
-    PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_team<SoloTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    PG_CUDA(ctx,
+            cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     PG_CUDA(ctx, cudaMemsetAsync(label, 0, sizeof(int32_t) * (n + 1), ctx->stream));
 
     std::vector<int32_t> hR(n + 1), hl(n);
     PG_TRY(pg_d2h(ctx, hR.data(), g->R, sizeof(int32_t) * (n + 1)));
     const int grid = ctx->sm_count * 4;
+    // the largest double whose correctly rounded square root is at most
+    // EPSILON: the loop test sqrt(e) > EPSILON is e > err_sq
+    double err_sq = EPSILON * EPSILON;
+    while (std::sqrt(err_sq) > EPSILON) err_sq = std::nextafter(err_sq, 0.0);
+    while (std::sqrt(std::nextafter(err_sq, 1.0)) <= EPSILON) err_sq = std::nextafter(err_sq, 1.0);
     std::vector<int32_t> adjust((size_t)n + 2, 0);
     int Round = 0, Max_Result = 0, Module_Num = 1, Index = 1;
     char line[512];
     std::vector<int32_t> hAD(n), hgidx(n), hpos(n, 0);
     // wall time per kind of power-iteration launch, reported in the log
-    double t_small = 0, t_medium = 0, t_large = 0, t_setup = 0;
-    long long it_small = 0, it_medium = 0, it_large = 0;
+    double t_small = 0, t_large = 0, t_setup = 0;
+    long long it_small = 0, it_large = 0;
     int generations = 0;
     auto now = [] { return std::chrono::steady_clock::now(); };
     auto ms_since = [&](std::chrono::steady_clock::time_point t0) {
@@ -678,55 +1005,113 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         // ---- power iterations, groups by size
         Inputs in;
         in.goff = goff; in.eoff = eoff; in.AD = AD; in.sR = sR; in.sC = sC; in.kdeg = kdeg; in.sumBG = sumBG;
-        in.v = v; in.v0 = v0; in.M = M; in.gpu_rule_above = gpu_rule_above; in.out = out;
-        std::vector<int> small, medium, large;
-        size_t smem_small = 16;
+        in.v = v; in.v0 = v0; in.M = M; in.gpu_rule_above = gpu_rule_above; in.out = out; in.err_sq = err_sq;
+        // Shared memory of the largest CTA of group q split over c CTAs,
+        // before its sliced columns
+        auto team_need = [&](int q, int c) {
+            const int ng = (int)(hgoff[q + 1] - hgoff[q]);
+            std::vector<int32_t> rel(ng + 1);
+            for (int p = 0; p <= ng; p++) rel[p] = (int32_t)(hsoff[hgoff[q] + p] - heoff[q]);
+            size_t need = 0;
+            for (int r = 0; r < c; r++) {
+                const int a = team_split(rel.data(), ng, r, c), b = team_split(rel.data(), ng, r + 1, c);
+                need = std::max(need, team_layout(ng, b - a).need_min);
+            }
+            return need;
+        };
+        // groups by size: teams (one cluster of 1-16 CTAs each), the rest on
+        // the whole grid
+        std::vector<int> team, large;
+        std::vector<int> csz;
         for (int q = 0; q < G; q++) {
             const long long ng = hgoff[q + 1] - hgoff[q];
             if (ng == 0) continue;
             const long long edges = heoff[q + 1] - heoff[q];
-            const size_t b = small_bytes(ng, edges);
-            if (b <= smem_cap) {
-                small.push_back(q);
-                smem_small = std::max(smem_small, b);
-            } else if (edges <= MEDIUM_EDGES && cluster > 1) {
-                medium.push_back(q);
+            int c = 0;
+            if (edges <= MEDIUM_EDGES && ng <= TEAM_MAX_ROWS)
+                for (int cc = 1; cc <= max_cluster && !c; cc *= 2)
+                    if (team_need(q, cc) <= smem_cap) c = cc;
+            if (c) {
+                team.push_back(q);
+                csz.push_back(c);
             } else {
                 large.push_back(q);
             }
         }
+        // SMs: double the team with the most edges per CTA while SMs are
+        // left and each CTA keeps at least MIN_CTA_EDGES edges
+        {
+            int used = 0;
+            for (int c : csz) used += c;
+            const int budget = std::max(ctx->sm_count, used);
+            for (;;) {
+                int best = -1;
+                double best_load = 0.0;
+                for (size_t j = 0; j < team.size(); j++) {
+                    const long long e = heoff[team[j] + 1] - heoff[team[j]];
+                    const double load = (double)e / csz[j];
+                    if (csz[j] * 2 <= max_cluster && load >= 2.0 * MIN_CTA_EDGES && load > best_load) {
+                        best = (int)j;
+                        best_load = load;
+                    }
+                }
+                if (best < 0 || used + csz[best] > budget) break;
+                used += csz[best];
+                csz[best] *= 2;
+            }
+        }
+        // glist by cluster size, largest first; one launch per size
+        std::vector<int> lists;
+        struct Bucket { int c; size_t b, e; size_t smem; };
+        std::vector<Bucket> buckets;
+        for (int c = max_cluster; c >= 1; c >>= 1) {
+            // every CTA gets the whole budget; what its rows leave holds the slices
+            Bucket bk{c, lists.size(), 0, smem_cap};
+            for (size_t j = 0; j < team.size(); j++)
+                if (csz[j] == c) lists.push_back(team[j]);
+            bk.e = lists.size();
+            if (bk.e > bk.b) buckets.push_back(bk);
+        }
         std::vector<double> hout((size_t)G * 8, 0.0);
-        std::vector<int> lists(small);
-        lists.insert(lists.end(), medium.begin(), medium.end());
         if (!lists.empty())
             PG_CUDA(ctx, cudaMemcpyAsync(glist, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice,
                                          ctx->stream));
         auto t0 = now();
-        if (!small.empty()) {
-            k_nm_block<<<(int)small.size(), GROUP_THREADS, smem_small, ctx->stream>>>(glist, in);
-            PG_LAUNCHED(ctx);
+        if (!buckets.empty()) {
+            // the launches of a generation run beside each other, one stream each
+            PG_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+            int si = 0;
+            for (const Bucket& bk : buckets) {
+                cudaStream_t st = ctx->side[si++];
+                PG_CUDA(ctx, cudaStreamWaitEvent(st, ctx->ev[0], 0));
+                const int* blist = glist + bk.b;
+                const int nbytes = (int)bk.smem;
+                if (bk.c == 1) {
+                    k_nm_team<SoloTeam><<<(unsigned)(bk.e - bk.b), TEAM_THREADS, bk.smem, st>>>(blist, in, nbytes);
+                } else {
+                    cudaLaunchConfig_t cfg = {};
+                    cudaLaunchAttribute attr[1];
+                    attr[0].id = cudaLaunchAttributeClusterDimension;
+                    attr[0].val.clusterDim.x = bk.c;
+                    attr[0].val.clusterDim.y = 1;
+                    attr[0].val.clusterDim.z = 1;
+                    cfg.gridDim = dim3((unsigned)((bk.e - bk.b) * bk.c));
+                    cfg.blockDim = dim3(TEAM_THREADS);
+                    cfg.dynamicSmemBytes = bk.smem;
+                    cfg.stream = st;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = 1;
+                    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_team<ClusterTeam>, blist, in, nbytes));
+                }
+                PG_LAUNCHED(ctx);
+            }
+            for (int j = 0; j < si; j++) {
+                PG_CUDA(ctx, cudaEventRecord(ctx->ev[1 + j], ctx->side[j]));
+                PG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev[1 + j], 0));
+            }
             PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         }
         t_small += ms_since(t0);
-        t0 = now();
-        if (!medium.empty()) {
-            cudaLaunchConfig_t cfg = {};
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeClusterDimension;
-            attr[0].val.clusterDim.x = cluster;
-            attr[0].val.clusterDim.y = 1;
-            attr[0].val.clusterDim.z = 1;
-            cfg.gridDim = dim3((unsigned)(medium.size() * cluster));
-            cfg.blockDim = dim3(GROUP_THREADS);
-            cfg.stream = ctx->stream;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            const int* mlist = glist + small.size();
-            PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_cluster, mlist, in));
-            PG_LAUNCHED(ctx);
-            PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        }
-        t_medium += ms_since(t0);
         t0 = now();
         for (int q : large) {
             int qq = q;
@@ -737,8 +1122,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         }
         PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * 8));
         t_large += ms_since(t0);
-        for (int q : small) it_small += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
-        for (int q : medium) it_medium += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
+        for (int q : team) it_small += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
         for (int q : large) it_large += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
         // ---- decisions in round order (labels exactly as the sequential reference)
         std::vector<int> hbase(G, -1);
@@ -801,9 +1185,9 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         snprintf(line, sizeof line, "Number of Modules: %d,\tQ=%.6g", Module_Num, q);
         log(line, user);
         snprintf(line, sizeof line,
-                 "Timing (ms): generations %d, setup %.1f, one-CTA groups %.1f (%lld iterations), "
-                 "cluster groups %.1f (%lld), cooperative groups %.1f (%lld)",
-                 generations, t_setup, t_small, it_small, t_medium, it_medium, t_large, it_large);
+                 "Timing (ms): generations %d, setup %.1f, team groups %.1f (%lld iterations), "
+                 "cooperative groups %.1f (%lld)",
+                 generations, t_setup, t_small, it_small, t_large, it_large);
         log(line, user);
     }
     return PG_OK;

@@ -16,6 +16,7 @@ struct pg_ctx {
     int sm_count = 0;
     size_t smem_optin = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side[6] = {};  // created on first use; kernels that run beside `stream`
     cudaEvent_t ev[8] = {};
     int64_t launches = 0;
     std::string err;
