@@ -41,7 +41,7 @@ constexpr int COOP_THREADS = 1024;
 constexpr int MAX_ITER = 10000;
 constexpr double EPSILON = 1e-6;
 constexpr double LAMBDA = 0.01;
-constexpr size_t SMEM_CAP = 200 * 1024;        // dynamic shared memory of a team CTA
+constexpr size_t SMEM_CAP = 220 * 1024;        // dynamic shared memory of a team CTA
 constexpr long long MEDIUM_EDGES = 1LL << 22;  // at most this many edges: one team per group
 constexpr int CLUSTER = 16;                    // largest team (CTAs of one cluster)
 constexpr long long MIN_CTA_EDGES = 16384;     // a team CTA keeps at least this many edges
@@ -924,7 +924,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     }
     for (auto& st : ctx->side)
         if (!st) PG_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    const size_t smem_cap = std::min(SMEM_CAP, (size_t)ctx->smem_optin - 8192);
+    const size_t smem_cap = std::min(SMEM_CAP, (size_t)ctx->smem_optin - 4096);
     PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_team<SoloTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     PG_CUDA(ctx,
             cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
