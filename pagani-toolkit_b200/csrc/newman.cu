@@ -852,6 +852,227 @@ k_nm_coop(int gi, Inputs in, double* __restrict__ part)
     sub_partition(g, in, gi, red, tid, nthr, threadIdx.x & 31, tid >> 5, nthr >> 5, tid == 0);
 }
 
+// ---------------------------------------------------------------- whole grid
+// Groups too large for a team run on the whole GPU as one cooperative grid,
+// one group per launch.  Each CTA owns an edge-balanced range of rows; the
+// vector lives in global memory.  A step walks the vector in column blocks
+// of 2^cb_log entries: every CTA copies a block into shared memory and adds
+// the block's share of each own row.  The columns of a row are sorted, so a
+// row's edges split into one contiguous range per block, found once per
+// launch by binary search; columns are read as 16-bit offsets inside their
+// block (a copy made once per launch), which halves the column traffic of a
+// step and keeps it in L2.  Two grid-wide reductions per step as in
+// Lead_Vector.
+
+struct GridLayout {
+    size_t vblk, vown, prev, kdo, bgo, ypart, split, need;
+};
+
+__host__ __device__ inline GridLayout grid_layout(int nown, int nblk, int cb)
+{
+    GridLayout t;
+    size_t at = 0;
+    t.vblk = team_take(at, (size_t)cb * 8);
+    t.vown = team_take(at, (size_t)nown * 8);
+    t.prev = team_take(at, (size_t)nown * 8);
+    t.kdo = team_take(at, (size_t)nown * 8);
+    t.bgo = team_take(at, (size_t)nown * 8);
+    t.ypart = team_take(at, (size_t)nown * 8);
+    t.split = team_take(at, (size_t)(nblk + 1) * nown * 4);
+    t.need = at;
+    return t;
+}
+
+struct GridPart {
+    double *vblk, *vown, *prev, *kdo, *bgo, *ypart;
+    const int32_t* split;    // [own row][nblk + 1] edge offsets (global edge index in the group)
+    const uint16_t* c16;     // the group's columns modulo the block size
+    int n, r0, nown, nblk, cb_log;
+};
+
+// add block b's share of every own row to ypart, L lanes per row
+template <int L>
+__device__ __forceinline__ void grid_rows(const GridPart& gp, int b, int lane, int wid, int nwarp)
+{
+    constexpr int RPW = 32 / L;
+    const int sub = lane & (L - 1);
+    const double* __restrict__ vb = gp.vblk;
+    const uint16_t* __restrict__ cols = gp.c16;
+    for (int base = wid * RPW; base < gp.nown; base += nwarp * RPW) {
+        const int lp = base + lane / L;
+        const bool act = lp < gp.nown;
+        int q = 0, q1 = 0;
+        if (act) {
+            q = gp.split[lp * (gp.nblk + 1) + b] + sub;
+            q1 = gp.split[lp * (gp.nblk + 1) + b + 1];
+        }
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (; q + 3 * L < q1; q += 4 * L) {
+            const int c0 = cols[q], c1 = cols[q + L], c2 = cols[q + 2 * L], c3 = cols[q + 3 * L];
+            s0 += vb[c0];
+            s1 += vb[c1];
+            s2 += vb[c2];
+            s3 += vb[c3];
+        }
+        for (; q < q1; q += L) s0 += vb[cols[q]];
+        double y = (s0 + s1) + (s2 + s3);
+        for (int o = L / 2; o; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        if (act && sub == 0) gp.ypart[lp] = b == 0 ? y : gp.ypart[lp] + y;
+    }
+}
+
+__device__ __forceinline__ void grid_block(int L, const GridPart& gp, int b, int lane, int wid, int nwarp)
+{
+    switch (L) {
+    case 1: grid_rows<1>(gp, b, lane, wid, nwarp); return;
+    case 2: grid_rows<2>(gp, b, lane, wid, nwarp); return;
+    case 4: grid_rows<4>(gp, b, lane, wid, nwarp); return;
+    case 8: grid_rows<8>(gp, b, lane, wid, nwarp); return;
+    case 16: grid_rows<16>(gp, b, lane, wid, nwarp); return;
+    default: grid_rows<32>(gp, b, lane, wid, nwarp); return;
+    }
+}
+
+// Lead_Vector (Modularity_CPU.cpp:224-298) on the whole grid
+__device__ double grid_lead_vector(const GridPart& gp, const Group& gg, int M, double beta, double err_sq, int* iters,
+                                   double* resid, GridRed& red, int& ph)
+{
+    const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, wid = tid >> 5, nwarp = nthr >> 5;
+    double x[3];
+    double vk = 0.0;
+    for (int lp = tid; lp < gp.nown; lp += nthr) {
+        const double vp = (double)gg.AD[gp.r0 + lp];
+        gp.vown[lp] = vp;
+        gg.v[gp.r0 + lp] = vp;
+        vk += vp * gp.kdo[lp];
+    }
+    x[0] = vk;
+    red.sum(x, 1, ph);   // also publishes the start vector
+    vk = x[0];
+    const long long own_edges = gp.nown > 0 ? (long long)gp.split[gp.nown * (gp.nblk + 1) - 1] - gp.split[0] : 0;
+    const int L = lanes_per_row(gp.nown, own_edges / gp.nblk, nthr);
+    const int cb = 1 << gp.cb_log;
+    double s1 = 1.0, s2 = 1.0, vnorm = 0.0;
+    int iter = 0;
+    while (s1 > err_sq && s2 > err_sq && iter < MAX_ITER) {
+        const double c = vk * 0.5 / (double)M;   // vk / 2 / M, the same double
+        for (int b = 0; b < gp.nblk; b++) {
+            const int len = min(cb, gp.n - b * cb);
+            const double* src = gg.v + (size_t)b * cb;
+            for (int p = tid; p < len; p += nthr) gp.vblk[p] = src[p];
+            __syncthreads();
+            grid_block(L, gp, b, lane, wid, nwarp);
+            __syncthreads();
+        }
+        double y2 = 0.0;
+        for (int lp = tid; lp < gp.nown; lp += nthr) {
+            const double y = gp.ypart[lp] - (c * gp.kdo[lp] + (gp.bgo[lp] - beta) * gp.vown[lp]);
+            gp.ypart[lp] = y;
+            y2 += y * y;
+        }
+        x[0] = y2;
+        red.sum(x, 1, ph);
+        vnorm = sqrt(x[0]);
+        double e1 = 0.0, e2 = 0.0;
+        vk = 0.0;
+        for (int lp = tid; lp < gp.nown; lp += nthr) {
+            const double vold = gp.vown[lp];
+            const double vp = gp.ypart[lp] / vnorm;
+            const double d1 = vp - vold, d2 = vp + vold;
+            e1 += d1 * d1;
+            e2 += d2 * d2;
+            vk += vp * gp.kdo[lp];
+            gp.prev[lp] = vold;
+            gp.vown[lp] = vp;
+            gg.v[gp.r0 + lp] = vp;
+        }
+        x[0] = e1;
+        x[1] = e2;
+        x[2] = vk;
+        red.sum(x, 3, ph);   // also publishes the new vector
+        s1 = x[0];
+        s2 = x[1];
+        vk = x[2];
+        iter++;
+    }
+    *iters = iter;
+    *resid = fmin(sqrt(s1), sqrt(s2));
+    for (int lp = tid; lp < gp.nown; lp += nthr) gg.v0[gp.r0 + lp] = gp.prev[lp];
+    red.sync();
+    // first entry of largest magnitude decides the sign (Modularity_CPU.cpp:291-296)
+    const int gt = blockIdx.x * blockDim.x + tid, gn = gridDim.x * blockDim.x;
+    const int mx = red.argmax_abs(gg.v, gp.n, gt, gn, ph);
+    const double lam = (gg.v[mx] * gg.v0[mx] > 0) ? vnorm : -vnorm;
+    red.sync();   // every read of v and v0 is done before they change
+    return lam;
+}
+
+__global__ void __launch_bounds__(COOP_THREADS)
+k_nm_grid(int gi, Inputs in, double* __restrict__ part, uint16_t* __restrict__ c16, int cb_log)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ GridRed red;
+    red.init(part);
+    const Group gg = global_group(in, gi);
+    GridPart gp;
+    gp.n = gg.ng;
+    gp.cb_log = cb_log;
+    const int cb = 1 << cb_log;
+    gp.nblk = (gp.n + cb - 1) >> cb_log;
+    gp.r0 = team_split(gg.sR, gp.n, blockIdx.x, gridDim.x);
+    const int r1 = team_split(gg.sR, gp.n, blockIdx.x + 1, gridDim.x);
+    gp.nown = r1 - gp.r0;
+    const GridLayout t = grid_layout(gp.nown, gp.nblk, cb);
+    gp.vblk = (double*)(sm + t.vblk);
+    gp.vown = (double*)(sm + t.vown);
+    gp.prev = (double*)(sm + t.prev);
+    gp.kdo = (double*)(sm + t.kdo);
+    gp.bgo = (double*)(sm + t.bgo);
+    gp.ypart = (double*)(sm + t.ypart);
+    int32_t* split = (int32_t*)(sm + t.split);
+    gp.split = split;
+    uint16_t* cg16 = c16 + in.eoff[gi];
+    gp.c16 = cg16;
+    // own edges: 16-bit offsets inside their column block
+    for (int q = gg.sR[gp.r0] + threadIdx.x; q < gg.sR[r1]; q += blockDim.x)
+        cg16[q] = (uint16_t)(gg.sC[q] & (cb - 1));
+    for (int lp = threadIdx.x; lp < gp.nown; lp += blockDim.x) {
+        const int p = gp.r0 + lp;
+        gp.kdo[lp] = gg.kdeg[p];
+        gp.bgo[lp] = gg.sumBG[p];
+        const int a = gg.sR[p], e = gg.sR[p + 1];
+        int32_t* sp = split + lp * (gp.nblk + 1);
+        sp[0] = a;
+        for (int b = 1; b < gp.nblk; b++) {
+            int lo = a, hi = e;   // first edge whose column is at least b * cb
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (gg.sC[mid] >= b * cb) hi = mid;
+                else lo = mid + 1;
+            }
+            sp[b] = lo;
+        }
+        sp[gp.nblk] = e;
+    }
+    __syncthreads();
+    int it0, it1 = 0, ph = 0;
+    double res0, res1 = 0.0;
+    double lam = grid_lead_vector(gp, gg, in.M, 0.0, in.err_sq, &it0, &res0, red, ph);
+    const double below = gg.ng > in.gpu_rule_above ? -LAMBDA : 0.0;
+    const bool shifted = lam < below;
+    if (shifted) lam += grid_lead_vector(gp, gg, in.M, -lam, in.err_sq, &it1, &res1, red, ph);
+    double x[3] = {0.0, 0.0, 0.0};
+    for (int lp = threadIdx.x; lp < gp.nown; lp += blockDim.x) {
+        x[0] += gp.vown[lp] > 0.0;
+        x[1] += gp.vown[lp] <= 0.0;
+    }
+    red.sum(x, 2, ph);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double* o = in.out + (size_t)gi * 8;
+        o[0] = lam; o[1] = it0; o[2] = res0; o[3] = it1; o[4] = res1; o[5] = x[0]; o[6] = x[1]; o[7] = shifted;
+    }
+}
+
 __global__ void k_nm_gassign(const int32_t* __restrict__ AD, const int32_t* __restrict__ gidx,
                              const double* __restrict__ v, int32_t P, const int* __restrict__ base,
                              const double* __restrict__ coef, int32_t* __restrict__ label)
@@ -916,6 +1137,8 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "power iteration kernel cannot be resident");
     const int coop_grid = ctx->sm_count;   // one fat block per SM keeps the grid barrier short
     PG_TRY(pg_wst(ctx, "nm.part", (size_t)coop_grid * 8 + 8, &part));
+    uint16_t* c16;
+    PG_TRY(pg_wst(ctx, "nm.c16", (size_t)nnz + 8, &c16));
     int max_cluster = CLUSTER;  // 16 needs the non-portable opt-in
     if (cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
         cudaSuccess) {
@@ -928,6 +1151,9 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_team<SoloTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     PG_CUDA(ctx,
             cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    int grid_per_sm = 0;
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_nm_grid, COOP_THREADS, smem_cap));
     PG_CUDA(ctx, cudaMemsetAsync(label, 0, sizeof(int32_t) * (n + 1), ctx->stream));
 
     std::vector<int32_t> hR(n + 1), hl(n);
@@ -1115,9 +1341,29 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         t0 = now();
         for (int q : large) {
             int qq = q;
-            void* args[] = {(void*)&qq, (void*)&in, (void*)&part};
-            PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_nm_coop, dim3(coop_grid), dim3(COOP_THREADS), args, 0,
-                                                     ctx->stream));
+            // column blocks as large as the shared memory of the CTA with the
+            // most rows allows; the gather kernel when even 1024 do not fit
+            const int ng = (int)(hgoff[q + 1] - hgoff[q]);
+            std::vector<int32_t> rel(ng + 1);
+            for (int p = 0; p <= ng; p++) rel[p] = (int32_t)(hsoff[hgoff[q] + p] - heoff[q]);
+            int most = 0;
+            for (int r = 0; r < coop_grid; r++)
+                most = std::max(most, team_split(rel.data(), ng, r + 1, coop_grid) - team_split(rel.data(), ng, r, coop_grid));
+            int cb_log = 0;
+            for (int lg = 14; lg >= 10 && !cb_log; lg--) {
+                const int nblk = (ng + (1 << lg) - 1) >> lg;
+                if (grid_layout(most, nblk, 1 << lg).need <= smem_cap) cb_log = lg;
+            }
+            if (cb_log && grid_per_sm >= 1) {
+                const size_t need = grid_layout(most, (ng + (1 << cb_log) - 1) >> cb_log, 1 << cb_log).need;
+                void* args[] = {(void*)&qq, (void*)&in, (void*)&part, (void*)&c16, (void*)&cb_log};
+                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_nm_grid, dim3(coop_grid), dim3(COOP_THREADS), args,
+                                                         need, ctx->stream));
+            } else {
+                void* args[] = {(void*)&qq, (void*)&in, (void*)&part};
+                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_nm_coop, dim3(coop_grid), dim3(COOP_THREADS), args, 0,
+                                                         ctx->stream));
+            }
             PG_LAUNCHED(ctx);
         }
         PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * 8));
