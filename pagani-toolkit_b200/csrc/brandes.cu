@@ -2,10 +2,11 @@
 // BC_GPU_node_pred.cu:6-155; Betweenness_CPU, U/BC/BC_CPU/BC_CPU/BC_CPU.cpp:6-82)
 // with exact 64-bit path counts and FP64 dependencies.
 //
-// 64 sources run together, two per warp lane (lane l owns sources l and
-// l+32): per node the state is a row of 64 entries (level int32, sigma
-// uint64, coefficient double), so a neighbour's state for all sources is two
-// coalesced 256-byte reads.  Source bits are 64-bit masks per node.
+// 128 sources run together, four per warp lane (lane l owns sources l,
+// l+32, l+64, l+96): per node the state is a row of 128 entries (level int32,
+// sigma uint64, coefficient double), so a neighbour's state for all sources
+// is four coalesced 256-byte reads.  Source bits are 128-bit masks per node
+// (two 64-bit words).
 //   forward level d:  node v sums sigma[u][s] over neighbours u that are in
 //                     the frontier of a source s not yet seen at v; the
 //                     non-zero sums are exactly the sources reaching v at d;
@@ -29,7 +30,8 @@ namespace cg = cooperative_groups;
 
 namespace {
 constexpr int THREADS = 256;
-constexpr int S = 64;         // sources per batch
+constexpr int S = 128;        // sources per batch
+constexpr int SL = S / 32;    // sources per lane
 constexpr int LCAP = 48;      // levels whose frontier masks are kept for the backward sweep
 typedef unsigned long long u64;
 
@@ -42,9 +44,9 @@ struct BCArgs {
     int32_t* dist;            // [n][S]
     u64* sigma;               // [n][S]
     double* coef;             // [n][S]
-    u64* front;               // [2][n]
-    u64* fhist;               // [LCAP][n] frontier mask of every level < LCAP
-    u64* seen;                // [n]
+    ulonglong2* front;        // [2][n] source masks (x: sources 0-63, y: 64-127)
+    ulonglong2* fhist;        // [LCAP][n] frontier mask of every level < LCAP
+    ulonglong2* seen;         // [n]
     int* flags;               // [3] rotating "something changed" flags
     double* bc;               // [n] accumulated FP64 betweenness (null: forward only)
     double* inv;              // [n] sum of 1/d (null: skip)
@@ -76,7 +78,23 @@ __device__ __forceinline__ int next_node(const BCArgs& a, int slot, int& k, int 
 
 __device__ __forceinline__ u64 shfl64(u64 x, int j) { return __shfl_sync(0xffffffffu, x, j); }
 
-__global__ void __launch_bounds__(THREADS)
+// bit of source lane + 32 k in a 128-bit mask
+__device__ __forceinline__ bool has_src(const ulonglong2& m, int lane, int k)
+{
+    const u64 w = k < 2 ? m.x : m.y;
+    return (w >> (lane + 32 * (k & 1))) & 1ULL;
+}
+
+// mask with bit lane + 32 k set where f[k] holds, over the warp
+__device__ __forceinline__ ulonglong2 lane_mask(const bool (&f)[SL])
+{
+    const unsigned b0 = __ballot_sync(0xffffffffu, f[0]), b1 = __ballot_sync(0xffffffffu, f[1]);
+    const unsigned b2 = __ballot_sync(0xffffffffu, f[2]), b3 = __ballot_sync(0xffffffffu, f[3]);
+    return make_ulonglong2((u64)b0 | ((u64)b1 << 32), (u64)b2 | ((u64)b3 << 32));
+}
+
+// four CTAs per SM (64 registers): occupancy hides the L2 latency of the row gathers
+__global__ void __launch_bounds__(THREADS, 4)
 k_brandes(BCArgs a, int batch_first, int batch_last)
 {
     cg::grid_group grid = cg::this_grid();
@@ -85,14 +103,18 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int n = a.n;
     const size_t gt = (size_t)blockIdx.x * blockDim.x + threadIdx.x, gstride = (size_t)gridDim.x * blockDim.x;
-    const u64 lo_bit = 1ULL << lane, hi_bit = 1ULL << (lane + 32);
     for (int b = batch_first; b < batch_last; b++) {
         const int s0 = b * S;
         const int ns = min(S, a.nsrc - s0);
-        const u64 full = ns == S ? ~0ULL : ((1ULL << ns) - 1ULL);
+        const ulonglong2 full = make_ulonglong2(ns >= 64 ? ~0ULL : ((1ULL << ns) - 1ULL),
+                                                ns >= 128 ? ~0ULL : ns > 64 ? ((1ULL << (ns - 64)) - 1ULL) : 0ULL);
         // ---- init: levels -1, frontier = sources
         for (size_t q = gt; q < (size_t)n * S; q += gstride) a.dist[q] = -1;
-        for (size_t v = gt; v < (size_t)n; v += gstride) { a.front[v] = 0ULL; a.seen[v] = 0ULL; a.fhist[v] = 0ULL; }
+        for (size_t v = gt; v < (size_t)n; v += gstride) {
+            a.front[v] = make_ulonglong2(0ULL, 0ULL);
+            a.seen[v] = make_ulonglong2(0ULL, 0ULL);
+            a.fhist[v] = make_ulonglong2(0ULL, 0ULL);
+        }
         for (size_t q = gt; q < (size_t)WORK_SLOTS; q += gstride) a.work[q] = 0;
         if (gt < 3) a.flags[gt] = 0;
         grid.sync();
@@ -100,83 +122,87 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
             int s = a.sources ? a.sources[s0 + gt] : s0 + (int)gt;
             a.dist[(size_t)s * S + gt] = 0;
             a.sigma[(size_t)s * S + gt] = 1ULL;
-            atomicOr(&a.front[s], 1ULL << gt);
-            atomicOr(&a.seen[s], 1ULL << gt);
-            atomicOr(&a.fhist[s], 1ULL << gt);
+            const u64 bit = 1ULL << (gt & 63);
+            u64* w = gt < 64 ? &a.front[s].x : &a.front[s].y;
+            atomicOr(w, bit);
+            atomicOr(gt < 64 ? &a.seen[s].x : &a.seen[s].y, bit);
+            atomicOr(gt < 64 ? &a.fhist[s].x : &a.fhist[s].y, bit);
         }
         grid.sync();
         // ---- forward
         int d = 1;
-        u64* cur = a.front;
-        u64* nxt = a.front + n;
+        ulonglong2* cur = a.front;
+        ulonglong2* nxt = a.front + n;
         for (;; d++) {
             if (gt == 0) a.flags[(d + 1) % 3] = 0;
             int found = 0;
             int kk = 0;
             const int fslot = d < WORK_SLOTS / 2 ? d : WORK_SLOTS;
             for (int v = next_node(a, fslot, kk, gw, nw); v < n; v = next_node(a, fslot, kk, gw, nw)) {
-                const u64 sv = a.seen[v];
-                const u64 need = full & ~sv;
-                u64 nb = 0ULL;
-                if (need) {
+                const ulonglong2 sv = a.seen[v];
+                const ulonglong2 need = make_ulonglong2(full.x & ~sv.x, full.y & ~sv.y);
+                ulonglong2 nb = make_ulonglong2(0ULL, 0ULL);
+                if (need.x | need.y) {
                     const int32_t s = a.R[v], e = a.R[v + 1];
-                    u64 sg0 = 0ULL, sg1 = 0ULL;
+                    u64 sg[SL] = {0ULL, 0ULL, 0ULL, 0ULL};
                     for (int32_t base = s; base < e; base += 32) {
                         int32_t f = base + lane;
                         int u = f < e ? a.C[f] : 0;
-                        u64 fu = f < e ? (cur[u] & need) : 0ULL;
-                        unsigned m = __ballot_sync(0xffffffffu, fu != 0ULL);
-                        // up to four active neighbours per step, loads issued together
+                        ulonglong2 fu = make_ulonglong2(0ULL, 0ULL);
+                        if (f < e) {
+                            const ulonglong2 c = cur[u];
+                            fu = make_ulonglong2(c.x & need.x, c.y & need.y);
+                        }
+                        unsigned m = __ballot_sync(0xffffffffu, (fu.x | fu.y) != 0ULL);
+                        // two active neighbours per step, their loads issued together
                         while (m) {
-                            int j[4];
+                            int j[2];
 #pragma unroll
-                            for (int t = 0; t < 4; t++) {
+                            for (int t = 0; t < 2; t++) {
                                 j[t] = m ? __ffs(m) - 1 : -1;
                                 m &= m ? m - 1 : 0u;
                             }
-                            u64 x0[4], x1[4];
+                            u64 x[2][SL];
 #pragma unroll
-                            for (int t = 0; t < 4; t++) {
+                            for (int t = 0; t < 2; t++) {
                                 const int jj = j[t] < 0 ? j[0] : j[t];
                                 const int uj = __shfl_sync(0xffffffffu, u, jj);
-                                const u64 fj = j[t] < 0 ? 0ULL : shfl64(fu, jj);
+                                ulonglong2 fj;
+                                fj.x = j[t] < 0 ? 0ULL : shfl64(fu.x, jj);
+                                fj.y = j[t] < 0 ? 0ULL : shfl64(fu.y, jj);
                                 const u64* row = a.sigma + (size_t)uj * S;
-                                x0[t] = (fj & lo_bit) ? row[lane] : 0ULL;
-                                x1[t] = (fj & hi_bit) ? row[lane + 32] : 0ULL;
+#pragma unroll
+                                for (int k = 0; k < SL; k++) x[t][k] = has_src(fj, lane, k) ? row[lane + 32 * k] : 0ULL;
                             }
 #pragma unroll
-                            for (int t = 0; t < 4; t++) {
-                                sg0 += x0[t];
-                                sg1 += x1[t];
-                            }
+                            for (int t = 0; t < 2; t++)
+#pragma unroll
+                                for (int k = 0; k < SL; k++) sg[k] += x[t][k];
                         }
                     }
-                    const unsigned b0 = __ballot_sync(0xffffffffu, sg0 != 0ULL);
-                    const unsigned b1 = __ballot_sync(0xffffffffu, sg1 != 0ULL);
-                    nb = (u64)b0 | ((u64)b1 << 32);
-                    if (sg0) {
-                        a.sigma[(size_t)v * S + lane] = sg0;
-                        a.dist[(size_t)v * S + lane] = d;
-                    }
-                    if (sg1) {
-                        a.sigma[(size_t)v * S + lane + 32] = sg1;
-                        a.dist[(size_t)v * S + lane + 32] = d;
-                    }
-                    if (nb) {
-                        if (lane == 0 && a.inv) a.inv[v] += (double)__popcll(nb) / (double)d;
+                    const bool fs[SL] = {sg[0] != 0ULL, sg[1] != 0ULL, sg[2] != 0ULL, sg[3] != 0ULL};
+                    nb = lane_mask(fs);
+#pragma unroll
+                    for (int k = 0; k < SL; k++)
+                        if (sg[k]) {
+                            a.sigma[(size_t)v * S + lane + 32 * k] = sg[k];
+                            a.dist[(size_t)v * S + lane + 32 * k] = d;
+                        }
+                    if (nb.x | nb.y) {
+                        if (lane == 0 && a.inv) a.inv[v] += (double)(__popcll(nb.x) + __popcll(nb.y)) / (double)d;
                         found = 1;
                     }
                 }
                 if (lane == 0) {
                     nxt[v] = nb;
-                    a.seen[v] = sv | nb;
+                    a.seen[v] = make_ulonglong2(sv.x | nb.x, sv.y | nb.y);
                     if (d < LCAP) a.fhist[(size_t)d * n + v] = nb;
                 }
             }
             if (found && lane == 0) a.flags[d % 3] = 1;
             grid.sync();
             const int any = a.flags[d % 3];
-            u64* t = cur; cur = nxt; nxt = t;
+            ulonglong2* t = cur; cur = nxt; nxt = t;
             if (!any) break;
         }
         const int maxd = d - 1;  // deepest level reached
@@ -195,16 +221,17 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                 int kk = 0;
                 for (int v = next_node(a, bslot, kk, gw, nw); v < n; v = next_node(a, bslot, kk, gw, nw)) {
                     // sources for which v sits on level lv
-                    u64 mine_m;
+                    ulonglong2 mine;
                     if (lv < LCAP) {
-                        mine_m = a.fhist[(size_t)lv * n + v];
+                        mine = a.fhist[(size_t)lv * n + v];
                     } else {
-                        unsigned x0 = __ballot_sync(0xffffffffu, a.dist[(size_t)v * S + lane] == lv);
-                        unsigned x1 = __ballot_sync(0xffffffffu, a.dist[(size_t)v * S + lane + 32] == lv);
-                        mine_m = (u64)x0 | ((u64)x1 << 32);
+                        bool on[SL];
+#pragma unroll
+                        for (int k = 0; k < SL; k++) on[k] = a.dist[(size_t)v * S + lane + 32 * k] == lv;
+                        mine = lane_mask(on);
                     }
-                    if (!mine_m) continue;
-                    double acc0 = 0.0, acc1 = 0.0;
+                    if (!(mine.x | mine.y)) continue;
+                    double acc[SL] = {0.0, 0.0, 0.0, 0.0};
                     if (lv < maxd) {
                         const int32_t s = a.R[v], e = a.R[v + 1];
                         for (int32_t base = s; base < e; base += 32) {
@@ -212,56 +239,59 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                             int w = f < e ? a.C[f] : 0;
                             if (lv + 1 < LCAP) {
                                 // neighbours one level deeper for some of v's sources
-                                u64 mw = f < e ? (a.fhist[(size_t)(lv + 1) * n + w] & mine_m) : 0ULL;
-                                unsigned bm = __ballot_sync(0xffffffffu, mw != 0ULL);
+                                ulonglong2 mw = make_ulonglong2(0ULL, 0ULL);
+                                if (f < e) {
+                                    const ulonglong2 h = a.fhist[(size_t)(lv + 1) * n + w];
+                                    mw = make_ulonglong2(h.x & mine.x, h.y & mine.y);
+                                }
+                                unsigned bm = __ballot_sync(0xffffffffu, (mw.x | mw.y) != 0ULL);
                                 while (bm) {
-                                    int j[4];
+                                    int j[2];
 #pragma unroll
-                                    for (int t = 0; t < 4; t++) {
+                                    for (int t = 0; t < 2; t++) {
                                         j[t] = bm ? __ffs(bm) - 1 : -1;
                                         bm &= bm ? bm - 1 : 0u;
                                     }
-                                    double y0[4], y1[4];
+                                    double y[2][SL];
 #pragma unroll
-                                    for (int t = 0; t < 4; t++) {
+                                    for (int t = 0; t < 2; t++) {
                                         const int jj = j[t] < 0 ? j[0] : j[t];
                                         const int wj = __shfl_sync(0xffffffffu, w, jj);
-                                        const u64 mj = j[t] < 0 ? 0ULL : shfl64(mw, jj);
+                                        ulonglong2 mj;
+                                        mj.x = j[t] < 0 ? 0ULL : shfl64(mw.x, jj);
+                                        mj.y = j[t] < 0 ? 0ULL : shfl64(mw.y, jj);
                                         const double* row = a.coef + (size_t)wj * S;
-                                        y0[t] = (mj & lo_bit) ? row[lane] : 0.0;
-                                        y1[t] = (mj & hi_bit) ? row[lane + 32] : 0.0;
+#pragma unroll
+                                        for (int k = 0; k < SL; k++) y[t][k] = has_src(mj, lane, k) ? row[lane + 32 * k] : 0.0;
                                     }
 #pragma unroll
-                                    for (int t = 0; t < 4; t++) {
-                                        acc0 += y0[t];
-                                        acc1 += y1[t];
-                                    }
+                                    for (int t = 0; t < 2; t++)
+#pragma unroll
+                                        for (int k = 0; k < SL; k++) acc[k] += y[t][k];
                                 }
                             } else {
                                 int cnt = min(32, e - base);
-                                for (int j = 0; j < cnt; j++) {
-                                    int wj = __shfl_sync(0xffffffffu, w, j);
+                                for (int jn = 0; jn < cnt; jn++) {
+                                    int wj = __shfl_sync(0xffffffffu, w, jn);
                                     const int32_t* dw = a.dist + (size_t)wj * S;
                                     const double* row = a.coef + (size_t)wj * S;
-                                    if ((mine_m & lo_bit) && dw[lane] == lv + 1) acc0 += row[lane];
-                                    if ((mine_m & hi_bit) && dw[lane + 32] == lv + 1) acc1 += row[lane + 32];
+#pragma unroll
+                                    for (int k = 0; k < SL; k++)
+                                        if (has_src(mine, lane, k) && dw[lane + 32 * k] == lv + 1) acc[k] += row[lane + 32 * k];
                                 }
                             }
                         }
                     }
                     double delta = 0.0;
-                    if (mine_m & lo_bit) {
-                        double sg = __ull2double_rn(a.sigma[(size_t)v * S + lane]);
-                        double dl = sg * acc0;
-                        a.coef[(size_t)v * S + lane] = (1.0 + dl) / sg;
-                        delta += dl;
-                    }
-                    if (mine_m & hi_bit) {
-                        double sg = __ull2double_rn(a.sigma[(size_t)v * S + lane + 32]);
-                        double dl = sg * acc1;
-                        a.coef[(size_t)v * S + lane + 32] = (1.0 + dl) / sg;
-                        delta += dl;
-                    }
+#pragma unroll
+                    for (int k = 0; k < SL; k++)
+                        if (has_src(mine, lane, k)) {
+                            const size_t at = (size_t)v * S + lane + 32 * k;
+                            const double sg = __ull2double_rn(a.sigma[at]);
+                            const double dl = sg * acc[k];
+                            a.coef[at] = (1.0 + dl) / sg;
+                            delta += dl;
+                        }
                     for (int o = 16; o; o >>= 1) delta += __shfl_xor_sync(0xffffffffu, delta, o);
                     if (lane == 0 && a.bc) a.bc[v] += delta;
                 }
@@ -352,7 +382,7 @@ extern "C" pg_status pg_betweenness(pg_ctx* ctx, const pg_graph* g, float* bc, d
     }
     const int nb = (n + S - 1) / S;
     // a bounded number of batches per launch keeps every launch short
-    const int per_launch = 32;
+    const int per_launch = 16;
     for (int b = 0; b < nb; b += per_launch) PG_TRY(launch_brandes(ctx, a, b, std::min(nb, b + per_launch)));
     float *dbc, *deff = nullptr;
     PG_TRY(pg_wst(ctx, "bc.bcf", (size_t)n + 1, &dbc));
