@@ -692,10 +692,12 @@ __device__ double team_lead_vector(const Team& tm, const Group& gg, int M, doubl
     return lam;
 }
 
-// Sliced layout of the own rows: sort, choose L, fill.  Returns the number of
-// slices, 0 when they do not fit in `space` bytes.
+// Sliced layout of the own rows: sort, choose L, fill.  The slices go to
+// shared memory (`cols`, `space` bytes) when some L fits there, else to the
+// CTA's region of global memory (`gcols`, `gspace` bytes, which always holds
+// L = 32).  Returns the number of slices and sets tm.cols.
 __device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int32_t* soff, uint16_t* cols,
-                          size_t space, int* sL)
+                          size_t space, uint16_t* gcols, size_t gspace, int* sL, int* sIn)
 {
     const int tid = threadIdx.x, nthr = blockDim.x, nown = tm.nown;
     const int P2 = pow2_at_least(nown);
@@ -746,6 +748,10 @@ __device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int3
         int best = -1;
         for (int t = 0; t < 6; t++)
             if ((size_t)size[t] * 2 <= space && (best < 0 || cost[t] < cost[best])) best = t;
+        *sIn = best >= 0;   // in shared memory
+        if (best < 0)
+            for (int t = 0; t < 6; t++)
+                if ((size_t)size[t] * 2 <= gspace && (best < 0 || cost[t] < cost[best])) best = t;
         *sL = best < 0 ? 0 : 1 << best;
         if (best >= 0) {
             const int L = 1 << best, RPS = 32 / L, ns = (nown + RPS - 1) / RPS;
@@ -761,6 +767,8 @@ __device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int3
     __syncthreads();
     const int L = *sL;
     if (L == 0) return 0;
+    if (!*sIn) cols = gcols;
+    tm.cols = cols;
     const int RPS = 32 / L, ns = (nown + RPS - 1) / RPS;
     const int lane = tid & 31, sub = lane & (L - 1);
     for (int s = tid >> 5; s < ns; s += nthr >> 5) {
@@ -784,11 +792,11 @@ __device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int3
 // One team per group of `glist`; the cluster size is set at launch.
 template <class Kind>
 __global__ void __launch_bounds__(TEAM_THREADS)
-k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes)
+k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes, uint16_t* __restrict__ slices)
 {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ Partials ps;
-    __shared__ int sL;
+    __shared__ int sL, sIn;
     cg::cluster_group cl = cg::this_cluster();
     const int nb = Kind::kCluster ? (int)cl.num_blocks() : 1, rank = Kind::kCluster ? (int)cl.block_rank() : 0;
     const int gi = glist[blockIdx.x / nb];
@@ -816,10 +824,14 @@ k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes)
     int32_t* soff = (int32_t*)(sm + t.soff);
     uint16_t* cols = (uint16_t*)(sm + t.cols);
     const size_t space = (size_t)smem_bytes > t.cols ? (size_t)smem_bytes - t.cols : 0;
-    tm.nslices = tm.n < 65535 ? team_slice(tm, gg, e0, key, soff, cols, space, &sL) : 0;
+    // this CTA's region of the global slice store: 2 entries per edge and 64
+    // per row, counted from the group's first edge and row
+    const long long own_e = (long long)tm.oR[tm.nown];
+    uint16_t* gcols = slices + 2 * (in.eoff[gi] + e0) + 64 * (in.goff[gi] + tm.r0);
+    const size_t gspace = (size_t)(2 * own_e + 64LL * tm.nown) * 2;
+    tm.nslices = tm.n < 65535 ? team_slice(tm, gg, e0, key, soff, cols, space, gcols, gspace, &sL, &sIn) : 0;
     tm.perm = key;
     tm.soff = soff;
-    tm.cols = cols;
     tm.gcols = gg.sC + e0;
     tm.L = tm.nslices > 0 ? sL : lanes_per_row(tm.nown, tm.nown > 0 ? (long long)tm.oR[tm.nown] : 0, blockDim.x);
     // both passes of Sub_Partition
@@ -1139,6 +1151,8 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     PG_TRY(pg_wst(ctx, "nm.part", (size_t)coop_grid * 8 + 8, &part));
     uint16_t* c16;
     PG_TRY(pg_wst(ctx, "nm.c16", (size_t)nnz + 8, &c16));
+    uint16_t* slices;   // team CTAs whose sliced rows do not fit shared memory
+    PG_TRY(pg_wst(ctx, "nm.slices", (size_t)2 * nnz + 64 * (size_t)n + 64, &slices));
     int max_cluster = CLUSTER;  // 16 needs the non-portable opt-in
     if (cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
         cudaSuccess) {
@@ -1313,7 +1327,8 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                 const int* blist = glist + bk.b;
                 const int nbytes = (int)bk.smem;
                 if (bk.c == 1) {
-                    k_nm_team<SoloTeam><<<(unsigned)(bk.e - bk.b), TEAM_THREADS, bk.smem, st>>>(blist, in, nbytes);
+                    k_nm_team<SoloTeam><<<(unsigned)(bk.e - bk.b), TEAM_THREADS, bk.smem, st>>>(blist, in, nbytes,
+                                                                                             slices);
                 } else {
                     cudaLaunchConfig_t cfg = {};
                     cudaLaunchAttribute attr[1];
@@ -1327,7 +1342,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                     cfg.stream = st;
                     cfg.attrs = attr;
                     cfg.numAttrs = 1;
-                    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_team<ClusterTeam>, blist, in, nbytes));
+                    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_team<ClusterTeam>, blist, in, nbytes, slices));
                 }
                 PG_LAUNCHED(ctx);
             }
