@@ -40,10 +40,10 @@ import numpy as np  # noqa: E402
 
 N_VOX, T_LEN, N_SIG, SPARSITY = 58000, 240, 20, 1.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one-pass ncu
-# capture) of one k_brandes launch -- 32 batches of 64 sources -- on the
+# capture) of one k_brandes launch -- 16 batches of 128 sources -- on the
 # 58000-voxel subject; the workload is deterministic, so it holds for every run
-BRANDES_DRAM_BYTES_PER_LAUNCH_58K = 32.76e9
-BRANDES_SOURCES_PER_LAUNCH = 32 * 64
+BRANDES_DRAM_BYTES_PER_LAUNCH_58K = 30.47e9
+BRANDES_SOURCES_PER_LAUNCH = 16 * 128
 WORKLOAD = "subject-58k: N=58000 voxels, T=240, 20 latent signals, top 1% |r| -> binary CSR; " \
            "degree, Cp (triangles), Lp/efficiency, Brandes BC all sources, Newman modularity"
 
@@ -348,7 +348,7 @@ def main():
                      "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": BRANDES_DRAM_BYTES_PER_LAUNCH_58K if N_VOX == 58000 else None,
                      "algorithmic_bytes_per_launch": per_src * BRANDES_SOURCES_PER_LAUNCH,
-                     "per_launch": "32 batches of 64 sources",
+                     "per_launch": "16 batches of 128 sources",
                      "peak_source": peak_kind},
         "bc_gteps": gteps, "bc_mteps_reference_formula": nnz * N_VOX / (tm["bc_ms"]) / 1024 ** 2,
         "stage_ms": {"build": {k: tm["build"][k] for k in ("ms_zscore", "ms_hist", "ms_emit", "ms_select", "ms_csr")},
