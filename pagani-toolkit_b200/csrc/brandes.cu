@@ -85,6 +85,37 @@ __device__ __forceinline__ bool has_src(const ulonglong2& m, int lane, int k)
     return (w >> (lane + 32 * (k & 1))) & 1ULL;
 }
 
+// Per 32-neighbour chunk the sweeps pick one of two layouts:
+//  - by neighbour: the warp takes the active neighbours one by one and every
+//    lane handles its four sources (all 128 sources per neighbour step);
+//  - by source: lanes hold the 32 neighbours and the warp walks the sources
+//    the node still needs, one warp-wide sum per source.
+// The cost of a chunk is about BY_NB per active neighbour in the first and
+// BY_SRC_* per needed source in the second (tuned on the 58k subject graphs);
+// the cheaper one runs.  Late forward levels and the first backward level
+// need few sources per node.
+constexpr int BY_NB = 40, BY_SRC_FWD = 96, BY_SRC_BWD = 32;
+
+__device__ __forceinline__ int next_src(u64& w0, u64& w1)
+{
+    if (w0) {
+        const int s = __ffsll((long long)w0) - 1;
+        w0 &= w0 - 1;
+        return s;
+    }
+    if (w1) {
+        const int s = 64 + __ffsll((long long)w1) - 1;
+        w1 &= w1 - 1;
+        return s;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ bool mask_bit(const ulonglong2& m, int s)
+{
+    return ((s < 64 ? m.x : m.y) >> (s & 63)) & 1ULL;
+}
+
 // mask with bit lane + 32 k set where f[k] holds, over the warp
 __device__ __forceinline__ ulonglong2 lane_mask(const bool (&f)[SL])
 {
@@ -144,6 +175,7 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                 ulonglong2 nb = make_ulonglong2(0ULL, 0ULL);
                 if (need.x | need.y) {
                     const int32_t s = a.R[v], e = a.R[v + 1];
+                    const int kneed = __popcll(need.x) + __popcll(need.y);
                     u64 sg[SL] = {0ULL, 0ULL, 0ULL, 0ULL};
                     for (int32_t base = s; base < e; base += 32) {
                         int32_t f = base + lane;
@@ -154,7 +186,32 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                             fu = make_ulonglong2(c.x & need.x, c.y & need.y);
                         }
                         unsigned m = __ballot_sync(0xffffffffu, (fu.x | fu.y) != 0ULL);
-                        // two active neighbours per step, their loads issued together
+                        if (m && kneed * BY_SRC_FWD < __popc(m) * BY_NB) {
+                            // by source, two at a time; integer sums, exact in any order
+                            u64 w0 = need.x, w1 = need.y;
+                            for (;;) {
+                                const int sa = next_src(w0, w1), sb = next_src(w0, w1);
+                                if (sa < 0) break;
+                                u64 xa = mask_bit(fu, sa) ? a.sigma[(size_t)u * S + sa] : 0ULL;
+                                u64 xb = (sb >= 0 && mask_bit(fu, sb)) ? a.sigma[(size_t)u * S + sb] : 0ULL;
+#pragma unroll
+                                for (int o = 16; o; o >>= 1) {
+                                    xa += __shfl_xor_sync(0xffffffffu, xa, o);
+                                    xb += __shfl_xor_sync(0xffffffffu, xb, o);
+                                }
+                                {
+                                    const u64 adda = lane == (sa & 31) ? xa : 0ULL;
+                                    const u64 addb = (sb >= 0 && lane == (sb & 31)) ? xb : 0ULL;
+                                    const int ka = sa >> 5, kb = sb >> 5;
+                                    sg[0] += (ka == 0 ? adda : 0ULL) + (kb == 0 ? addb : 0ULL);
+                                    sg[1] += (ka == 1 ? adda : 0ULL) + (kb == 1 ? addb : 0ULL);
+                                    sg[2] += (ka == 2 ? adda : 0ULL) + (kb == 2 ? addb : 0ULL);
+                                    sg[3] += (ka == 3 ? adda : 0ULL) + (kb == 3 ? addb : 0ULL);
+                                }
+                            }
+                            m = 0u;
+                        }
+                        // by neighbour: two active neighbours per step, their loads issued together
                         while (m) {
                             int j[2];
 #pragma unroll
@@ -234,6 +291,7 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                     double acc[SL] = {0.0, 0.0, 0.0, 0.0};
                     if (lv < maxd) {
                         const int32_t s = a.R[v], e = a.R[v + 1];
+                        const int kmine = __popcll(mine.x) + __popcll(mine.y);
                         for (int32_t base = s; base < e; base += 32) {
                             int32_t f = base + lane;
                             int w = f < e ? a.C[f] : 0;
@@ -245,6 +303,36 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
                                     mw = make_ulonglong2(h.x & mine.x, h.y & mine.y);
                                 }
                                 unsigned bm = __ballot_sync(0xffffffffu, (mw.x | mw.y) != 0ULL);
+                                if (bm && kmine * BY_SRC_BWD < __popc(bm) * BY_NB) {
+                                    // by source, two at a time; each chunk's terms meet in a
+                                    // fixed shuffle tree, so the FP64 sums are deterministic
+                                    u64 w0 = mine.x, w1 = mine.y;
+                                    for (;;) {
+                                        const int sa = next_src(w0, w1), sb = next_src(w0, w1);
+                                        if (sa < 0) break;
+                                        double xa = mask_bit(mw, sa) ? a.coef[(size_t)w * S + sa] : 0.0;
+                                        double xb = (sb >= 0 && mask_bit(mw, sb)) ? a.coef[(size_t)w * S + sb] : 0.0;
+#pragma unroll
+                                        for (int o = 16; o; o >>= 1) {
+                                            xa += __shfl_xor_sync(0xffffffffu, xa, o);
+                                            xb += __shfl_xor_sync(0xffffffffu, xb, o);
+                                        }
+                                        {
+                                            const double adda = lane == (sa & 31) ? xa : 0.0;
+                                            const double addb = (sb >= 0 && lane == (sb & 31)) ? xb : 0.0;
+                                            const int ka = sa >> 5, kb = sb >> 5;
+                                            if (ka == 0) acc[0] += adda;
+                                            if (ka == 1) acc[1] += adda;
+                                            if (ka == 2) acc[2] += adda;
+                                            if (ka == 3) acc[3] += adda;
+                                            if (kb == 0) acc[0] += addb;
+                                            if (kb == 1) acc[1] += addb;
+                                            if (kb == 2) acc[2] += addb;
+                                            if (kb == 3) acc[3] += addb;
+                                        }
+                                    }
+                                    bm = 0u;
+                                }
                                 while (bm) {
                                     int j[2];
 #pragma unroll
