@@ -42,7 +42,7 @@ N_VOX, T_LEN, N_SIG, SPARSITY = 58000, 240, 20, 1.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one-pass ncu
 # capture) of one k_brandes launch -- 16 batches of 128 sources -- on the
 # 58000-voxel subject; the workload is deterministic, so it holds for every run
-BRANDES_DRAM_BYTES_PER_LAUNCH_58K = 30.47e9
+BRANDES_DRAM_BYTES_PER_LAUNCH_58K = 28.74e9
 BRANDES_SOURCES_PER_LAUNCH = 16 * 128
 WORKLOAD = "subject-58k: N=58000 voxels, T=240, 20 latent signals, top 1% |r| -> binary CSR; " \
            "degree, Cp (triangles), Lp/efficiency, Brandes BC all sources, Newman modularity"
