@@ -189,6 +189,20 @@ typedef void (*pg_log_fn)(const char* line, void* user);
 pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_above, int32_t* labels,
                     double* Q, int32_t* n_modules, pg_log_fn log, void* user);
 
+/* Eigenvector centrality by the power method of the CUEC tools:
+ * Lead_Vector_GPU in U/CUEC/CUEC/CUEC_unweighted.cu:61-214 (edges count 1)
+ * and W/CUEC/weighted-net.cu:55-218 (a graph with weights uses them).  The
+ * iteration starts from the node ids, normalises by the 2-norm each step and
+ * stops when |y - u0| or |y + u0| is at most 1e-6 or after 10,000 steps.
+ * raw = 0 returns the normalised vector of the last step, as the unweighted
+ * tool writes it (CUEC_unweighted.cu:161); raw = 1 returns y = A x of the
+ * last step, as the weighted tool writes it (weighted-net.cu:190).
+ * ec: host double[n]; eigenvalue = the 2-norm of the last step's vector
+ * before normalisation (the tools' _evalue.txt); iterations and residual
+ * (min of the two errors) are optional. */
+pg_status pg_eigen_centrality(pg_ctx* ctx, const pg_graph* g, int32_t raw, double* ec, double* eigenvalue,
+                              int32_t* iterations, double* residual);
+
 /* Maslov-Sneppen degree-preserving rewiring: Maslov/Rewire (U/cuda_EC/cuda_EC/
  * Maslov.cpp:8-109) and Maslov_weighted_1 (W/Maslov/Maslov/Maslov.cpp:106-196).
  * `attempts` swap attempts from a seeded counter-based generator, in rounds

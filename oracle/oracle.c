@@ -708,3 +708,51 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
     free(ea); free(eb); free(ew); free(bits); free(owner); free(av); free(ai); free(ok); free(coin);
     return committed;
 }
+
+/* ------------------------------------------------- eigenvector centrality */
+/* The power method of the two CUEC tools: Lead_Vector_GPU in
+ * U/CUEC/CUEC/CUEC_unweighted.cu:61-214 (every edge value 1) and in
+ * W/CUEC/weighted-net.cu:55-218 (the CSR weights as double).  u starts as the
+ * node ids (init_AD, :38-43 in both files).  A step (:153-188 / :154-187):
+ * u0 = u; vNorm = |u|; u = u * (1 / vNorm); y = A u; err1 = |y - u0|,
+ * err2 = |y + u0|; the loop ends when either is at most 1e-6 or after 10,000
+ * steps.  The unweighted tool keeps the normalised u of the last step
+ * (:161), the weighted tool the last y (:190); both return vNorm as the
+ * eigenvalue.  `raw` selects the weighted tool's output.  Norms are plain
+ * sequential sums of squares (the reference's cuBLAS nrm2 is not vendored).
+ * Returns the number of steps. */
+int or_eigen_centrality(const int32_t* R, const int32_t* C, const float* V, int N, int raw,
+                        double* ec, double* eigenvalue, double* residual)
+{
+    double* u = (double*)malloc(sizeof(double) * (size_t)(N > 0 ? N : 1));
+    double* u0 = (double*)malloc(sizeof(double) * (size_t)(N > 0 ? N : 1));
+    double* x = (double*)malloc(sizeof(double) * (size_t)(N > 0 ? N : 1));
+    for (int i = 0; i < N; i++) u[i] = (double)i;
+    double err1 = 1.0, err2 = 1.0, vnorm = 0.0;
+    int iter = 0;
+    while (err1 > 1e-6 && err2 > 1e-6 && iter < 10000) {
+        for (int i = 0; i < N; i++) u0[i] = u[i];
+        vnorm = nm_norm(u, N);
+        const double inv = 1.0 / vnorm;
+        for (int i = 0; i < N; i++) x[i] = u[i] * inv;
+        for (int i = 0; i < N; i++) {
+            double t = 0.0;
+            for (int32_t j = R[i]; j < R[i + 1]; j++) t += (V ? (double)V[j] : 1.0) * x[C[j]];
+            u[i] = t;
+        }
+        double s1 = 0.0, s2 = 0.0;
+        for (int i = 0; i < N; i++) {
+            const double d1 = u[i] - u0[i], d2 = u[i] + u0[i];
+            s1 += d1 * d1;
+            s2 += d2 * d2;
+        }
+        err1 = sqrt(s1);
+        err2 = sqrt(s2);
+        iter++;
+    }
+    for (int i = 0; i < N; i++) ec[i] = raw ? u[i] : x[i];
+    if (eigenvalue) *eigenvalue = vnorm;
+    if (residual) *residual = err1 < err2 ? err1 : err2;
+    free(u); free(u0); free(x);
+    return iter;
+}

@@ -84,6 +84,9 @@ def lib():
         L.or_maslov.restype = ct.c_int64
         L.or_maslov_round_size.argtypes = [ct.c_int64]
         L.or_maslov_round_size.restype = ct.c_int64
+        L.or_eigen_centrality.argtypes = [_i32p, _i32p, _vp, ct.c_int, ct.c_int, _f64p,
+                                          ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
+        L.or_eigen_centrality.restype = ct.c_int
         _lib = L
     return _lib
 
@@ -226,6 +229,19 @@ def maslov(R, C, V, seed, attempts):
 
 def maslov_round_size(M):
     return int(lib().or_maslov_round_size(M))
+
+
+def eigen_centrality(R, C, V=None, raw=False):
+    """Power-method eigenvector centrality of the CUEC tools (or_eigen_centrality):
+    returns (ec, eigenvalue, iterations, residual)."""
+    R = np.ascontiguousarray(R, np.int32)
+    C = np.ascontiguousarray(C, np.int32)
+    N = len(R) - 1
+    Vc = None if V is None else np.ascontiguousarray(V, np.float32)
+    ec = np.zeros(max(N, 1), np.float64)
+    lam, res = ct.c_double(0.0), ct.c_double(0.0)
+    it = lib().or_eigen_centrality(R, C, _ptr(Vc), N, int(bool(raw)), ec, ct.byref(lam), ct.byref(res))
+    return ec[:N], lam.value, int(it), res.value
 
 
 # ------------------------------------------------------------ compiled reference

@@ -164,3 +164,58 @@ def test_maslov_bit_exact(ctx, weighted):
     rows = np.repeat(np.arange(n), np.diff(R2))
     assert not np.any(rows == C2)                    # no self loops
     assert committed > attempts // 20
+
+
+def _check_ec(ec, lam, it, ec_or, lam_or, it_or):
+    """Same step count: values agree to rounding (summation order differs);
+    a step count one apart (a borderline stop) still agrees to 1e-4."""
+    assert np.array_equal(np.isnan(ec), np.isnan(ec_or))
+    ok = ~np.isnan(ec_or)
+    if it == it_or:
+        np.testing.assert_allclose(ec[ok], ec_or[ok], rtol=1e-9, atol=1e-12 * max(1.0, np.abs(ec_or[ok]).max(initial=0)))
+        assert lam == pytest.approx(lam_or, rel=1e-12)
+    else:
+        assert abs(it - it_or) <= 1
+        np.testing.assert_allclose(ec[ok], ec_or[ok], rtol=1e-4, atol=1e-8)
+
+
+@pytest.mark.parametrize("raw", [False, True])
+def test_eigen_centrality(ctx, case, raw):
+    name, R, C, g = case
+    ec, lam, it, res = ctx.eigen_centrality(g, raw=raw)
+    ec_or, lam_or, it_or, res_or = O.eigen_centrality(R, C, raw=raw)
+    _check_ec(ec, lam, it, ec_or, lam_or, it_or)
+
+
+@pytest.mark.parametrize("raw", [False, True])
+def test_eigen_centrality_weighted(ctx, raw):
+    for R, C, V in (G.random_weighted(300, 0.05, 4), G.from_bold(900, 200, 0.25, 31, weighted=True)):
+        g = ctx.graph(R, C, V)
+        ec, lam, it, res = ctx.eigen_centrality(g, raw=raw)
+        ec_or, lam_or, it_or, res_or = O.eigen_centrality(R, C, V, raw=raw)
+        _check_ec(ec, lam, it, ec_or, lam_or, it_or)
+
+
+def test_eigen_centrality_degenerate(ctx):
+    # no edges: the second step normalises a zero vector (0 * inf = NaN in the
+    # normalised output, as in the reference); one node; isolated nodes
+    for R, C in ((np.zeros(6, np.int32), np.zeros(0, np.int32)),
+                 (np.zeros(2, np.int32), np.zeros(0, np.int32)),
+                 G.two_components_with_isolated()[:2]):
+        g = ctx.graph(R, C)
+        for raw in (False, True):
+            ec, lam, it, res = ctx.eigen_centrality(g, raw=raw)
+            ec_or, lam_or, it_or, res_or = O.eigen_centrality(R, C, raw=raw)
+            assert it == it_or
+            _check_ec(ec, lam, it, ec_or, lam_or, it_or)
+
+
+def test_eigen_centrality_subject20k(ctx):
+    # a subject graph built on the GPU (20,000 voxels, top 1% |r|)
+    from pagani import synth
+    bold = synth.bold_series(20000, 240, 20, synth.subject_seed(2, 5))
+    g, info = ctx.build_graph(bold, mode="s", value=1.0, sign="abs")
+    R, C, _ = g.to_csr()
+    ec, lam, it, res = ctx.eigen_centrality(g)
+    ec_or, lam_or, it_or, res_or = O.eigen_centrality(R, C)
+    _check_ec(ec, lam, it, ec_or, lam_or, it_or)
