@@ -320,6 +320,26 @@ def main():
         ms_fp32, _ = timed("fp32", True, max(1, args.steps), 1)
         fp32 = {"value": world * 60000.0 / ms_fp32, "unit": "subjects/min", "ms_per_step": ms_fp32}
 
+    # eigenvector centrality (the CUEC power method) on the same subject
+    # graph, outside the timed step: CUDA events around the call, after one
+    # warm-up call
+    g_ec, _ = ctx.build_graph(None, mode="s", value=SPARSITY, sign="abs", precision=args.precision,
+                              device_ptr=(bold_dev.data_ptr(), (T_LEN, N_VOX)))
+    ctx.eigen_centrality(g_ec)
+    ec_ms = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, ec_lam, ec_it, _ = ctx.eigen_centrality(g_ec)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ec_ms.append(e0.elapsed_time(e1))
+    ec_nnz = g_ec.info[1]
+    g_ec.free()
+    ec_t = float(np.median(ec_ms))
+    eigen = {"ms": ec_t, "iterations": ec_it, "eigenvalue": ec_lam,
+             "gteps": ec_nnz * ec_it / (ec_t / 1000.0) / 1e9}
+
     value = world * 60000.0 / ms_dev
     e2e = world * 60000.0 / ms_e2e
     tm = timings[-1]
@@ -354,6 +374,7 @@ def main():
         "stage_ms": {"build": {k: tm["build"][k] for k in ("ms_zscore", "ms_hist", "ms_emit", "ms_select", "ms_csr")},
                      "betweenness_and_paths": tm["bc_ms"], "newman": tm["newman_ms"]},
         "step_ms_all": all_ms,
+        "eigen_centrality": eigen,
         "clocks": clk,
     }
     if fp32:

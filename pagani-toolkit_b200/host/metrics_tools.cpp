@@ -7,6 +7,7 @@
 //   CUBFW_Lp <dir> <n_rand> <g|n|l|gn|gl|nl|gnl>  W/Lp/CUBFW_Lp/CUBFW_Lp/CUBFW_Lp_main.cpp
 //   CUBC <dir>                                U/BC/CUBC/CUBC_main.cpp
 //   Newman_Modularity <dir> <n_rand>          U/cuda_EC/cuda_EC/modularity_GPU.cu:532-717
+//   CUEC <dir>                                U/CUEC/CUEC/CUEC_unweighted.cu:216-312, W/CUEC/weighted-net.cu:220-331
 //   Maslov <file.csr>                         W/Maslov/Maslov/Maslov_main.cpp
 //   SmallWorldProperty <dir>                  W/SmallWorldProperty/SmallWorldProperty.cpp
 // Random surrogates use pg_maslov with 2*M attempts (the reference's
@@ -229,6 +230,37 @@ int main(int argc, char** argv)
             pg_graph_free(r);
         }
         if (log) fclose(log);
+        pg_graph_free(g);
+    }
+    pg_destroy(ctx);
+    return 0;
+}
+#elif defined(PG_TOOL_EC)
+// Eigenvector centrality of every .csr in the directory: <stem>_ec.nm and
+// <stem>_evalue.txt.  A file with weights is treated as the weighted tool
+// does (weights used, y = A x of the last step written); a binary file as
+// the unweighted tool does (the normalised vector written).
+int main(int argc, char** argv)
+{
+    if (argc < 2) { fprintf(stderr, "Input format: CUEC dir_for_csr\n"); return 1; }
+    pg_ctx* ctx = pgio::open_ctx();
+    for (const std::string& fn : csr_files(argv[1])) {
+        std::string path = pgio::join(argv[1], fn);
+        printf("\ncalculating eigenvalue centrality for %s ...\n", path.c_str());
+        Csr c;
+        if (!load(path, c)) continue;
+        const bool weighted = !c.V.empty();
+        pg_graph* g = pgio::upload(ctx, c);
+        std::vector<double> ec(c.n());
+        double lam = 0.0, res = 0.0;
+        int32_t it = 0;
+        pgio::check(ctx, pg_eigen_centrality(ctx, g, weighted ? 1 : 0, ec.data(), &lam, &it, &res),
+                    "pg_eigen_centrality");
+        printf("Iterations:\t%d\tresidual:\t%g\teigenvalue:\t%g\t\n", it, res, lam);
+        std::vector<float> ecf(ec.begin(), ec.end());
+        pgio::write_nm(pgio::stem(path) + "_ec.nm", ecf);
+        // the unweighted tool returns the eigenvalue as float before printing it
+        pgio::write_values(pgio::stem(path) + "_evalue.txt", {weighted ? lam : (double)(float)lam});
         pg_graph_free(g);
     }
     pg_destroy(ctx);

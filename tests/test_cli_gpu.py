@@ -131,3 +131,29 @@ def test_weighted_tools_and_smallworld(subject_dir, tmp_path):
     lam = float(open(glob.glob(str(gdir / "*_lambda.txt"))[0]).read())
     gam = float(open(glob.glob(str(gdir / "*_gamma.txt"))[0]).read())
     assert float(open(sw[0]).read()) == pytest.approx(gam / lam, rel=1e-5)
+
+
+def write_csr(path, R, C, V=None):
+    with open(path, "wb") as f:
+        np.array([len(R)], np.int32).tofile(f)
+        np.asarray(R, np.int32).tofile(f)
+        np.array([len(C)], np.int32).tofile(f)
+        np.asarray(C, np.int32).tofile(f)
+        if V is not None:
+            np.array([len(V)], np.int32).tofile(f)
+            np.asarray(V, np.float32).tofile(f)
+
+
+def test_cuec_unweighted_and_weighted(tmp_path):
+    from tests import graphs as G
+    Ru, Cu, _ = G.from_bold(500, 150, 0.3, 41)
+    Rw, Cw, Vw = G.from_bold(450, 150, 0.25, 42, weighted=True)
+    write_csr(tmp_path / "bin_500.csr", Ru, Cu)
+    write_csr(tmp_path / "wei_450.csr", Rw, Cw, Vw)
+    run("CUEC", tmp_path)
+    for stem, (R, C, V) in (("bin_500", (Ru, Cu, None)), ("wei_450", (Rw, Cw, Vw))):
+        ec = read_nm(tmp_path / f"{stem}_ec.nm")
+        ec_or, lam_or, it_or, _ = O.eigen_centrality(R, C, V, raw=V is not None)
+        np.testing.assert_allclose(ec, ec_or.astype(np.float32), rtol=1e-5, atol=1e-7)
+        lam = float(open(tmp_path / f"{stem}_evalue.txt").read().split()[0])
+        assert lam == pytest.approx(lam_or, rel=1e-5)
