@@ -86,6 +86,15 @@ bool write_cormat(const std::string& path, const float* r, long long M1)
     return f.good();
 }
 
+bool read_nm(const std::string& path, std::vector<float>& x)
+{
+    std::ifstream f(path, std::ios::binary);
+    int32_t n = 0;
+    if (!f.read((char*)&n, 4) || n < 0) return false;
+    x.resize((size_t)n);
+    return (bool)f.read((char*)x.data(), (std::streamsize)(4 * (size_t)n));
+}
+
 bool write_values(const std::string& path, const std::vector<double>& v)
 {
     std::ofstream f(path);
@@ -99,37 +108,112 @@ bool read_first_value(const std::string& path, double& v)
     return (bool)(f >> v);
 }
 
+namespace {
+template <class T>
+T swapped(T v)
+{
+    unsigned char* b = (unsigned char*)&v;
+    for (size_t i = 0; i < sizeof(T) / 2; i++) std::swap(b[i], b[sizeof(T) - 1 - i]);
+    return v;
+}
+template <class T>
+T field(const unsigned char* hdr, int at, bool swap)
+{
+    T v;
+    memcpy(&v, hdr + at, sizeof(T));
+    return swap ? swapped(v) : v;
+}
+template <class T>
+bool read_values(std::ifstream& f, long long total, bool swap, std::vector<float>& out)
+{
+    std::vector<T> b((size_t)total);
+    if (!f.read((char*)b.data(), (std::streamsize)(sizeof(T) * total))) return false;
+    for (long long q = 0; q < total; q++) out[q] = (float)(swap ? swapped(b[q]) : b[q]);
+    return true;
+}
+}  // namespace
+
 bool read_nifti(const std::string& path, Nifti& img, std::string& err)
 {
     std::ifstream f(path, std::ios::binary);
     if (!f.good()) { err = "cannot open " + path; return false; }
-    short hdr[176];
+    unsigned char hdr[352];
     if (!f.read((char*)hdr, 352)) { err = path + ": truncated NIfTI header"; return false; }
-    img.dims[0] = hdr[21];
-    img.dims[1] = hdr[22];
-    img.dims[2] = hdr[23];
-    img.T = hdr[24] > 0 ? hdr[24] : 1;
-    img.datatype = hdr[35];
-    img.bitpix = hdr[36];
+    memcpy(img.header, hdr, 352);
+    // sizeof_hdr is 348; read in the other byte order it marks a big-endian file
+    const bool swap = field<int32_t>(hdr, 0, false) != 348 && field<int32_t>(hdr, 0, true) == 348;
+    img.swapped = swap;
+    img.dims[0] = field<int16_t>(hdr, 42, swap);
+    img.dims[1] = field<int16_t>(hdr, 44, swap);
+    img.dims[2] = field<int16_t>(hdr, 46, swap);
+    const int16_t t = field<int16_t>(hdr, 48, swap);
+    img.T = t > 0 ? t : 1;
+    img.datatype = field<int16_t>(hdr, 70, swap);
+    img.bitpix = field<int16_t>(hdr, 72, swap);
+    // the data starts at vox_offset (352 when there are no extensions)
+    const float vox_offset = field<float>(hdr, 108, swap);
+    const long long at = vox_offset >= 352.0f ? (long long)vox_offset : 352;
+    img.vox_offset = at;
+    const float slope = field<float>(hdr, 112, swap), inter = field<float>(hdr, 116, swap);
     const long long V = (long long)img.dims[0] * img.dims[1] * img.dims[2];
     if (V <= 0) { err = path + ": empty volume"; return false; }
     const long long total = V * img.T;
     img.data.resize((size_t)total);
-    if (img.datatype == 2 || img.bitpix == 8) {          // uint8 (masks)
-        std::vector<unsigned char> b((size_t)total);
-        if (!f.read((char*)b.data(), total)) { err = path + ": truncated data"; return false; }
-        for (long long q = 0; q < total; q++) img.data[q] = (float)b[q];
-    } else if (img.bitpix == 32) {                        // float32
-        if (!f.read((char*)img.data.data(), 4 * total)) { err = path + ": truncated data"; return false; }
-    } else if (img.bitpix == 64) {                        // float64
-        std::vector<double> b((size_t)total);
-        if (!f.read((char*)b.data(), 8 * total)) { err = path + ": truncated data"; return false; }
-        for (long long q = 0; q < total; q++) img.data[q] = (float)b[q];
-    } else {
-        err = path + ": data type is neither uint8, float nor double";
+    f.seekg(at);
+    bool ok;
+    if (img.datatype == 2 || (img.datatype == 0 && img.bitpix == 8)) ok = read_values<uint8_t>(f, total, false, img.data);
+    else if (img.datatype == 4) ok = read_values<int16_t>(f, total, swap, img.data);
+    else if (img.datatype == 8) ok = read_values<int32_t>(f, total, swap, img.data);
+    else if (img.datatype == 16 || (img.datatype == 0 && img.bitpix == 32)) ok = read_values<float>(f, total, swap, img.data);
+    else if (img.datatype == 64 || (img.datatype == 0 && img.bitpix == 64)) ok = read_values<double>(f, total, swap, img.data);
+    else {
+        err = path + ": data type is not uint8, int16, int32, float32 or float64";
         return false;
     }
+    if (!ok) { err = path + ": truncated data"; return false; }
+    // NIfTI value scaling, when the header asks for one
+    if (slope != 0.0f && (slope != 1.0f || inter != 0.0f))
+        for (float& v : img.data) v = v * slope + inter;
     return true;
+}
+
+bool write_nifti_like(const std::string& path, const Nifti& like, const std::vector<float>& vol)
+{
+    unsigned char hdr[352];
+    memcpy(hdr, like.header, 352);
+    auto put16 = [&](int at, int16_t v) {
+        if (like.swapped) v = swapped(v);
+        memcpy(hdr + at, &v, 2);
+    };
+    auto putf = [&](int at, float v) {
+        if (like.swapped) v = swapped(v);
+        memcpy(hdr + at, &v, 4);
+    };
+    put16(70, 16);   // float32
+    put16(72, 32);
+    if (like.vox_offset != 352) {
+        // the output carries no extensions: the data follows the header
+        putf(108, 352.0f);
+        memset(hdr + 348, 0, 4);
+    }
+    {
+        const float slope = field<float>(like.header, 112, like.swapped);
+        const float inter = field<float>(like.header, 116, like.swapped);
+        if (slope != 0.0f && (slope != 1.0f || inter != 0.0f)) {   // the values are written unscaled
+            putf(112, 0.0f);
+            putf(116, 0.0f);
+        }
+    }
+    std::ofstream f(path, std::ios::binary);
+    f.write((const char*)hdr, 352);
+    if (like.swapped) {
+        std::vector<float> b(vol.size());
+        for (size_t q = 0; q < vol.size(); q++) b[q] = swapped(vol[q]);
+        f.write((const char*)b.data(), (std::streamsize)(4 * b.size()));
+    } else {
+        f.write((const char*)vol.data(), (std::streamsize)(4 * vol.size()));
+    }
+    return f.good();
 }
 
 std::vector<std::string> list_dir(const std::string& dir, const std::string& ext, const std::string& skip)

@@ -22,6 +22,7 @@ bool read_csr(const std::string& path, Csr& g, std::string& err);
 bool write_csr(const std::string& path, const Csr& g);
 // .nm: int32 N, float[N] (e.g. U/Degree/Degree/Degree.cpp:99-101).
 bool write_nm(const std::string& path, const std::vector<float>& x);
+bool read_nm(const std::string& path, std::vector<float>& x);
 // .modu: int32 N, int32 label[N] (U/cuda_EC/cuda_EC/modularity_GPU.cu:653-655).
 bool write_modu(const std::string& path, const std::vector<int32_t>& labels);
 // .cormat: int32 M1 (low 32 bits of the long long, CorMat.cpp:291), float[M1].
@@ -33,14 +34,25 @@ bool read_first_value(const std::string& path, double& v);
 
 // NIfTI-1 as the reference reads it (CorMat.cpp:138-235): 352-byte header
 // viewed as short[176]: dims hdr[21..23], time points hdr[24], datatype
-// hdr[35], bitpix hdr[36]; data at byte 352.
+// hdr[35], bitpix hdr[36]; data at byte 352.  Beyond the reference, the data
+// is read at vox_offset (files with extensions), scl_slope/scl_inter are
+// applied when they are not the identity, big-endian files are byte-swapped,
+// and int16/int32 volumes are accepted; the files the reference reads give
+// the same values.
 struct Nifti {
     int dims[3] = {0, 0, 0};
     int T = 1;
     int datatype = 0, bitpix = 0;
+    long long vox_offset = 352;
+    bool swapped = false;             // big-endian file
+    unsigned char header[352] = {};   // as read
     std::vector<float> data;  // voxel-major per volume: data[t * V + k]
 };
 bool read_nifti(const std::string& path, Nifti& img, std::string& err);
+// A float32 volume with the header of `like` (datatype 16, bitpix 32), as
+// ConvertNII writes it (ConvertNII.cpp:139-157): header bytes kept, except
+// that a header with extensions or value scaling is written without them.
+bool write_nifti_like(const std::string& path, const Nifti& like, const std::vector<float>& vol);
 
 // Files in `dir` with extension `ext` (".csr", ".nii", ...), sorted by name;
 // `skip` is left out (the mask).

@@ -3,12 +3,13 @@ reported before any GPU work (CPU only)."""
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "pagani-toolkit_b200", "bin")
 TOOLS = ["CUCorMat", "CUCorMat_weighted", "Degree", "Cp", "BFS_MulCPU", "CUBFW_Lp", "CUBC",
-         "Newman_Modularity", "CUEC", "Maslov", "SmallWorldProperty"]
+         "Newman_Modularity", "CUEC", "Maslov", "SmallWorldProperty", "ConvertNII"]
 
 
 @pytest.mark.parametrize("tool", TOOLS)
@@ -24,3 +25,84 @@ def test_cucormat_rejects_bad_threshold_type(tmp_path):
     exe = os.path.join(BIN, "CUCorMat")
     p = subprocess.run([exe, str(tmp_path), "0.5", "n", "n", "x", "0.3"], capture_output=True, text=True, timeout=60)
     assert p.returncode == 1 and "threshold type error" in p.stderr
+
+
+# ---------------------------------------------------------------- ConvertNII
+def _write_nm(path, x):
+    with open(path, "wb") as f:
+        np.array([len(x)], np.int32).tofile(f)
+        np.asarray(x, np.float32).tofile(f)
+
+
+def _convert_expected(mask_flat, hdr, x, cut):
+    """The reference's output: the mask's 352 header bytes with datatype 16 and
+    bitpix 32 (ConvertNII.cpp:139-142), then float32 values in mask voxels."""
+    out = bytearray(hdr)
+    out[70:74] = np.array([16, 32], np.int16).tobytes()
+    vol = np.zeros(mask_flat.size, np.float32)
+    vol[mask_flat >= cut] = x
+    return bytes(out) + vol.tobytes()
+
+
+def _flat(mask_xyz):
+    return np.asarray(mask_xyz).transpose(2, 1, 0).reshape(-1)   # x fastest
+
+
+@pytest.mark.parametrize("code,cut", [(2, None), (16, 0.4)])
+def test_convertnii_matches_reference_layout(tmp_path, code, cut):
+    from tests.nifti import write_nifti
+    rng = np.random.default_rng(3)
+    mask = (rng.random((5, 4, 3)) > 0.5).astype(np.uint8) if code == 2 else rng.random((5, 4, 3)).astype(np.float32)
+    write_nifti(tmp_path / "mask.nii", mask, code)
+    flat = _flat(mask).astype(np.float32)
+    c = 0.5 if cut is None else cut
+    n = int((flat >= c).sum())
+    d = tmp_path / "nm"
+    d.mkdir()
+    x = rng.standard_normal(n).astype(np.float32)
+    _write_nm(d / "subj_deg.nm", x)
+    _write_nm(d / "bad_cp.nm", x[:-1])            # wrong length: skipped and logged
+    (d / "notes.nmx").write_bytes(b"x")            # other extensions are ignored
+    args = [os.path.join(BIN, "ConvertNII"), str(d), str(tmp_path / "mask.nii")] + ([] if cut is None else [str(cut)])
+    p = subprocess.run(args, capture_output=True, text=True, timeout=60, cwd=tmp_path)
+    assert p.returncode == 0, p.stderr
+    hdr = (tmp_path / "mask.nii").read_bytes()[:352]
+    assert (d / "subj_deg.nii").read_bytes() == _convert_expected(flat, hdr, x, c)
+    assert not (d / "bad_cp.nii").exists()
+    assert "bad_cp.nm" in (tmp_path / "BNA_time_log").read_text()
+
+
+def test_convertnii_robust_masks(tmp_path):
+    """Big-endian mask, a mask with a header extension, a mask with value
+    scaling: the voxels and values land as for the plain mask."""
+    from tests.nifti import write_nifti
+    rng = np.random.default_rng(5)
+    m = (rng.random((6, 5, 2)) > 0.4).astype(np.float32)
+    n = int(m.sum())
+    x = rng.standard_normal(n).astype(np.float32)
+    flat = _flat(m)
+    want = np.zeros(flat.size, np.float32)
+    want[flat >= 0.5] = x
+    variants = {
+        "big": dict(endian=">"),
+        "ext": dict(extension=b"\x01\x00\x00\x00" + bytes(12)),
+        "scaled": dict(slope=2.0, inter=0.0),    # stored 0.5 reads as 1.0
+    }
+    for name, kw in variants.items():
+        d = tmp_path / name
+        d.mkdir()
+        stored = m / 2 if name == "scaled" else m
+        write_nifti(d / "mask.nii", stored, 16, **kw)
+        _write_nm(d / "v.nm", x)
+        p = subprocess.run([os.path.join(BIN, "ConvertNII"), str(d), str(d / "mask.nii")], capture_output=True,
+                           text=True, timeout=60, cwd=d)
+        assert p.returncode == 0, p.stderr
+        raw = (d / "v.nii").read_bytes()
+        endian = ">" if name == "big" else "<"
+        import struct
+        assert struct.unpack_from(endian + "hh", raw, 70) == (16, 32)
+        assert struct.unpack_from(endian + "f", raw, 108)[0] == 352.0
+        if name == "scaled":
+            assert struct.unpack_from("<ff", raw, 112) == (0.0, 0.0)
+        got = np.frombuffer(raw[352:], np.dtype(np.float32).newbyteorder(endian))
+        np.testing.assert_array_equal(got, want)

@@ -157,3 +157,29 @@ def test_cuec_unweighted_and_weighted(tmp_path):
         np.testing.assert_allclose(ec, ec_or.astype(np.float32), rtol=1e-5, atol=1e-7)
         lam = float(open(tmp_path / f"{stem}_evalue.txt").read().split()[0])
         assert lam == pytest.approx(lam_or, rel=1e-5)
+
+
+def test_cucormat_robust_nifti_inputs(tmp_path):
+    """The same subject stored big-endian, with a header extension, and as
+    halved values with scl_slope 2: CUCorMat writes byte-identical graphs."""
+    N, T, shape = 400, 120, (10, 8, 5)
+    bold = synth.bold_series(N, T, 10, 4242)
+    mask = np.zeros(shape, np.uint8)
+    flat = np.zeros(np.prod(shape), np.uint8)
+    flat[:N] = 1
+    mask[:] = flat.reshape(shape[2], shape[1], shape[0]).transpose(2, 1, 0)
+    vol = volume_from_series(bold, shape)
+    variants = {"plain": {}, "big": dict(endian=">"), "ext": dict(extension=b"\x01\x00\x00\x00" + bytes(28)),
+                "scaled": dict(slope=2.0)}
+    out = {}
+    for name, kw in variants.items():
+        d = tmp_path / name
+        d.mkdir()
+        write_nifti(d / "mask.nii", mask, 2, **({"endian": kw["endian"]} if "endian" in kw else {}))
+        write_nifti(d / "subj01.nii", vol / 2 if name == "scaled" else vol, 16, **kw)
+        run("CUCorMat", d, 0.5, "n", "n", "s", 2)
+        f = glob.glob(str(d / f"subj01_{N}_spa2.000%_cor*.csr"))
+        assert len(f) == 1
+        out[name] = open(f[0], "rb").read()
+    for name in variants:
+        assert out[name] == out["plain"], name
