@@ -203,6 +203,15 @@ pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_above, int3
 pg_status pg_eigen_centrality(pg_ctx* ctx, const pg_graph* g, int32_t raw, double* ec, double* eigenvalue,
                               int32_t* iterations, double* residual);
 
+/* Participation coefficient from module labels: PC_CPU
+ * (W/PC_CPU/PC_CPU/main.cpp:100-174), float arithmetic in the reference's
+ * order (bit-identical).  module: host float[n] labels 1..K (the _modu.nm
+ * file); edges count their weight (1 in a graph without weights).
+ * pc, pc_norm: host float[n] (PC, and PC / ((K-1)/K) unless K = 1);
+ * n_modules = K (optional). */
+pg_status pg_participation(pg_ctx* ctx, const pg_graph* g, const float* module, float* pc, float* pc_norm,
+                           int32_t* n_modules);
+
 /* Maslov-Sneppen degree-preserving rewiring: Maslov/Rewire (U/cuda_EC/cuda_EC/
  * Maslov.cpp:8-109) and Maslov_weighted_1 (W/Maslov/Maslov/Maslov.cpp:106-196).
  * `attempts` swap attempts from a seeded counter-based generator, in rounds

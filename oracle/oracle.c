@@ -756,3 +756,42 @@ int or_eigen_centrality(const int32_t* R, const int32_t* C, const float* V, int 
     free(u); free(u0); free(x);
     return iter;
 }
+
+/* --------------------------------------------- participation coefficient */
+/* PC_CPU (W/PC_CPU/PC_CPU/main.cpp:100-174), float arithmetic in the same
+ * order: strength s_i = sum of the row's weights (row order), per-module
+ * weight sums in row order, PC_i = 1 - sum_m (w_im / s_i)^2 over modules
+ * 1..K in order (0 when s_i = 0); normalised = PC / ((K-1)/K) unless K = 1.
+ * module: float labels 1..K per node (the _modu.nm file).  V null: weight 1.
+ * Labels below 1 are skipped (the reference would write outside its array). */
+int or_participation(const int32_t* R, const int32_t* C, const float* V, int N, const float* module,
+                     float* pc, float* pc_norm)
+{
+    int K = 0;
+    for (int i = 0; i < N; i++)
+        if ((int)module[i] > K) K = (int)module[i];
+    float* within = (float*)calloc((size_t)(K > 0 ? K : 1), sizeof(float));
+    for (int i = 0; i < N; i++) {
+        float deg = 0.0f;
+        for (int32_t j = R[i]; j < R[i + 1]; j++) deg += V ? V[j] : 1.0f;
+        if (deg == 0.0f) {
+            pc[i] = 0.0f;
+            continue;
+        }
+        memset(within, 0, sizeof(float) * (size_t)(K > 0 ? K : 1));
+        for (int32_t j = R[i]; j < R[i + 1]; j++) {
+            const int m = (int)module[C[j]];
+            if (m >= 1) within[m - 1] += V ? V[j] : 1.0f;
+        }
+        float sum = 0.0f;
+        for (int m = 0; m < K; m++) {
+            const float t = within[m] / deg;
+            sum += t * t;
+        }
+        pc[i] = 1.0f - sum;
+    }
+    const float mx = K != 1 ? (float)(K - 1) / (float)K : 1.0f;
+    for (int i = 0; i < N; i++) pc_norm[i] = K != 1 ? pc[i] / mx : pc[i];
+    free(within);
+    return K;
+}

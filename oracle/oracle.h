@@ -47,6 +47,8 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
                   int64_t attempts, int32_t* R_out, int32_t* C_out, float* V_out);
 int     or_eigen_centrality(const int32_t* R, const int32_t* C, const float* V, int N, int raw,
                             double* ec, double* eigenvalue, double* residual);
+int     or_participation(const int32_t* R, const int32_t* C, const float* V, int N, const float* module,
+                         float* pc, float* pc_norm);
 
 #ifdef __cplusplus
 }

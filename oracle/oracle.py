@@ -87,6 +87,8 @@ def lib():
         L.or_eigen_centrality.argtypes = [_i32p, _i32p, _vp, ct.c_int, ct.c_int, _f64p,
                                           ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
         L.or_eigen_centrality.restype = ct.c_int
+        L.or_participation.argtypes = [_i32p, _i32p, _vp, ct.c_int, _f32p, _f32p, _f32p]
+        L.or_participation.restype = ct.c_int
         _lib = L
     return _lib
 
@@ -364,3 +366,17 @@ class Ref:
         d = np.zeros((N, N), np.float32)
         self._weighted.ref_bfw(R, C, V, N, block, d)
         return d
+
+
+def participation(R, C, V, module):
+    """PC_CPU's participation coefficient (or_participation): returns
+    (pc, pc_normalised, n_modules), float32."""
+    R = np.ascontiguousarray(R, np.int32)
+    C = np.ascontiguousarray(C, np.int32)
+    N = len(R) - 1
+    Vc = None if V is None else np.ascontiguousarray(V, np.float32)
+    mod = np.ascontiguousarray(module, np.float32)
+    pc = np.zeros(max(N, 1), np.float32)
+    pn = np.zeros(max(N, 1), np.float32)
+    K = lib().or_participation(R, C, _ptr(Vc), N, mod, pc, pn)
+    return pc[:N], pn[:N], int(K)

@@ -8,10 +8,13 @@
 //   CUBC <dir>                                U/BC/CUBC/CUBC_main.cpp
 //   Newman_Modularity <dir> <n_rand>          U/cuda_EC/cuda_EC/modularity_GPU.cu:532-717
 //   CUEC <dir>                                U/CUEC/CUEC/CUEC_unweighted.cu:216-312, W/CUEC/weighted-net.cu:220-331
+//   PC_CPU <dir>                              W/PC_CPU/PC_CPU/main.cpp:8-205
 //   Maslov <file.csr>                         W/Maslov/Maslov/Maslov_main.cpp
 //   SmallWorldProperty <dir>                  W/SmallWorldProperty/SmallWorldProperty.cpp
 // Random surrogates use pg_maslov with 2*M attempts (the reference's
 // Rewire count, Maslov.cpp:19) and a seed from PAGANI_SEED.
+#include <dirent.h>
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -261,6 +264,51 @@ int main(int argc, char** argv)
         pgio::write_nm(pgio::stem(path) + "_ec.nm", ecf);
         // the unweighted tool returns the eigenvalue as float before printing it
         pgio::write_values(pgio::stem(path) + "_evalue.txt", {weighted ? lam : (double)(float)lam});
+        pg_graph_free(g);
+    }
+    pg_destroy(ctx);
+    return 0;
+}
+#elif defined(PG_TOOL_PC)
+// Participation coefficient of every X.csr in the directory (names holding
+// ".csr"; the first ".csr" is cut to form X) whose module file X_modu.nm
+// (float labels) exists: X_pc.nm and X_pc.nm_Normalized.nm.
+int main(int argc, char** argv)
+{
+    if (argc != 2 && argc != 3) {
+        fprintf(stderr, "No Directory Input\nInput format: PC_CPU dir_for_csr_and_modu\n");
+        return 1;
+    }
+    std::vector<std::string> names;
+    if (DIR* dp = opendir(argv[1])) {
+        while (dirent* e = readdir(dp)) {
+            std::string nm = e->d_name;
+            const size_t pos = nm.find(".csr");
+            if (pos != std::string::npos) names.push_back(nm.replace(pos, 4, ""));
+        }
+        closedir(dp);
+    } else {
+        printf("can't open %s\n", argv[1]);
+        return 1;
+    }
+    std::sort(names.begin(), names.end());
+    pg_ctx* ctx = pgio::open_ctx();
+    for (const std::string& x : names) {
+        const std::string base = pgio::join(argv[1], x);
+        printf("calculate participant coefficient of %s.csr\n\n", base.c_str());
+        Csr c;
+        if (!load(base + ".csr", c)) continue;
+        std::vector<float> mod;
+        if (!pgio::read_nm(base + "_modu.nm", mod) || (int)mod.size() != c.n()) {
+            printf("%s_modu.nm not found!\n", base.c_str());
+            continue;
+        }
+        pg_graph* g = pgio::upload(ctx, c);
+        std::vector<float> pc(c.n()), pn(c.n());
+        int32_t K = 0;
+        pgio::check(ctx, pg_participation(ctx, g, mod.data(), pc.data(), pn.data(), &K), "pg_participation");
+        pgio::write_nm(base + "_pc.nm", pc);
+        pgio::write_nm(base + "_pc.nm_Normalized.nm", pn);
         pg_graph_free(g);
     }
     pg_destroy(ctx);

@@ -28,7 +28,7 @@ EXPORTS = [
     "pg_launch_count", "pg_graph_from_csr", "pg_graph_info", "pg_graph_to_csr", "pg_graph_free",
     "pg_build_opts_default", "pg_build_graph", "pg_sparsity_edges", "pg_correlation_packed",
     "pg_degree", "pg_clustering", "pg_paths", "pg_betweenness", "pg_bfs_sigma", "pg_fw_paths",
-    "pg_fw_batched", "pg_newman", "pg_eigen_centrality", "pg_maslov", "pg_maslov_round_size", "pg_smallworld",
+    "pg_fw_batched", "pg_newman", "pg_eigen_centrality", "pg_participation", "pg_maslov", "pg_maslov_round_size", "pg_smallworld",
     "pg_clustering_noalloc", "pg_clustering_noalloc_max_nodes",
 ]
 
@@ -102,6 +102,7 @@ def lib():
         L.pg_fw_batched.argtypes = [vp, P(vp), i32, vp, vp, vp, vp]
         L.pg_newman.argtypes = [vp, vp, i32, vp, P(dbl), P(i32), LOG_FN, vp]
         L.pg_eigen_centrality.argtypes = [vp, vp, i32, vp, P(dbl), P(i32), P(dbl)]
+        L.pg_participation.argtypes = [vp, vp, vp, vp, vp, P(i32)]
         L.pg_maslov.argtypes = [vp, vp, ct.c_uint64, i64, P(vp), P(i64)]
         L.pg_maslov_round_size.argtypes = [i64]
         L.pg_maslov_round_size.restype = i64
@@ -325,6 +326,17 @@ class Context:
         self._check(lib().pg_eigen_centrality(self.h, g.h, int(bool(raw)), _p(ec), ct.byref(lam), ct.byref(it),
                                               ct.byref(res)))
         return ec[:n], lam.value, it.value, res.value
+
+    def participation(self, g, module):
+        """Participation coefficient (pg_participation): module = float labels
+        1..K per node; returns (pc, pc_normalised, K), float32."""
+        n = g.info[0]
+        mod = np.ascontiguousarray(module, np.float32)
+        pc = np.empty(max(n, 1), np.float32)
+        pn = np.empty(max(n, 1), np.float32)
+        K = ct.c_int32()
+        self._check(lib().pg_participation(self.h, g.h, _p(mod), _p(pc), _p(pn), ct.byref(K)))
+        return pc[:n], pn[:n], K.value
 
     def maslov(self, g, seed, attempts):
         h = ct.c_void_p()

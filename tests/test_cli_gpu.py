@@ -183,3 +183,20 @@ def test_cucormat_robust_nifti_inputs(tmp_path):
         out[name] = open(f[0], "rb").read()
     for name in variants:
         assert out[name] == out["plain"], name
+
+
+def test_pc_cpu_tool(tmp_path):
+    from tests import graphs as G
+    R, C, V = G.from_bold(500, 150, 0.25, 43, weighted=True)
+    n = len(R) - 1
+    mod = np.random.default_rng(7).integers(1, 12, n).astype(np.float32)
+    write_csr(tmp_path / "s1.csr", R, C, V)
+    with open(tmp_path / "s1_modu.nm", "wb") as f:
+        np.array([n], np.int32).tofile(f)
+        mod.tofile(f)
+    write_csr(tmp_path / "s2.csr", R, C, V)      # no module file: skipped
+    run("PC_CPU", tmp_path)
+    pc_or, pn_or, _ = O.participation(R, C, V, mod)
+    assert np.array_equal(read_nm(tmp_path / "s1_pc.nm"), pc_or)
+    assert np.array_equal(read_nm(tmp_path / "s1_pc.nm_Normalized.nm"), pn_or)
+    assert not (tmp_path / "s2_pc.nm").exists()

@@ -219,3 +219,37 @@ def test_eigen_centrality_subject20k(ctx):
     ec, lam, it, res = ctx.eigen_centrality(g)
     ec_or, lam_or, it_or, res_or = O.eigen_centrality(R, C)
     _check_ec(ec, lam, it, ec_or, lam_or, it_or)
+
+
+def test_participation_bit_exact(ctx):
+    rng = np.random.default_rng(12)
+    cases = [G.from_bold(600, 150, 0.25, 61, weighted=True), G.random_weighted(250, 0.05, 3),
+             G.two_components_with_isolated()]
+    for R, C, V in cases:
+        n = len(R) - 1
+        g = ctx.graph(R, C, V)
+        for K in (1, 5, 40):
+            mod = rng.integers(1, K + 1, n).astype(np.float32)
+            pc, pn, k = ctx.participation(g, mod)
+            pc_or, pn_or, k_or = O.participation(R, C, V, mod)
+            assert k == k_or
+            assert np.array_equal(pc, pc_or) and np.array_equal(pn, pn_or)
+
+
+def test_participation_many_modules_and_newman_labels(ctx):
+    # every node its own module (the per-warp sums no longer fit shared
+    # memory), and the labels of a Newman partition
+    R, C, V = G.from_bold(9000, 60, 0.6, 62, weighted=True)
+    n = len(R) - 1
+    g = ctx.graph(R, C, V)
+    mod = np.arange(1, n + 1, dtype=np.float32)
+    pc, pn, k = ctx.participation(g, mod)
+    pc_or, pn_or, _ = O.participation(R, C, V, mod)
+    assert k == n and np.array_equal(pc, pc_or) and np.array_equal(pn, pn_or)
+    Rb, Cb, _ = G.bench_like()
+    gb = ctx.graph(Rb, Cb)
+    labels, Q, nm = ctx.newman(gb)
+    mod = labels.astype(np.float32)
+    pc, pn, k = ctx.participation(gb, mod)
+    pc_or, pn_or, _ = O.participation(Rb, Cb, None, mod)
+    assert k == nm and np.array_equal(pc, pc_or) and np.array_equal(pn, pn_or)

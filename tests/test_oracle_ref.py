@@ -53,3 +53,32 @@ def test_ring_chord_betweenness_is_twice_the_undirected_value(ref):
     bc = ref.betweenness(R, C)
     assert np.allclose(bc, [15, 5, 2, 5, 15, 5, 2, 5])
     assert np.allclose(O.brandes(R, C), bc)
+
+
+def test_participation_matches_reference_pc_cpu(tmp_path):
+    """The reference's PC_CPU program (oracle/_ref/ref_pc_cpu) on real files.
+    It joins paths with a backslash, so the inputs are given names of the form
+    'd\\<stem>.csr' in its working directory, beside a directory 'd' that it
+    lists."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(O.__file__), "_ref", "ref_pc_cpu")
+    if not os.path.exists(exe):
+        pytest.skip("ref_pc_cpu not built")
+    from tests import graphs as G
+    R, C, V = G.from_bold(300, 150, 0.25, 77, weighted=True)
+    n = len(R) - 1
+    mod = np.random.default_rng(0).integers(1, 9, n).astype(np.float32)
+    (tmp_path / "d").mkdir()
+    (tmp_path / "d" / "x.csr").write_bytes(b"")
+    with open(tmp_path / "d\\x.csr", "wb") as f:
+        for a in (np.array([len(R)], np.int32), R, np.array([len(C)], np.int32), C, np.array([len(V)], np.int32), V):
+            np.asarray(a).tofile(f)
+    with open(tmp_path / "d\\x_modu.nm", "wb") as f:
+        np.array([n], np.int32).tofile(f)
+        mod.tofile(f)
+    subprocess.run([exe, "d"], cwd=tmp_path, capture_output=True, timeout=60)
+    pc_ref = np.fromfile(tmp_path / "d\\x_pc.nm", np.int32)[1:].view(np.float32)
+    pn_ref = np.fromfile(tmp_path / "d\\x_pc.nm_Normalized.nm", np.int32)[1:].view(np.float32)
+    pc, pn, K = O.participation(R, C, V, mod)
+    assert np.array_equal(pc, pc_ref) and np.array_equal(pn, pn_ref)
