@@ -189,6 +189,18 @@ typedef void (*pg_log_fn)(const char* line, void* user);
 pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_above, int32_t* labels,
                     double* Q, int32_t* n_modules, pg_log_fn log, void* user);
 
+/* The weighted Newman tool (W/Newman_Modularity_GPU/CUmodularity): the same
+ * partition with edge values in the power iteration's products only; the
+ * degrees, M and Q stay binary as in the reference.  The tool reads the values
+ * by position in the value array of the file's graph: a sub-graph above
+ * gpu_rule_above nodes multiplies its q-th edge by value q
+ * (modularity_GPU.cu:135), a smaller one every term of its i-th row by value
+ * i (Modularity_CPU.cpp:261); positions past the array count 0.  weights_of
+ * holds that array (null: g itself; the tool passes the original graph when
+ * it partitions a random surrogate).  Labels and Q as pg_newman. */
+pg_status pg_newman_weighted(pg_ctx* ctx, const pg_graph* g, const pg_graph* weights_of, int32_t gpu_rule_above,
+                             int32_t* labels, double* Q, int32_t* n_modules, pg_log_fn log, void* user);
+
 /* Eigenvector centrality by the power method of the CUEC tools:
  * Lead_Vector_GPU in U/CUEC/CUEC/CUEC_unweighted.cu:61-214 (edges count 1)
  * and W/CUEC/weighted-net.cu:55-218 (a graph with weights uses them).  The

@@ -456,6 +456,14 @@ typedef struct {
     double *v, *v0, *vv, *sumBG;
     int last_iter;
     double last_res;
+    /* weighted tool (W/Newman_Modularity_GPU/CUmodularity): weights by
+     * position in the full graph's value array, indexed by the sub-graph's
+     * edge (groups above the GPU rule, modularity_GPU.cu:135) or by its row
+     * (the CPU Lead_Vector, Modularity_CPU.cpp:261); positions past the array
+     * count 0 */
+    const float* Vw;
+    int64_t wn;
+    int wmode;   /* 0 none, 1 by row, 2 by edge */
 } nm_state;
 
 static double nm_norm(const double* x, int n)
@@ -481,7 +489,14 @@ static double nm_lead_vector(nm_state* st, const int32_t* sR, const int32_t* sC,
         for (int i = 0; i < n; i++) v_k += v0[i] * (R[AD[i] + 1] - R[AD[i]]);
         for (int i = 0; i < n; i++) {
             double t = 0;
-            for (int32_t j = sR[i]; j < sR[i + 1]; j++) t += vv[sC[j]];
+            if (st->wmode == 0) {
+                for (int32_t j = sR[i]; j < sR[i + 1]; j++) t += vv[sC[j]];
+            } else if (st->wmode == 2) {
+                for (int32_t j = sR[i]; j < sR[i + 1]; j++) t += vv[sC[j]] * (j < st->wn ? (double)st->Vw[j] : 0.0);
+            } else {
+                const double w = i < st->wn ? (double)st->Vw[i] : 0.0;
+                for (int32_t j = sR[i]; j < sR[i + 1]; j++) t += vv[sC[j]] * w;
+            }
             t -= v_k / 2 / M * (R[AD[i] + 1] - R[AD[i]]) + (sumBG[i] - beta) * v0[i];
             v[i] = t;
         }
@@ -501,12 +516,13 @@ static double nm_lead_vector(nm_state* st, const int32_t* sR, const int32_t* sC,
     return (v[mx] * v0[mx] > 0) ? vNorm : -vNorm;
 }
 
-int or_newman(const int32_t* R, const int32_t* C, int N, int gpu_rule_above,
-              int32_t* labels, double* Qout, int* n_modules, int* n_rounds)
+static int newman_core(const int32_t* R, const int32_t* C, const float* Vw, int64_t wn, int N, int gpu_rule_above,
+                       int32_t* labels, double* Qout, int* n_modules, int* n_rounds)
 {
     int M = R[N] / 2;
     nm_state st;
     st.N = N; st.M = M; st.R = R;
+    st.Vw = Vw; st.wn = wn; st.wmode = 0;
     st.v = (double*)calloc((size_t)N + 1, sizeof(double));
     st.v0 = (double*)calloc((size_t)N + 1, sizeof(double));
     st.vv = (double*)calloc((size_t)N + 1, sizeof(double));
@@ -538,6 +554,7 @@ int or_newman(const int32_t* R, const int32_t* C, int N, int gpu_rule_above,
             int n = NumG;
             for (int i = 0; i < n; i++)
                 st.sumBG[i] = (sR[i + 1] - sR[i]) - (R[AD[i] + 1] - R[AD[i]]) * (double)innerM / 2 / M;
+            st.wmode = Vw ? (n > gpu_rule_above ? 2 : 1) : 0;
             double lambda = nm_lead_vector(&st, sR, sC, n, AD, 0.0);
             double shift_below = (n > gpu_rule_above) ? -0.01 : 0.0;
             if (lambda < shift_below) lambda += nm_lead_vector(&st, sR, sC, n, AD, -lambda);
@@ -576,6 +593,21 @@ int or_newman(const int32_t* R, const int32_t* C, int N, int gpu_rule_above,
     free(st.v); free(st.v0); free(st.vv); free(st.sumBG);
     free(Adjust); free(AD); free(sR); free(sC); free(G);
     return 0;
+}
+
+int or_newman(const int32_t* R, const int32_t* C, int N, int gpu_rule_above,
+              int32_t* labels, double* Qout, int* n_modules, int* n_rounds)
+{
+    return newman_core(R, C, NULL, 0, N, gpu_rule_above, labels, Qout, n_modules, n_rounds);
+}
+
+/* The weighted Newman tool: the same partition with the weights Vw[0..wn) in
+ * the power iteration's products only (degrees, M and Q stay binary, as in
+ * the reference). */
+int or_newman_weighted(const int32_t* R, const int32_t* C, const float* Vw, int64_t wn, int N, int gpu_rule_above,
+                       int32_t* labels, double* Qout, int* n_modules, int* n_rounds)
+{
+    return newman_core(R, C, Vw, wn, N, gpu_rule_above, labels, Qout, n_modules, n_rounds);
 }
 
 /* --------------------------------------------------------- Maslov rewiring */

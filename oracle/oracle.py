@@ -89,6 +89,9 @@ def lib():
         L.or_eigen_centrality.restype = ct.c_int
         L.or_participation.argtypes = [_i32p, _i32p, _vp, ct.c_int, _f32p, _f32p, _f32p]
         L.or_participation.restype = ct.c_int
+        L.or_newman_weighted.argtypes = [_i32p, _i32p, _f32p, ct.c_int64, ct.c_int, ct.c_int, _i32p,
+                                         ct.POINTER(ct.c_double), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]
+        L.or_newman_weighted.restype = ct.c_int
         _lib = L
     return _lib
 
@@ -220,6 +223,19 @@ def newman(R, C, gpu_rule_above=25000):
     return labels, Q.value, nm.value, nr.value
 
 
+def newman_weighted(R, C, Vw, gpu_rule_above=25000):
+    """The weighted Newman tool's partition (or_newman_weighted); Vw is the
+    value array the tool indexes by position."""
+    R = np.ascontiguousarray(R, np.int32)
+    C = np.ascontiguousarray(C, np.int32)
+    Vw = np.ascontiguousarray(Vw, np.float32)
+    N = len(R) - 1
+    labels = np.zeros(max(N, 1), np.int32)
+    Q, nm, nr = ct.c_double(), ct.c_int(), ct.c_int()
+    lib().or_newman_weighted(R, C, Vw, len(Vw), N, gpu_rule_above, labels, ct.byref(Q), ct.byref(nm), ct.byref(nr))
+    return labels[:N], Q.value, nm.value
+
+
 def maslov(R, C, V, seed, attempts):
     N = len(R) - 1
     Ro = np.empty(N + 1, np.int32)
@@ -281,6 +297,10 @@ class Ref:
         x = self._wcormat
         x.ref_wform_graph_r.argtypes = [_f32p, ct.c_int, ct.c_float, _i32p, _i32p, _f32p, ct.c_longlong]
         x.ref_wform_graph_r.restype = ct.c_longlong
+        wn = os.path.join(REF_DIR, "libref_wnewman.so")
+        self._wnewman = _load(wn) if os.path.exists(wn) else None
+        if self._wnewman is not None:
+            self._wnewman.ref_wpartition.argtypes = [_i32p, _i32p, _f32p, ct.c_int, _i32p]
 
     @staticmethod
     def available() -> bool:
@@ -353,6 +373,17 @@ class Ref:
         N = len(R) - 1
         res = np.zeros(N, np.int32)
         self._metrics.ref_partition(R, C, N, res)
+        return res
+
+    def wpartition(self, R, C, V):
+        """The weighted tool's CPU Partition (every group on the CPU rule);
+        None when libref_wnewman.so was not built."""
+        if self._wnewman is None:
+            return None
+        N = len(R) - 1
+        res = np.zeros(N, np.int32)
+        self._wnewman.ref_wpartition(np.ascontiguousarray(R, np.int32), np.ascontiguousarray(C, np.int32),
+                                     np.ascontiguousarray(V, np.float32), N, res)
         return res
 
     def cp2(self, R, C, V):

@@ -158,6 +158,36 @@ long long ref_wform_graph_r(float* cormat, int N, float thr, int* R, int* C, flo
     return nnz;
 }
 }
+#elif defined(REF_GROUP_WNEWMAN)
+/* W/Newman_Modularity_GPU/CUmodularity/Modularity_CPU.cpp: the weighted
+ * tool's CPU Partition, which reads the edge values through the global Vf
+ * (defined by modularity_GPU.cu in the tool, here by the caller). */
+void Partition(int* R, int* C, int* Result);
+extern long long N, Ntemp, seed;
+extern double *v, *v0, *verr, *vv, *sumBG;
+float* Vf;
+#include <new>
+void* operator new[](size_t sz) { void* p = std::malloc(sz + 64); if (!p) throw std::bad_alloc(); return p; }
+void operator delete[](void* p) noexcept { std::free(p); }
+void operator delete[](void* p, size_t) noexcept { std::free(p); }
+void Setup(int) {}
+void Start(int) {}
+void Stop(int) {}
+void Reset(int) {}
+double GetElapsedTime(int) { return 0.0; }
+void PrintTime(int) {}
+void Maslov(int*, int*, int*, int*, int, int) {}
+extern "C" {
+void ref_wpartition(int* R, int* C, float* V, int n, int* result)
+{
+    N = n;
+    std::vector<double> a(n), b(n), c(n), d(n), e(n);
+    v = a.data(); v0 = b.data(); vv = c.data(); verr = d.data(); sumBG = e.data();
+    seed = 0;
+    Vf = V;
+    Partition(R, C, result);
+}
+}
 #else
 #error "select a reference group with -DREF_GROUP_<NAME>"
 #endif

@@ -120,12 +120,31 @@ struct Group {
     double* v;      // current vector (the reference's v0 entering a step)
     double* v0;     // previous vector; holds y inside a step
     int ng;
+    // weighted tool: the full graph's values by position, taken at the
+    // group's row (wmode 1) or edge (wmode 2) index; wmode 0: no weights
+    const float* wv;
+    long long wn;
+    int wmode;
 };
+
+// value at position i of the weight array, 0 past its end
+__device__ __forceinline__ double wpos(const float* wv, long long wn, long long i)
+{
+    return i < wn ? (double)wv[i] : 0.0;
+}
+
+// one product term of the weighted tool's SpMV (vv[C[j]] * Vf[..]); the
+// product is rounded on its own, as in the reference
+template <int WM>
+__device__ __forceinline__ double wterm(double x, double w)
+{
+    return WM == 0 ? x : __dmul_rn(x, w);
+}
 
 // Rows of y = B v for the rows this warp owns, L lanes per row.  Each lane
 // keeps four independent gathers in flight; the L partial sums meet in a
 // shuffle tree.  Returns this lane's share of |y|^2.
-template <int L>
+template <int L, int WM>
 __device__ __forceinline__ double spmv_rows(const Group& g, double c, double beta, int lane, int wid, int nwarp)
 {
     constexpr int RPW = 32 / L;
@@ -139,15 +158,16 @@ __device__ __forceinline__ double spmv_rows(const Group& g, double c, double bet
             q = g.sR[p] + sub;
             q1 = g.sR[p + 1];
         }
+        const double wr = WM == 1 ? wpos(g.wv, g.wn, p) : 1.0;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         for (; q + 3 * L < q1; q += 4 * L) {
             const int c0 = g.sC[q], c1 = g.sC[q + L], c2 = g.sC[q + 2 * L], c3 = g.sC[q + 3 * L];
-            s0 += g.v[c0];
-            s1 += g.v[c1];
-            s2 += g.v[c2];
-            s3 += g.v[c3];
+            s0 += wterm<WM>(g.v[c0], WM == 2 ? wpos(g.wv, g.wn, q) : wr);
+            s1 += wterm<WM>(g.v[c1], WM == 2 ? wpos(g.wv, g.wn, q + L) : wr);
+            s2 += wterm<WM>(g.v[c2], WM == 2 ? wpos(g.wv, g.wn, q + 2 * L) : wr);
+            s3 += wterm<WM>(g.v[c3], WM == 2 ? wpos(g.wv, g.wn, q + 3 * L) : wr);
         }
-        for (; q < q1; q += L) s0 += g.v[g.sC[q]];
+        for (; q < q1; q += L) s0 += wterm<WM>(g.v[g.sC[q]], WM == 2 ? wpos(g.wv, g.wn, q) : wr);
         double s = (s0 + s1) + (s2 + s3);
         for (int o = L / 2; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (act && sub == 0) {
@@ -170,22 +190,33 @@ __device__ __forceinline__ int lanes_per_row(int ng, long long edges, int nthr)
     return L;
 }
 
-__device__ __forceinline__ double spmv(int L, const Group& g, double c, double beta, int lane, int wid, int nwarp)
+template <int WM>
+__device__ __forceinline__ double spmv_w(int L, const Group& g, double c, double beta, int lane, int wid, int nwarp)
 {
     switch (L) {
-    case 1: return spmv_rows<1>(g, c, beta, lane, wid, nwarp);
-    case 2: return spmv_rows<2>(g, c, beta, lane, wid, nwarp);
-    case 4: return spmv_rows<4>(g, c, beta, lane, wid, nwarp);
-    case 8: return spmv_rows<8>(g, c, beta, lane, wid, nwarp);
-    case 16: return spmv_rows<16>(g, c, beta, lane, wid, nwarp);
-    default: return spmv_rows<32>(g, c, beta, lane, wid, nwarp);
+    case 1: return spmv_rows<1, WM>(g, c, beta, lane, wid, nwarp);
+    case 2: return spmv_rows<2, WM>(g, c, beta, lane, wid, nwarp);
+    case 4: return spmv_rows<4, WM>(g, c, beta, lane, wid, nwarp);
+    case 8: return spmv_rows<8, WM>(g, c, beta, lane, wid, nwarp);
+    case 16: return spmv_rows<16, WM>(g, c, beta, lane, wid, nwarp);
+    default: return spmv_rows<32, WM>(g, c, beta, lane, wid, nwarp);
     }
+}
+
+// W: the kernel is built for the weighted tool (the unweighted build keeps
+// none of the weighted code and its register budget)
+template <bool W>
+__device__ __forceinline__ double spmv(int L, const Group& g, double c, double beta, int lane, int wid, int nwarp)
+{
+    return (!W || g.wmode == 0) ? spmv_w<0>(L, g, c, beta, lane, wid, nwarp)
+           : g.wmode == 1 ? spmv_w<1>(L, g, c, beta, lane, wid, nwarp)
+                          : spmv_w<2>(L, g, c, beta, lane, wid, nwarp);
 }
 
 // The reference's Lead_Vector (Modularity_CPU.cpp:224-298) with two
 // reductions per step; `Red` supplies barrier + sum over the threads that own
 // the group.  `ph` alternates the reduction buffers.
-template <class Red>
+template <class Red, bool W>
 __device__ double lead_vector(const Group& g, int M, double beta, double err_sq, int* iters, double* resid, Red& red,
                               int tid, int nthr, int lane, int wid, int nwarp, int& ph)
 {
@@ -205,7 +236,7 @@ __device__ double lead_vector(const Group& g, int M, double beta, double err_sq,
     int iter = 0;
     while (s1 > err_sq && s2 > err_sq && iter < MAX_ITER) {
         const double c = vk * 0.5 / (double)M;   // vk / 2 / M, the same double
-        x[0] = spmv(L, g, c, beta, lane, wid, nwarp);
+        x[0] = spmv<W>(L, g, c, beta, lane, wid, nwarp);
         red.sum(x, 1, ph);
         vnorm = sqrt(x[0]);
         double e1 = 0.0, e2 = 0.0;
@@ -380,6 +411,8 @@ struct Inputs {
     int M;
     int gpu_rule_above;
     double err_sq;           // largest double whose square root is at most EPSILON
+    const float* wv;         // weighted tool: value array taken by position (null: unweighted)
+    long long wn;
     double* out;             // per group: lambda, it0, res0, it1, res1, subP, subN, shifted
 };
 
@@ -395,20 +428,23 @@ __device__ __forceinline__ Group global_group(const Inputs& in, int gi)
     g.sumBG = in.sumBG + p0;
     g.v = in.v + p0;
     g.v0 = in.v0 + p0;
+    g.wv = in.wv;
+    g.wn = in.wn;
+    g.wmode = in.wv ? (g.ng > in.gpu_rule_above ? 2 : 1) : 0;
     return g;
 }
 
 // Both passes of Sub_Partition for one group.
-template <class Red>
+template <class Red, bool W>
 __device__ void sub_partition(const Group& g, const Inputs& in, int gi, Red& red, int tid, int nthr, int lane,
                               int wid, int nwarp, bool writer)
 {
     int it0, it1 = 0, ph = 0;
     double r0, r1 = 0.0;
-    double lam = lead_vector(g, in.M, 0.0, in.err_sq, &it0, &r0, red, tid, nthr, lane, wid, nwarp, ph);
+    double lam = lead_vector<Red, W>(g, in.M, 0.0, in.err_sq, &it0, &r0, red, tid, nthr, lane, wid, nwarp, ph);
     const double below = g.ng > in.gpu_rule_above ? -LAMBDA : 0.0;
     const bool shifted = lam < below;
-    if (shifted) lam += lead_vector(g, in.M, -lam, in.err_sq, &it1, &r1, red, tid, nthr, lane, wid, nwarp, ph);
+    if (shifted) lam += lead_vector<Red, W>(g, in.M, -lam, in.err_sq, &it1, &r1, red, tid, nthr, lane, wid, nwarp, ph);
     double x[3] = {0.0, 0.0, 0.0};
     for (int p = tid; p < g.ng; p += nthr) {
         x[0] += g.v[p] > 0.0;
@@ -520,10 +556,15 @@ struct Team {
     int L;                // lanes per row
     int nslices;          // 0: unsliced
     int n, r0, nown;
+    int e0;               // the group's index of the first own edge
+    const float* wv;      // weighted tool, as in Group
+    long long wn;
+    int wmode;
 };
 
 // own rows of y = B v from the sliced matrix, written to ydst[own row]
-template <int L>
+// (WM = 1: every term of a row times the weight at the row's position)
+template <int L, int WM>
 __device__ __forceinline__ void team_slices(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
                                             int nwarp)
 {
@@ -533,16 +574,21 @@ __device__ __forceinline__ void team_slices(const Team& tm, double* ydst, double
     for (int s = wid; s < tm.nslices; s += nwarp) {
         const int b = tm.soff[s], it = (tm.soff[s + 1] - b) >> 5;
         const uint16_t* __restrict__ cs = tm.cols + b + lane;
+        double w = 1.0;
+        if (WM == 1) {
+            const int slot = s * RPS + lane / L;
+            w = slot < tm.nown ? wpos(tm.wv, tm.wn, tm.r0 + (int)tm.perm[slot]) : 0.0;
+        }
         double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
         int j = 0;
         for (; j + 3 < it; j += 4) {
             const int c0 = cs[32 * j], c1 = cs[32 * j + 32], c2 = cs[32 * j + 64], c3 = cs[32 * j + 96];
-            a0 += rep[c0];
-            a1 += rep[c1];
-            a2 += rep[c2];
-            a3 += rep[c3];
+            a0 += wterm<WM>(rep[c0], w);
+            a1 += wterm<WM>(rep[c1], w);
+            a2 += wterm<WM>(rep[c2], w);
+            a3 += wterm<WM>(rep[c3], w);
         }
-        for (; j < it; j++) a0 += rep[cs[32 * j]];
+        for (; j < it; j++) a0 += wterm<WM>(rep[cs[32 * j]], w);
         double y = (a0 + a1) + (a2 + a3);
         for (int o = L / 2; o; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
         const int slot = s * RPS + lane / L;
@@ -554,7 +600,8 @@ __device__ __forceinline__ void team_slices(const Team& tm, double* ydst, double
 }
 
 // own rows of y = B v from the CSR in global memory, L lanes per row
-template <int L>
+// (WM = 1: weight at the row's position; WM = 2: at the edge's position)
+template <int L, int WM>
 __device__ __forceinline__ void team_rows(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
                                           int nwarp)
 {
@@ -570,15 +617,17 @@ __device__ __forceinline__ void team_rows(const Team& tm, double* ydst, double c
             q = tm.oR[lp] + sub;
             q1 = tm.oR[lp + 1];
         }
+        const double wr = WM == 1 ? wpos(tm.wv, tm.wn, tm.r0 + lp) : 1.0;
+        const long long qe = tm.e0;   // own edge q is the group's edge e0 + q
         double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         for (; q + 3 * L < q1; q += 4 * L) {
             const int c0 = cols[q], c1 = cols[q + L], c2 = cols[q + 2 * L], c3 = cols[q + 3 * L];
-            s0 += rep[c0];
-            s1 += rep[c1];
-            s2 += rep[c2];
-            s3 += rep[c3];
+            s0 += wterm<WM>(rep[c0], WM == 2 ? wpos(tm.wv, tm.wn, qe + q) : wr);
+            s1 += wterm<WM>(rep[c1], WM == 2 ? wpos(tm.wv, tm.wn, qe + q + L) : wr);
+            s2 += wterm<WM>(rep[c2], WM == 2 ? wpos(tm.wv, tm.wn, qe + q + 2 * L) : wr);
+            s3 += wterm<WM>(rep[c3], WM == 2 ? wpos(tm.wv, tm.wn, qe + q + 3 * L) : wr);
         }
-        for (; q < q1; q += L) s0 += rep[cols[q]];
+        for (; q < q1; q += L) s0 += wterm<WM>(rep[cols[q]], WM == 2 ? wpos(tm.wv, tm.wn, qe + q) : wr);
         double y = (s0 + s1) + (s2 + s3);
         for (int o = L / 2; o; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
         if (act && sub == 0) {
@@ -588,27 +637,37 @@ __device__ __forceinline__ void team_rows(const Team& tm, double* ydst, double c
     }
 }
 
-__device__ __forceinline__ void team_spmv(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
-                                          int nwarp)
+template <int WM>
+__device__ __forceinline__ void team_spmv_w(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
+                                            int nwarp)
 {
-    if (tm.nslices > 0) {
+    if (WM != 2 && tm.nslices > 0) {   // edge weights need the CSR's edge positions
         switch (tm.L) {
-        case 1: team_slices<1>(tm, ydst, c, beta, lane, wid, nwarp); return;
-        case 2: team_slices<2>(tm, ydst, c, beta, lane, wid, nwarp); return;
-        case 4: team_slices<4>(tm, ydst, c, beta, lane, wid, nwarp); return;
-        case 8: team_slices<8>(tm, ydst, c, beta, lane, wid, nwarp); return;
-        case 16: team_slices<16>(tm, ydst, c, beta, lane, wid, nwarp); return;
-        default: team_slices<32>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 1: team_slices<1, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 2: team_slices<2, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 4: team_slices<4, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 8: team_slices<8, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        case 16: team_slices<16, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+        default: team_slices<32, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
         }
     }
     switch (tm.L) {
-    case 1: team_rows<1>(tm, ydst, c, beta, lane, wid, nwarp); return;
-    case 2: team_rows<2>(tm, ydst, c, beta, lane, wid, nwarp); return;
-    case 4: team_rows<4>(tm, ydst, c, beta, lane, wid, nwarp); return;
-    case 8: team_rows<8>(tm, ydst, c, beta, lane, wid, nwarp); return;
-    case 16: team_rows<16>(tm, ydst, c, beta, lane, wid, nwarp); return;
-    default: team_rows<32>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 1: team_rows<1, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 2: team_rows<2, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 4: team_rows<4, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 8: team_rows<8, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    case 16: team_rows<16, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
+    default: team_rows<32, WM>(tm, ydst, c, beta, lane, wid, nwarp); return;
     }
+}
+
+template <bool W>
+__device__ __forceinline__ void team_spmv(const Team& tm, double* ydst, double c, double beta, int lane, int wid,
+                                          int nwarp)
+{
+    if (!W || tm.wmode == 0) team_spmv_w<0>(tm, ydst, c, beta, lane, wid, nwarp);
+    else if (tm.wmode == 1) team_spmv_w<1>(tm, ydst, c, beta, lane, wid, nwarp);
+    else team_spmv_w<2>(tm, ydst, c, beta, lane, wid, nwarp);
 }
 
 // first index of the largest |v| over the whole copy, computed by one CTA
@@ -629,7 +688,7 @@ __device__ __forceinline__ int block_argmax_abs(Partials& s, const double* v, in
 
 // Lead_Vector (Modularity_CPU.cpp:224-298) for a team: the reference's
 // per-entry arithmetic, sums in a fixed order over all rows.
-template <class Kind>
+template <class Kind, bool W>
 __device__ double team_lead_vector(const Team& tm, const Group& gg, int M, double beta, double err_sq, int* iters,
                                    double* resid, Partials& ps, int& ph)
 {
@@ -649,7 +708,7 @@ __device__ double team_lead_vector(const Team& tm, const Group& gg, int M, doubl
     while (s1 > err_sq && s2 > err_sq && iter < MAX_ITER) {
         const double c = vk * 0.5 / (double)M;   // vk / 2 / M, the same double
         double* ybuf = Kind::kCluster ? (yb ? gg.v0 : gg.v) : tm.oy;
-        team_spmv(tm, Kind::kCluster ? ybuf + tm.r0 : ybuf, c, beta, lane, wid, nwarp);
+        team_spmv<W>(tm, Kind::kCluster ? ybuf + tm.r0 : ybuf, c, beta, lane, wid, nwarp);
         Kind::barrier();
         x1[0] = 0.0;
         for (int p = tid; p < n; p += nthr) {
@@ -790,7 +849,7 @@ __device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int3
 }
 
 // One team per group of `glist`; the cluster size is set at launch.
-template <class Kind>
+template <class Kind, bool W>
 __global__ void __launch_bounds__(TEAM_THREADS)
 k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes, uint16_t* __restrict__ slices)
 {
@@ -829,7 +888,12 @@ k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes, uint16_t* __
     const long long own_e = (long long)tm.oR[tm.nown];
     uint16_t* gcols = slices + 2 * (in.eoff[gi] + e0) + 64 * (in.goff[gi] + tm.r0);
     const size_t gspace = (size_t)(2 * own_e + 64LL * tm.nown) * 2;
-    tm.nslices = tm.n < 65535 ? team_slice(tm, gg, e0, key, soff, cols, space, gcols, gspace, &sL, &sIn) : 0;
+    tm.e0 = e0;
+    tm.wv = gg.wv;
+    tm.wn = gg.wn;
+    tm.wmode = gg.wmode;
+    tm.nslices = (tm.n < 65535 && gg.wmode != 2) ? team_slice(tm, gg, e0, key, soff, cols, space, gcols, gspace, &sL, &sIn)
+                                                  : 0;
     tm.perm = key;
     tm.soff = soff;
     tm.gcols = gg.sC + e0;
@@ -837,10 +901,10 @@ k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes, uint16_t* __
     // both passes of Sub_Partition
     int it0, it1 = 0, ph = 0;
     double res0, res1 = 0.0;
-    double lam = team_lead_vector<Kind>(tm, gg, in.M, 0.0, in.err_sq, &it0, &res0, ps, ph);
+    double lam = team_lead_vector<Kind, W>(tm, gg, in.M, 0.0, in.err_sq, &it0, &res0, ps, ph);
     const double below = gg.ng > in.gpu_rule_above ? -LAMBDA : 0.0;
     const bool shifted = lam < below;
-    if (shifted) lam += team_lead_vector<Kind>(tm, gg, in.M, -lam, in.err_sq, &it1, &res1, ps, ph);
+    if (shifted) lam += team_lead_vector<Kind, W>(tm, gg, in.M, -lam, in.err_sq, &it1, &res1, ps, ph);
     double x2[2] = {0.0, 0.0};
     for (int p = threadIdx.x; p < tm.n; p += blockDim.x) {
         x2[0] += tm.rep[p] > 0.0;
@@ -854,6 +918,7 @@ k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes, uint16_t* __
 }
 
 // large groups: the whole cooperative grid, one group per launch
+template <bool W>
 __global__ void __launch_bounds__(COOP_THREADS)
 k_nm_coop(int gi, Inputs in, double* __restrict__ part)
 {
@@ -861,7 +926,7 @@ k_nm_coop(int gi, Inputs in, double* __restrict__ part)
     red.init(part);
     Group g = global_group(in, gi);
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
-    sub_partition(g, in, gi, red, tid, nthr, threadIdx.x & 31, tid >> 5, nthr >> 5, tid == 0);
+    sub_partition<GridRed, W>(g, in, gi, red, tid, nthr, threadIdx.x & 31, tid >> 5, nthr >> 5, tid == 0);
 }
 
 // ---------------------------------------------------------------- whole grid
@@ -900,10 +965,13 @@ struct GridPart {
     const int32_t* split;    // [own row][nblk + 1] edge offsets (global edge index in the group)
     const uint16_t* c16;     // the group's columns modulo the block size
     int n, r0, nown, nblk, cb_log;
+    const float* wv;         // weighted tool, as in Group
+    long long wn;
+    int wmode;
 };
 
 // add block b's share of every own row to ypart, L lanes per row
-template <int L>
+template <int L, int WM>
 __device__ __forceinline__ void grid_rows(const GridPart& gp, int b, int lane, int wid, int nwarp)
 {
     constexpr int RPW = 32 / L;
@@ -918,34 +986,45 @@ __device__ __forceinline__ void grid_rows(const GridPart& gp, int b, int lane, i
             q = gp.split[lp * (gp.nblk + 1) + b] + sub;
             q1 = gp.split[lp * (gp.nblk + 1) + b + 1];
         }
+        const double wr = WM == 1 ? wpos(gp.wv, gp.wn, gp.r0 + lp) : 1.0;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         for (; q + 3 * L < q1; q += 4 * L) {
             const int c0 = cols[q], c1 = cols[q + L], c2 = cols[q + 2 * L], c3 = cols[q + 3 * L];
-            s0 += vb[c0];
-            s1 += vb[c1];
-            s2 += vb[c2];
-            s3 += vb[c3];
+            s0 += wterm<WM>(vb[c0], WM == 2 ? wpos(gp.wv, gp.wn, q) : wr);
+            s1 += wterm<WM>(vb[c1], WM == 2 ? wpos(gp.wv, gp.wn, q + L) : wr);
+            s2 += wterm<WM>(vb[c2], WM == 2 ? wpos(gp.wv, gp.wn, q + 2 * L) : wr);
+            s3 += wterm<WM>(vb[c3], WM == 2 ? wpos(gp.wv, gp.wn, q + 3 * L) : wr);
         }
-        for (; q < q1; q += L) s0 += vb[cols[q]];
+        for (; q < q1; q += L) s0 += wterm<WM>(vb[cols[q]], WM == 2 ? wpos(gp.wv, gp.wn, q) : wr);
         double y = (s0 + s1) + (s2 + s3);
         for (int o = L / 2; o; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
         if (act && sub == 0) gp.ypart[lp] = b == 0 ? y : gp.ypart[lp] + y;
     }
 }
 
-__device__ __forceinline__ void grid_block(int L, const GridPart& gp, int b, int lane, int wid, int nwarp)
+template <int WM>
+__device__ __forceinline__ void grid_block_w(int L, const GridPart& gp, int b, int lane, int wid, int nwarp)
 {
     switch (L) {
-    case 1: grid_rows<1>(gp, b, lane, wid, nwarp); return;
-    case 2: grid_rows<2>(gp, b, lane, wid, nwarp); return;
-    case 4: grid_rows<4>(gp, b, lane, wid, nwarp); return;
-    case 8: grid_rows<8>(gp, b, lane, wid, nwarp); return;
-    case 16: grid_rows<16>(gp, b, lane, wid, nwarp); return;
-    default: grid_rows<32>(gp, b, lane, wid, nwarp); return;
+    case 1: grid_rows<1, WM>(gp, b, lane, wid, nwarp); return;
+    case 2: grid_rows<2, WM>(gp, b, lane, wid, nwarp); return;
+    case 4: grid_rows<4, WM>(gp, b, lane, wid, nwarp); return;
+    case 8: grid_rows<8, WM>(gp, b, lane, wid, nwarp); return;
+    case 16: grid_rows<16, WM>(gp, b, lane, wid, nwarp); return;
+    default: grid_rows<32, WM>(gp, b, lane, wid, nwarp); return;
     }
 }
 
+template <bool W>
+__device__ __forceinline__ void grid_block(int L, const GridPart& gp, int b, int lane, int wid, int nwarp)
+{
+    if (!W || gp.wmode == 0) grid_block_w<0>(L, gp, b, lane, wid, nwarp);
+    else if (gp.wmode == 1) grid_block_w<1>(L, gp, b, lane, wid, nwarp);
+    else grid_block_w<2>(L, gp, b, lane, wid, nwarp);
+}
+
 // Lead_Vector (Modularity_CPU.cpp:224-298) on the whole grid
+template <bool W>
 __device__ double grid_lead_vector(const GridPart& gp, const Group& gg, int M, double beta, double err_sq, int* iters,
                                    double* resid, GridRed& red, int& ph)
 {
@@ -973,7 +1052,7 @@ __device__ double grid_lead_vector(const GridPart& gp, const Group& gg, int M, d
             const double* src = gg.v + (size_t)b * cb;
             for (int p = tid; p < len; p += nthr) gp.vblk[p] = src[p];
             __syncthreads();
-            grid_block(L, gp, b, lane, wid, nwarp);
+            grid_block<W>(L, gp, b, lane, wid, nwarp);
             __syncthreads();
         }
         double y2 = 0.0;
@@ -1019,6 +1098,7 @@ __device__ double grid_lead_vector(const GridPart& gp, const Group& gg, int M, d
     return lam;
 }
 
+template <bool W>
 __global__ void __launch_bounds__(COOP_THREADS)
 k_nm_grid(int gi, Inputs in, double* __restrict__ part, uint16_t* __restrict__ c16, int cb_log)
 {
@@ -1029,6 +1109,9 @@ k_nm_grid(int gi, Inputs in, double* __restrict__ part, uint16_t* __restrict__ c
     GridPart gp;
     gp.n = gg.ng;
     gp.cb_log = cb_log;
+    gp.wv = gg.wv;
+    gp.wn = gg.wn;
+    gp.wmode = gg.wmode;
     const int cb = 1 << cb_log;
     gp.nblk = (gp.n + cb - 1) >> cb_log;
     gp.r0 = team_split(gg.sR, gp.n, blockIdx.x, gridDim.x);
@@ -1069,10 +1152,10 @@ k_nm_grid(int gi, Inputs in, double* __restrict__ part, uint16_t* __restrict__ c
     __syncthreads();
     int it0, it1 = 0, ph = 0;
     double res0, res1 = 0.0;
-    double lam = grid_lead_vector(gp, gg, in.M, 0.0, in.err_sq, &it0, &res0, red, ph);
+    double lam = grid_lead_vector<W>(gp, gg, in.M, 0.0, in.err_sq, &it0, &res0, red, ph);
     const double below = gg.ng > in.gpu_rule_above ? -LAMBDA : 0.0;
     const bool shifted = lam < below;
-    if (shifted) lam += grid_lead_vector(gp, gg, in.M, -lam, in.err_sq, &it1, &res1, red, ph);
+    if (shifted) lam += grid_lead_vector<W>(gp, gg, in.M, -lam, in.err_sq, &it1, &res1, red, ph);
     double x[3] = {0.0, 0.0, 0.0};
     for (int lp = threadIdx.x; lp < gp.nown; lp += blockDim.x) {
         x[0] += gp.vown[lp] > 0.0;
@@ -1113,11 +1196,17 @@ __global__ void k_nm_q(const int32_t* __restrict__ R, const int32_t* __restrict_
 }
 }  // namespace
 
-extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_above, int32_t* labels, double* Q,
-                               int32_t* n_modules, pg_log_fn log, void* user)
+// The partition of pg_newman; wv (device, wn values) is the weighted tool's
+// value array, null for the unweighted tool.
+static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, long long wn, int32_t gpu_rule_above,
+                            int32_t* labels, double* Q, int32_t* n_modules, pg_log_fn log, void* user)
 {
-    if (!ctx || !g || !labels) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman: null argument");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    const bool weighted = wv != nullptr;
+    auto k_coop = weighted ? k_nm_coop<true> : k_nm_coop<false>;
+    auto k_grid = weighted ? k_nm_grid<true> : k_nm_grid<false>;
+    auto k_solo = weighted ? k_nm_team<SoloTeam, true> : k_nm_team<SoloTeam, false>;
+    auto k_clu = weighted ? k_nm_team<ClusterTeam, true> : k_nm_team<ClusterTeam, false>;
     const int n = g->n;
     const long long nnz = g->nnz;
     const int M = (int)(nnz / 2);
@@ -1145,7 +1234,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     PG_TRY(pg_wst(ctx, "nm.kdeg", (size_t)n + 1, &kdeg));
     PG_TRY(pg_wst(ctx, "nm.acc", 4, &acc));
     int per_sm = 0;
-    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nm_coop, COOP_THREADS, 0));
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop, COOP_THREADS, 0));
     if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "power iteration kernel cannot be resident");
     const int coop_grid = ctx->sm_count;   // one fat block per SM keeps the grid barrier short
     PG_TRY(pg_wst(ctx, "nm.part", (size_t)coop_grid * 8 + 8, &part));
@@ -1154,20 +1243,19 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
     uint16_t* slices;   // team CTAs whose sliced rows do not fit shared memory
     PG_TRY(pg_wst(ctx, "nm.slices", (size_t)2 * nnz + 64 * (size_t)n + 64, &slices));
     int max_cluster = CLUSTER;  // 16 needs the non-portable opt-in
-    if (cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-        cudaSuccess) {
+    if (cudaFuncSetAttribute(k_clu, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
         max_cluster = 8;
     }
     for (auto& st : ctx->side)
         if (!st) PG_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     const size_t smem_cap = std::min(SMEM_CAP, (size_t)ctx->smem_optin - 4096);
-    PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_team<SoloTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    PG_CUDA(ctx, cudaFuncSetAttribute(k_solo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     PG_CUDA(ctx,
-            cudaFuncSetAttribute(k_nm_team<ClusterTeam>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
-    PG_CUDA(ctx, cudaFuncSetAttribute(k_nm_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+            cudaFuncSetAttribute(k_clu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    PG_CUDA(ctx, cudaFuncSetAttribute(k_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     int grid_per_sm = 0;
-    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_nm_grid, COOP_THREADS, smem_cap));
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k_grid, COOP_THREADS, smem_cap));
     PG_CUDA(ctx, cudaMemsetAsync(label, 0, sizeof(int32_t) * (n + 1), ctx->stream));
 
     std::vector<int32_t> hR(n + 1), hl(n);
@@ -1246,6 +1334,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         Inputs in;
         in.goff = goff; in.eoff = eoff; in.AD = AD; in.sR = sR; in.sC = sC; in.kdeg = kdeg; in.sumBG = sumBG;
         in.v = v; in.v0 = v0; in.M = M; in.gpu_rule_above = gpu_rule_above; in.out = out; in.err_sq = err_sq;
+        in.wv = wv; in.wn = wn;
         // Shared memory of the largest CTA of group q split over c CTAs,
         // before its sliced columns
         auto team_need = [&](int q, int c) {
@@ -1327,8 +1416,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                 const int* blist = glist + bk.b;
                 const int nbytes = (int)bk.smem;
                 if (bk.c == 1) {
-                    k_nm_team<SoloTeam><<<(unsigned)(bk.e - bk.b), TEAM_THREADS, bk.smem, st>>>(blist, in, nbytes,
-                                                                                             slices);
+                    k_solo<<<(unsigned)(bk.e - bk.b), TEAM_THREADS, bk.smem, st>>>(blist, in, nbytes, slices);
                 } else {
                     cudaLaunchConfig_t cfg = {};
                     cudaLaunchAttribute attr[1];
@@ -1342,7 +1430,7 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                     cfg.stream = st;
                     cfg.attrs = attr;
                     cfg.numAttrs = 1;
-                    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_nm_team<ClusterTeam>, blist, in, nbytes, slices));
+                    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_clu, blist, in, nbytes, slices));
                 }
                 PG_LAUNCHED(ctx);
             }
@@ -1372,11 +1460,11 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
             if (cb_log && grid_per_sm >= 1) {
                 const size_t need = grid_layout(most, (ng + (1 << cb_log) - 1) >> cb_log, 1 << cb_log).need;
                 void* args[] = {(void*)&qq, (void*)&in, (void*)&part, (void*)&c16, (void*)&cb_log};
-                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_nm_grid, dim3(coop_grid), dim3(COOP_THREADS), args,
+                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_grid, dim3(coop_grid), dim3(COOP_THREADS), args,
                                                          need, ctx->stream));
             } else {
                 void* args[] = {(void*)&qq, (void*)&in, (void*)&part};
-                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_nm_coop, dim3(coop_grid), dim3(COOP_THREADS), args, 0,
+                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_coop, dim3(coop_grid), dim3(COOP_THREADS), args, 0,
                                                          ctx->stream));
             }
             PG_LAUNCHED(ctx);
@@ -1452,4 +1540,22 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
         log(line, user);
     }
     return PG_OK;
+}
+
+extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_above, int32_t* labels, double* Q,
+                               int32_t* n_modules, pg_log_fn log, void* user)
+{
+    if (!ctx || !g || !labels) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman: null argument");
+    return newman_run(ctx, g, nullptr, 0, gpu_rule_above, labels, Q, n_modules, log, user);
+}
+
+extern "C" pg_status pg_newman_weighted(pg_ctx* ctx, const pg_graph* g, const pg_graph* weights_of,
+                                        int32_t gpu_rule_above, int32_t* labels, double* Q, int32_t* n_modules,
+                                        pg_log_fn log, void* user)
+{
+    if (!ctx || !g || !labels) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman_weighted: null argument");
+    const pg_graph* w = weights_of ? weights_of : g;
+    if (!w->V) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman_weighted: the weight graph has no weights");
+    if (w->device != g->device) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman_weighted: graphs on different devices");
+    return newman_run(ctx, g, w->V, w->nnz, gpu_rule_above, labels, Q, n_modules, log, user);
 }

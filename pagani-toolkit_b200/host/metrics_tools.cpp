@@ -7,6 +7,7 @@
 //   CUBFW_Lp <dir> <n_rand> <g|n|l|gn|gl|nl|gnl>  W/Lp/CUBFW_Lp/CUBFW_Lp/CUBFW_Lp_main.cpp
 //   CUBC <dir>                                U/BC/CUBC/CUBC_main.cpp
 //   Newman_Modularity <dir> <n_rand>          U/cuda_EC/cuda_EC/modularity_GPU.cu:532-717
+//   Newman_Modularity_weighted <dir> <n_rand> W/Newman_Modularity_GPU/CUmodularity/modularity_GPU.cu:527-724
 //   CUEC <dir>                                U/CUEC/CUEC/CUEC_unweighted.cu:216-312, W/CUEC/weighted-net.cu:220-331
 //   PC_CPU <dir>                              W/PC_CPU/PC_CPU/main.cpp:8-205
 //   Maslov <file.csr>                         W/Maslov/Maslov/Maslov_main.cpp
@@ -209,27 +210,54 @@ int main(int argc, char** argv)
     return 0;
 }
 #elif defined(PG_TOOL_NEWMAN)
+// The unweighted tool writes int32 labels to X.modu; the weighted build
+// (PG_WEIGHTED_TOOL) uses the file's values and writes float labels to
+// X_modu.nm, and partitions its random surrogates with the original values
+// (modularity_GPU.cu of the weighted package, :655-662 and :114-123).
 static void log_line(const char* line, void* user) { fprintf((FILE*)user, "%s\n", line); }
 int main(int argc, char** argv)
 {
-    if (argc != 3) { fprintf(stderr, "Input format: Newman_Modularity dir_for_csr num_of_random_networks\n"); return 1; }
+#ifdef PG_WEIGHTED_TOOL
+    const char* name = "Newman_Modularity_weighted";
+#else
+    const char* name = "Newman_Modularity";
+#endif
+    if (argc != 3) { fprintf(stderr, "Input format: %s dir_for_csr num_of_random_networks\n", name); return 1; }
     const int nrand = atoi(argv[2]);
     pg_ctx* ctx = pgio::open_ctx();
     for (const std::string& fn : csr_files(argv[1])) {
         std::string path = pgio::join(argv[1], fn);
         Csr c;
         if (!load(path, c)) continue;
+#ifdef PG_WEIGHTED_TOOL
+        if (c.V.empty()) {
+            fprintf(stderr, "Your csr file %s has no weights\n", path.c_str());
+            continue;
+        }
+#endif
         pg_graph* g = pgio::upload(ctx, c);
         FILE* log = fopen((pgio::stem(path) + "_modu.txt").c_str(), "w");
         std::vector<int32_t> labels(c.n());
         double Q = 0;
         int32_t nm = 0;
+#ifdef PG_WEIGHTED_TOOL
+        pgio::check(ctx, pg_newman_weighted(ctx, g, g, 25000, labels.data(), &Q, &nm, log ? log_line : nullptr, log),
+                    "pg_newman_weighted");
+        printf("Number of Modules: %d,\tQ=%.6g\n", nm, Q);
+        pgio::write_nm(pgio::stem(path) + "_modu.nm", std::vector<float>(labels.begin(), labels.end()));
+#else
         pgio::check(ctx, pg_newman(ctx, g, 25000, labels.data(), &Q, &nm, log ? log_line : nullptr, log), "pg_newman");
         printf("Number of Modules: %d,\tQ=%.6g\n", nm, Q);
         pgio::write_modu(pgio::stem(path) + ".modu", labels);
+#endif
         for (int l = 0; l < nrand; l++) {   // the reference logs the random partitions only
             pg_graph* r = surrogate(ctx, g, (uint64_t)l);
+#ifdef PG_WEIGHTED_TOOL
+            pgio::check(ctx, pg_newman_weighted(ctx, r, g, 25000, labels.data(), &Q, &nm, log ? log_line : nullptr, log),
+                        "pg_newman_weighted");
+#else
             pgio::check(ctx, pg_newman(ctx, r, 25000, labels.data(), &Q, &nm, log ? log_line : nullptr, log), "pg_newman");
+#endif
             pg_graph_free(r);
         }
         if (log) fclose(log);

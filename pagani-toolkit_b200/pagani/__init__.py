@@ -28,7 +28,7 @@ EXPORTS = [
     "pg_launch_count", "pg_graph_from_csr", "pg_graph_info", "pg_graph_to_csr", "pg_graph_free",
     "pg_build_opts_default", "pg_build_graph", "pg_sparsity_edges", "pg_correlation_packed",
     "pg_degree", "pg_clustering", "pg_paths", "pg_betweenness", "pg_bfs_sigma", "pg_fw_paths",
-    "pg_fw_batched", "pg_newman", "pg_eigen_centrality", "pg_participation", "pg_maslov", "pg_maslov_round_size", "pg_smallworld",
+    "pg_fw_batched", "pg_newman", "pg_newman_weighted", "pg_eigen_centrality", "pg_participation", "pg_maslov", "pg_maslov_round_size", "pg_smallworld",
     "pg_clustering_noalloc", "pg_clustering_noalloc_max_nodes",
 ]
 
@@ -101,6 +101,7 @@ def lib():
         L.pg_fw_paths.argtypes = [vp, vp, vp, vp, P(dbl)]
         L.pg_fw_batched.argtypes = [vp, P(vp), i32, vp, vp, vp, vp]
         L.pg_newman.argtypes = [vp, vp, i32, vp, P(dbl), P(i32), LOG_FN, vp]
+        L.pg_newman_weighted.argtypes = [vp, vp, vp, i32, vp, P(dbl), P(i32), LOG_FN, vp]
         L.pg_eigen_centrality.argtypes = [vp, vp, i32, vp, P(dbl), P(i32), P(dbl)]
         L.pg_participation.argtypes = [vp, vp, vp, vp, vp, P(i32)]
         L.pg_maslov.argtypes = [vp, vp, ct.c_uint64, i64, P(vp), P(i64)]
@@ -311,6 +312,26 @@ class Context:
 
         cb = LOG_FN(_cb)
         self._check(lib().pg_newman(self.h, g.h, gpu_rule_above, _p(labels), ct.byref(Q), ct.byref(nm), cb, None))
+        if log is not None:
+            log.extend(lines)
+        return labels, Q.value, nm.value
+
+    def newman_weighted(self, g, weights_of=None, gpu_rule_above=25000, log=None):
+        """The weighted Newman tool's partition (pg_newman_weighted); weights_of
+        is the graph whose value array is read by position (default g)."""
+        n = g.info[0]
+        labels = np.empty(n, np.int32)
+        Q = ct.c_double()
+        nm = ct.c_int32()
+        lines = []
+
+        def _cb(line, _u):
+            lines.append(line.decode())
+
+        cb = LOG_FN(_cb)
+        w = None if weights_of is None else weights_of.h
+        self._check(lib().pg_newman_weighted(self.h, g.h, w, gpu_rule_above, _p(labels), ct.byref(Q), ct.byref(nm),
+                                             cb, None))
         if log is not None:
             log.extend(lines)
         return labels, Q.value, nm.value

@@ -9,7 +9,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "pagani-toolkit_b200", "bin")
 TOOLS = ["CUCorMat", "CUCorMat_weighted", "Degree", "Cp", "BFS_MulCPU", "CUBFW_Lp", "CUBC",
-         "Newman_Modularity", "CUEC", "PC_CPU", "Maslov", "SmallWorldProperty", "ConvertNII"]
+         "Newman_Modularity", "Newman_Modularity_weighted", "CUEC", "PC_CPU", "Maslov", "SmallWorldProperty", "ConvertNII"]
 
 
 @pytest.mark.parametrize("tool", TOOLS)

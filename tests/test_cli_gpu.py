@@ -200,3 +200,17 @@ def test_pc_cpu_tool(tmp_path):
     assert np.array_equal(read_nm(tmp_path / "s1_pc.nm"), pc_or)
     assert np.array_equal(read_nm(tmp_path / "s1_pc.nm_Normalized.nm"), pn_or)
     assert not (tmp_path / "s2_pc.nm").exists()
+
+
+def test_newman_weighted_tool(tmp_path):
+    """Newman_Modularity_weighted: float labels in X_modu.nm equal to the
+    oracle's weighted partition; a file without values is skipped."""
+    from tests import graphs as G
+    R, C, V = G.from_bold(400, 120, 0.25, 44, weighted=True)
+    write_csr(tmp_path / "w1.csr", R, C, V)
+    write_csr(tmp_path / "b1.csr", R, C)
+    run("Newman_Modularity_weighted", tmp_path, 1)
+    lab, Q, nm = O.newman_weighted(R, C, V)
+    assert np.array_equal(read_nm(tmp_path / "w1_modu.nm"), lab.astype(np.float32))
+    assert "Round:" in open(tmp_path / "w1_modu.txt").read()
+    assert not (tmp_path / "b1_modu.nm").exists()

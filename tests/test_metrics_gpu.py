@@ -253,3 +253,41 @@ def test_participation_many_modules_and_newman_labels(ctx):
     pc, pn, k = ctx.participation(gb, mod)
     pc_or, pn_or, _ = O.participation(Rb, Cb, None, mod)
     assert k == nm and np.array_equal(pc, pc_or) and np.array_equal(pn, pn_or)
+
+
+@pytest.mark.parametrize("rule", [25000, 40])
+def test_newman_weighted(ctx, rule):
+    # rule 25000: every group takes the row rule (the tool's CPU path);
+    # rule 40: groups above 40 nodes take the edge rule (its GPU path)
+    for R, C, V in (G.from_bold(700, 200, 0.25, 63, weighted=True), G.random_weighted(400, 0.04, 8)):
+        g = ctx.graph(R, C, V)
+        labels, Q, nm = ctx.newman_weighted(g, gpu_rule_above=rule)
+        lab_or, Q_or, nm_or = O.newman_weighted(R, C, V, gpu_rule_above=rule)
+        assert nm == nm_or and np.array_equal(labels, lab_or)
+        assert Q == pytest.approx(Q_or, abs=1e-12)
+
+
+def test_newman_weighted_surrogate_uses_original_values(ctx):
+    # the tool partitions a random surrogate with the original graph's value array
+    R, C, V = G.from_bold(600, 200, 0.25, 64, weighted=True)
+    g = ctx.graph(R, C, V)
+    s, _ = ctx.maslov(g, 11, len(C))
+    Rs, Cs, _ = s.to_csr()
+    labels, Q, nm = ctx.newman_weighted(s, weights_of=g)
+    lab_or, Q_or, nm_or = O.newman_weighted(Rs, Cs, V)
+    assert nm == nm_or and np.array_equal(labels, lab_or)
+
+
+def test_newman_whole_grid_groups(ctx):
+    # a 13,000-voxel graph: the first groups exceed a team's 12,288 rows and
+    # run on the whole grid, unweighted and weighted (edge rule above 5,000)
+    from pagani import synth
+    bold = synth.bold_series(13000, 120, 10, 99)
+    g, info = ctx.build_graph(bold, mode="s", value=0.5, sign="abs", weighted=True)
+    R, C, V = g.to_csr()
+    labels, Q, nm = ctx.newman(g)
+    lab_or, Q_or, nm_or, _ = O.newman(R, C)
+    assert nm == nm_or and np.array_equal(labels, lab_or)
+    labels, Q, nm = ctx.newman_weighted(g, gpu_rule_above=5000)
+    lab_or, Q_or, nm_or = O.newman_weighted(R, C, V, gpu_rule_above=5000)
+    assert nm == nm_or and np.array_equal(labels, lab_or)

@@ -55,6 +55,21 @@ def test_ring_chord_betweenness_is_twice_the_undirected_value(ref):
     assert np.allclose(O.brandes(R, C), bc)
 
 
+@pytest.mark.parametrize("seed", [3, 4, 5])
+def test_weighted_newman_matches_reference_partition(ref, seed):
+    """The weighted tool's CPU Partition (every group split on the CPU rule,
+    weights read from the value array by position) against or_newman_weighted
+    with the GPU rule never taken."""
+    R, C, V = G.from_bold(300, 100, 0.25, 600 + seed, weighted=True)
+    res = ref.wpartition(R, C, V)
+    if res is None:
+        pytest.skip("libref_wnewman.so not built")
+    n = len(R) - 1
+    lab, Q, nm = O.newman_weighted(R, C, V, gpu_rule_above=n + 1)
+    assert np.array_equal(lab, res)
+    assert nm == len(np.unique(res))
+
+
 def test_participation_matches_reference_pc_cpu(tmp_path):
     """The reference's PC_CPU program (oracle/_ref/ref_pc_cpu) on real files.
     It joins paths with a backslash, so the inputs are given names of the form
