@@ -116,6 +116,35 @@ int64_t pg_sparsity_edges(int32_t N, float s_percent);
 pg_status pg_correlation_packed(pg_ctx* ctx, const float* bold, int32_t N, int32_t T,
                                 int32_t weighted, int32_t input_on_device, float* r_packed);
 
+/* ------------------------------------------------------ cohort averaging */
+/* Subject-averaged graphs: the to_average modes of CUCorMat (argv[3] = yn,
+ * yf, bn, bf), U/CorMat/CUCorMat/CUCORMAT/CorMat.cpp:380-620 and
+ * W/CorMat/CUCorMat/CUCorMat/CorMat.cpp:386-620.  The reference adds each
+ * subject's r (n) or fisher_trans(r) (f, :35-41) into a float matrix in
+ * post_block (:775-838), divides by the subject count and applies
+ * inv_fisher_trans (:514-524).  Here the sum is FP64 and device-resident
+ * (N(N-1)/2 doubles), r is the exact FP64 r of pg_build_graph's recheck,
+ * and ln/exp are evaluated so that the averaged keys are bit-identical to
+ * the FP64 oracle's.  weighted != 0 selects the weighted tool: its range
+ * rule (-1-1e-6, 1+1e-6) and edge values V = float(average). */
+typedef struct pg_cohort pg_cohort;
+pg_status pg_cohort_create(pg_ctx* ctx, int32_t N, int32_t fisher, int32_t weighted, pg_cohort** out);
+/* Adds one subject: bold is time-major T x N float32 (host, or device when
+ * input_on_device != 0); subjects may differ in T. */
+pg_status pg_cohort_add(pg_ctx* ctx, pg_cohort* c, const float* bold, int32_t T, int32_t input_on_device);
+/* Thresholds the current average once: mode PG_THRESH_R keeps key > value
+ * (FormFullGraph, CorMat.cpp:633, signed, no 1e-6 shift in either tool's
+ * averaged branch), PG_THRESH_SPARSITY keeps the top pg_sparsity_edges(N, value)
+ * keys with the reference's tie rule (FormFullGraph_s, :693-773).  info: tau,
+ * edges, sparsity_percent and stage times. */
+pg_status pg_cohort_graph(pg_ctx* ctx, pg_cohort* c, int32_t mode, double value, pg_graph** out,
+                          pg_build_info* info);
+/* The averaged matrix as the .cormat payload (CorMat.cpp:534-543): M1 floats,
+ * packed upper triangle, row-major i < j; host buffer. */
+pg_status pg_cohort_packed(pg_ctx* ctx, pg_cohort* c, float* r_packed);
+pg_status pg_cohort_info(const pg_cohort* c, int32_t* N, int32_t* subjects);
+pg_status pg_cohort_free(pg_cohort* c);
+
 /* -------------------------------------------------------------- metrics */
 /* Degree (U/Degree/Degree/Degree.cpp:85-91) or strength for weighted graphs
  * (W/Degree/Degree/Degree.cpp:82-88).  deg: host float[n]. */

@@ -186,6 +186,130 @@ int64_t or_graph_k(const double* r, int N, int64_t k, int abs_mode, double* tau,
     return nnz;
 }
 
+/* ------------------------------------------------- cohort (subject average) */
+/* FP64 natural logarithm and exponential from +, -, *, / alone, so that this
+ * restatement and the device code round identically.  The method is the
+ * classical argument reduction (Cody & Waite, "Software Manual for the
+ * Elementary Functions", 1980):
+ *   ln x  = e ln2 + 2 atanh(s),  x = m 2^e,  m in [sqrt(1/2), sqrt(2)),
+ *           s = (m - 1) / (m + 1), atanh by its odd Taylor series to s^23
+ *           (|s| <= 0.1716: truncation below 2^-60 relative);
+ *   exp x = 2^k e^t,  k = x / ln2 rounded half away from zero,
+ *           t = (x - k ln2_hi) - k ln2_lo, e^t by its Taylor series to t^14
+ *           (|t| <= 0.347).
+ * ln2_hi keeps 42 significant bits, so k ln2_hi is exact for |k| < 2^11.
+ * The coefficients are 2/(2j+1) and 1/n!, rounded to nearest.  Measured
+ * against the C library: ln within 2 ulp, exp within 1 ulp. */
+static const double LN2_HI = 0x1.62e42fefa3800p-1, LN2_LO = 0x1.ef35793c76730p-45;
+static const double INV_LN2 = 0x1.71547652b82fep+0, SQRT2 = 0x1.6a09e667f3bcdp+0;
+static const double ATANH_C[11] = {   /* 2/3, 2/5, ..., 2/23 */
+    0x1.5555555555555p-1, 0x1.999999999999ap-2, 0x1.2492492492492p-2, 0x1.c71c71c71c71cp-3,
+    0x1.745d1745d1746p-3, 0x1.3b13b13b13b14p-3, 0x1.1111111111111p-3, 0x1.e1e1e1e1e1e1ep-4,
+    0x1.af286bca1af28p-4, 0x1.8618618618618p-4, 0x1.642c8590b2164p-4};
+static const double EXP_C[15] = {     /* 1/n!, n = 0..14 */
+    0x1.0000000000000p+0, 0x1.0000000000000p+0, 0x1.0000000000000p-1, 0x1.5555555555555p-3,
+    0x1.5555555555555p-5, 0x1.1111111111111p-7, 0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13,
+    0x1.a01a01a01a01ap-16, 0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26,
+    0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33, 0x1.93974a8c07c9dp-37};
+
+static double pow2i(int k)   /* 2^k for -1022 <= k <= 1023 */
+{
+    uint64_t u = (uint64_t)(k + 1023) << 52;
+    double d;
+    memcpy(&d, &u, 8);
+    return d;
+}
+
+double or_ln(double x)
+{
+    if (x != x || x < 0.0) return NAN;
+    if (x == 0.0) return -INFINITY;
+    if (isinf(x)) return x;
+    uint64_t u;
+    memcpy(&u, &x, 8);
+    int e = 0;
+    if (((u >> 52) & 0x7ff) == 0) {  /* subnormal: scale by 2^54 first */
+        x = x * 0x1p54;
+        memcpy(&u, &x, 8);
+        e = -54;
+    }
+    e += (int)((u >> 52) & 0x7ff) - 1023;
+    u = (u & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+    double m;
+    memcpy(&m, &u, 8);
+    if (m > SQRT2) { m = m * 0.5; e += 1; }
+    double s = (m - 1.0) / (m + 1.0);
+    double s2 = s * s;
+    double p = ATANH_C[10];
+    for (int j = 9; j >= 0; j--) p = ATANH_C[j] + s2 * p;
+    double ls = 2.0 * s + s * (s2 * p);
+    double de = (double)e;
+    return de * LN2_HI + (de * LN2_LO + ls);
+}
+
+double or_exp(double x)
+{
+    if (x != x) return x;
+    if (x > 709.782712893384) return INFINITY;
+    if (x < -745.2) return 0.0;
+    double kd = x * INV_LN2;
+    long long k = (long long)(kd + (kd >= 0.0 ? 0.5 : -0.5));
+    double dk = (double)k;
+    double t = (x - dk * LN2_HI) - dk * LN2_LO;
+    double p = EXP_C[14];
+    for (int n = 13; n >= 0; n--) p = EXP_C[n] + t * p;
+    if (k > 1023) return p * pow2i(1023) * pow2i((int)k - 1023);
+    if (k < -1022) return p * pow2i((int)k + 600) * pow2i(-600);
+    return p * pow2i((int)k);
+}
+
+/* fisher_trans, U/CorMat/CUCorMat/CUCORMAT/CorMat.cpp:35-41 (W :35-41 as
+ * fishertrans), in FP64: r == 1 becomes 1 - 1e-6, z = 0.5 ln((1+r)/(1-r)).
+ * Under the weighted range rule r may lie in (1, 1+1e-6) or (-1-1e-6, -1],
+ * where the reference's float log returns NaN; here r >= 1 is treated like
+ * r == 1 and r <= -1 gives -inf (what r == -1 gives in the reference). */
+double or_fisher(double r)
+{
+    if (r >= 1.0) r = 1.0 - 1e-6;
+    if (r <= -1.0) return -INFINITY;
+    return 0.5 * or_ln((1.0 + r) / (1.0 - r));
+}
+
+/* inv_fisher_trans, CorMat.cpp:43-49: r = (e^{2z} - 1) / (e^{2z} + 1). */
+double or_inv_fisher(double z)
+{
+    double e = or_exp(2.0 * z);
+    return (e - 1.0) / (e + 1.0);
+}
+
+/* One subject of the averaging branch of CUCorMat's main()
+ * (U CorMat.cpp:380-470, W :386-476): post_block (:775-838) adds, for every
+ * pair, r (to_average yn/bn) or fisher_trans(r) (yf/bf) to the running sum
+ * when r passes the range rule (an r that fails it adds nothing, which equals
+ * adding the 0 of range_rule: fisher(0) = 0).  Here the sum is FP64 and the
+ * subjects are added in call order. */
+void or_cohort_add(const double* z, int N, int T, int weighted, int fisher, double* acc)
+{
+    int64_t k = 0;
+    for (int i = 0; i < N; i++)
+        for (int j = i + 1; j < N; j++, k++) {
+            double r = or_pair_r(z, T, i, j, weighted);
+            acc[k] += fisher ? or_fisher(r) : r;
+        }
+}
+
+/* The end of the averaging branch (U CorMat.cpp:514-524, W :514-524): the
+ * sum divided by the subject count, then inv_fisher_trans for yf/bf.  The
+ * result is the key that FormFullGraph / FormFullGraph_s threshold (signed)
+ * and, in the weighted tool, the edge value. */
+void or_cohort_finish(const double* acc, int64_t M1, int subjects, int fisher, double* key)
+{
+    for (int64_t k = 0; k < M1; k++) {
+        double a = acc[k] / (double)subjects;
+        key[k] = fisher ? or_inv_fisher(a) : a;
+    }
+}
+
 /* ----------------------------------------------------------------- degree */
 /* U/Degree/Degree/Degree.cpp:85-91: (float)R[k+1] - R[k]; isolated count.
  * W/Degree/Degree/Degree.cpp:82-88: strength = float sum of V in CSR order. */

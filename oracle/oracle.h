@@ -49,6 +49,12 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
                   int64_t attempts, int32_t* R_out, int32_t* C_out, float* V_out);
 int     or_eigen_centrality(const int32_t* R, const int32_t* C, const float* V, int N, int raw,
                             double* ec, double* eigenvalue, double* residual);
+double  or_ln(double x);
+double  or_exp(double x);
+double  or_fisher(double r);
+double  or_inv_fisher(double z);
+void    or_cohort_add(const double* z, int N, int T, int weighted, int fisher, double* acc);
+void    or_cohort_finish(const double* acc, int64_t M1, int subjects, int fisher, double* key);
 int     or_participation(const int32_t* R, const int32_t* C, const float* V, int N, const float* module,
                          float* pc, float* pc_norm);
 

@@ -92,6 +92,11 @@ def lib():
         L.or_newman_weighted.argtypes = [_i32p, _i32p, _f32p, ct.c_int64, ct.c_int, ct.c_int, _i32p,
                                          ct.POINTER(ct.c_double), ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)]
         L.or_newman_weighted.restype = ct.c_int
+        for f in ("or_ln", "or_exp", "or_fisher", "or_inv_fisher"):
+            getattr(L, f).argtypes = [ct.c_double]
+            getattr(L, f).restype = ct.c_double
+        L.or_cohort_add.argtypes = [_f64p, ct.c_int, ct.c_int, ct.c_int, ct.c_int, _f64p]
+        L.or_cohort_finish.argtypes = [_f64p, ct.c_int64, ct.c_int, ct.c_int, _f64p]
         _lib = L
     return _lib
 
@@ -297,6 +302,9 @@ class Ref:
         x = self._wcormat
         x.ref_wform_graph_r.argtypes = [_f32p, ct.c_int, ct.c_float, _i32p, _i32p, _f32p, ct.c_longlong]
         x.ref_wform_graph_r.restype = ct.c_longlong
+        for lib_, pre in ((c, "ref_"), (x, "ref_w")):
+            getattr(lib_, pre + "cohort_add").argtypes = [_f32p, _f32p, ct.c_int, ct.c_int]
+            getattr(lib_, pre + "cohort_finish").argtypes = [_f32p, ct.c_longlong, ct.c_int, ct.c_int]
         wn = os.path.join(REF_DIR, "libref_wnewman.so")
         self._wnewman = _load(wn) if os.path.exists(wn) else None
         if self._wnewman is not None:
@@ -386,6 +394,17 @@ class Ref:
                                      np.ascontiguousarray(V, np.float32), N, res)
         return res
 
+    def cohort(self, r_subjects, N, fisher, weighted=False):
+        """The reference's averaging branch (post_block with fisher_trans, then
+        division and inv_fisher_trans) over float packed r of each subject."""
+        M1 = N * (N - 1) // 2
+        lib_, pre = (self._wcormat, "ref_w") if weighted else (self._cucormat, "ref_")
+        cm = np.zeros(max(M1, 1), np.float32)
+        for r in r_subjects:
+            getattr(lib_, pre + "cohort_add")(cm, np.ascontiguousarray(r, np.float32), N, int(fisher))
+        getattr(lib_, pre + "cohort_finish")(cm, M1, len(r_subjects), int(fisher))
+        return cm[:M1]
+
     def cp2(self, R, C, V):
         N = len(R) - 1
         cp = np.zeros(N, np.float32)
@@ -411,3 +430,24 @@ def participation(R, C, V, module):
     pn = np.zeros(max(N, 1), np.float32)
     K = lib().or_participation(R, C, _ptr(Vc), N, mod, pc, pn)
     return pc[:N], pn[:N], int(K)
+
+
+def fp64_fn(name, xs):
+    """Elementwise or_ln / or_exp / or_fisher / or_inv_fisher over an array."""
+    f = getattr(lib(), "or_" + name)
+    return np.array([f(float(x)) for x in np.asarray(xs, np.float64).ravel()], np.float64)
+
+
+def cohort_keys(bolds, fisher=False, weighted=False):
+    """Subject-averaged keys of CUCorMat's to_average branch
+    (or_cohort_add / or_cohort_finish): packed upper triangle, FP64.
+    bolds: list of (T_s, N) float32 series with the same N."""
+    N = bolds[0].shape[1]
+    M1 = N * (N - 1) // 2
+    acc = np.zeros(max(M1, 1), np.float64)
+    for b in bolds:
+        z, _ = zscore(b)
+        lib().or_cohort_add(np.ascontiguousarray(z), N, z.shape[1], int(weighted), int(fisher), acc)
+    key = np.zeros(max(M1, 1), np.float64)
+    lib().or_cohort_finish(acc, M1, len(bolds), int(fisher), key)
+    return key[:M1]

@@ -19,6 +19,8 @@ long long FormFullGraph(bool* adjacent, float* Cormat, int N, float threshold);
 float FormFullGraph_s(bool* adjacent, float* Cormat, int N, long long threshold);
 void FormCSRGraph(int* R, int* C, bool* adjacent, int N);
 void CorMat_cpu(float* Cormat, float* BOLD, int N, int L);
+void post_block(float* Cormat, float* Cormat_blocked, int N, int block_size, bool fishtran_flag);
+float inv_fisher_trans(float z);
 /* main() of CorMat.cpp references the GPU routines; they are never reached
  * through this driver. */
 int CorMat_gpu(float*, float*, int, int, int) { return -1; }
@@ -42,6 +44,26 @@ long long ref_form_graph_s(float* cormat, int N, long long k, int* R, int* C, fl
     *tau = FormFullGraph_s((bool*)adj.data(), cormat, N, k);
     FormCSRGraph(R, C, (bool*)adj.data(), N);
     return (long long)R[N];
+}
+/* One subject of the averaging branch (CorMat.cpp:466-469): post_block adds
+ * r or fisher_trans(r).  The packed r are laid out as a single N x N block
+ * (block_size = N), so post_block's block arithmetic maps (i, j) to i*N + j. */
+void ref_cohort_add(float* cormat, const float* r_packed, int N, int fisher)
+{
+    std::vector<float> blocked((size_t)N * N, 0.0f);
+    long long k = 0;
+    for (int i = 0; i < N; i++)
+        for (int j = i + 1; j < N; j++) blocked[(size_t)i * N + j] = r_packed[k++];
+    post_block(cormat, blocked.data(), N, N, fisher != 0);
+}
+/* The end of the branch, restated from main() (CorMat.cpp:514-524), with the
+ * reference's own inv_fisher_trans. */
+void ref_cohort_finish(float* cormat, long long M1, int files, int fisher)
+{
+    for (long long i = 0; i < M1; i++) {
+        cormat[i] /= files;
+        if (fisher) cormat[i] = inv_fisher_trans(cormat[i]);
+    }
 }
 }
 #elif defined(REF_GROUP_CORMAT_CPU)
@@ -144,6 +166,8 @@ void ref_bfw(int* R, int* C, float* V, int n, int block, float* dist_out)
 long long FormFullGraph(bool* adjacent, float* Cormat, int N, float threshold);
 float FormFullGraph_s(bool* adjacent, float* Cormat, int N, long long threshold);
 void FormCSRGraph(int* R, int* C, float* V, bool* adjacent, int N, float* Cormat);
+void post_block(float* Cormat, float* Cormat_blocked, int N, int block_size, bool fishtran_flag);
+float inv_fishertrans(float z);
 int CorMat_gpu(float*, float*, int, int, int) { return -1; }
 long long find_max(float*, long long) { return 0; }
 float select_GPU(float*, long long, long long) { return 0.0f; }
@@ -156,6 +180,24 @@ long long ref_wform_graph_r(float* cormat, int N, float thr, int* R, int* C, flo
     if (nnz > cap) return -1;
     FormCSRGraph(R, C, V, (bool*)adj.data(), N, cormat);
     return nnz;
+}
+/* The weighted tool's averaging branch: post_block with its range rule
+ * (-1-ep, 1+ep) and fishertrans (W CorMat.cpp:466-469, :826-852), then the
+ * division and inv_fishertrans of main() (:514-524). */
+void ref_wcohort_add(float* cormat, const float* r_packed, int N, int fisher)
+{
+    std::vector<float> blocked((size_t)N * N, 0.0f);
+    long long k = 0;
+    for (int i = 0; i < N; i++)
+        for (int j = i + 1; j < N; j++) blocked[(size_t)i * N + j] = r_packed[k++];
+    post_block(cormat, blocked.data(), N, N, fisher != 0);
+}
+void ref_wcohort_finish(float* cormat, long long M1, int files, int fisher)
+{
+    for (long long i = 0; i < M1; i++) {
+        cormat[i] /= files;
+        if (fisher) cormat[i] = inv_fishertrans(cormat[i]);
+    }
 }
 }
 #elif defined(REF_GROUP_WNEWMAN)

@@ -92,11 +92,6 @@ __global__ void k_recheck(const int2* __restrict__ band, long long nband, const 
 // Finds the m-th largest (1-based) of n uint64 keys restricted to entries
 // with (key & mask) == prefix, 8 bits per pass from the top.  State lives on
 // the device so that no pass needs the host.
-struct SelState {
-    unsigned long long prefix, mask;
-    long long m;         // rank still to find inside the current prefix
-    long long above;     // number of keys strictly above the final key
-};
 
 __global__ void k_sel_hist(const unsigned long long* __restrict__ keys, long long n, const SelState* __restrict__ st,
                            int shift, unsigned long long* __restrict__ hist)
@@ -132,7 +127,7 @@ __global__ void k_sel_pick(SelState* __restrict__ st, int shift, unsigned long l
     for (int b = 0; b < 256; b++) hist[b] = 0;
 }
 
-static pg_status radix_select(pg_ctx* ctx, const unsigned long long* keys, long long n, long long m,
+pg_status pg_radix_select(pg_ctx* ctx, const unsigned long long* keys, long long n, long long m,
                               SelState* st_dev, unsigned long long* hist)
 {
     SelState init = {0ULL, 0ULL, m, 0};
@@ -259,6 +254,14 @@ static pg_status prepare_operands(pg_ctx* ctx, const float* bold, int N, int T, 
     k_zwrite<<<g, dim3(32, 8), 0, ctx->stream>>>(dbold, N, T, z.Tp, mu, sd, z.z64, z.z32, z.zhi, z.zlo);
     PG_LAUNCHED(ctx);
     if (nzero_host) PG_TRY(pg_d2h(ctx, nzero_host, nz, sizeof(int)));
+    return PG_OK;
+}
+
+pg_status pg_zstats(pg_ctx* ctx, const float* dbold, int N, int T, double* mu, double* sd, int* nz)
+{
+    PG_CUDA(ctx, cudaMemsetAsync(nz, 0, sizeof(int), ctx->stream));
+    k_zstats<<<ceil_div(N, 256), 256, 0, ctx->stream>>>(dbold, N, T, mu, sd, nz);
+    PG_LAUNCHED(ctx);
     return PG_OK;
 }
 
@@ -471,7 +474,7 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
         int grid = std::max(1, std::min(ctx->sm_count * 8, ceil_div(n_band, 256)));
         k_band_keys<<<grid, 256, 0, ctx->stream>>>(key64, n_band, bkeys);
         PG_LAUNCHED(ctx);
-        PG_TRY(radix_select(ctx, bkeys, n_band, m, st, hist64));
+        PG_TRY(pg_radix_select(ctx, bkeys, n_band, m, st, hist64));
         SelState sh;
         PG_TRY(pg_d2h(ctx, &sh, st, sizeof sh));
         tau = dkey_inv(sh.prefix);
@@ -487,7 +490,7 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
         if ((long long)nt_host <= need) {
             tie_cut = ~0ULL;
         } else {
-            PG_TRY(radix_select(ctx, tkeys, (long long)nt_host, need, st, hist64));
+            PG_TRY(pg_radix_select(ctx, tkeys, (long long)nt_host, need, st, hist64));
             PG_TRY(pg_d2h(ctx, &sh, st, sizeof sh));
             tie_cut = ~sh.prefix;
         }

@@ -153,3 +153,17 @@ __device__ __forceinline__ void tri_tile(long long L, int nb, int& bi, int& bj)
 pg_status launch_gram_simt(pg_ctx* ctx, const ZOperands& z, int mode, const EpiParams& p);
 pg_status launch_gram_tc(pg_ctx* ctx, const ZOperands& z, int mode, const EpiParams& p);
 bool gram_tc_supported(pg_ctx* ctx, const ZOperands& z);
+
+// Radix selection state (device): the m-th largest of n uint64 keys is found
+// 8 bits per pass from the top; `prefix` holds its bits when done.
+struct SelState {
+    unsigned long long prefix, mask;
+    long long m;         // rank still to find inside the current prefix
+    long long above;     // number of keys strictly above the final key
+};
+// m-th largest (1-based) of n keys; hist is 256 device counters.
+pg_status pg_radix_select(pg_ctx* ctx, const unsigned long long* keys, long long n, long long m,
+                          SelState* st_dev, unsigned long long* hist);
+// FP64 z-score statistics of a device T x N series (k_zstats): mean and root
+// sum of squares per voxel, sd = 0 for zero-variance voxels, counted in *nz.
+pg_status pg_zstats(pg_ctx* ctx, const float* dbold, int N, int T, double* mu, double* sd, int* nz);

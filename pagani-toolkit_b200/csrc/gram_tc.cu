@@ -25,16 +25,17 @@
 // records an error, drains its own TMA copies (bounded), frees TMEM and
 // returns.
 #include "build_graph.cuh"
+#include "tma.cuh"
 #include <cuda.h>
 
 namespace {
+using namespace pg_tma;
 constexpr int BM = 128, BN = 128, KC = 64;
 constexpr int STAGES = 3;
 constexpr int THREADS = 128;
 constexpr uint32_t TILE_BYTES = BM * KC * 2;       // 16 KB per operand tile
 constexpr uint32_t STAGE_BYTES = 4 * TILE_BYTES;   // A_hi, A_lo, B_hi, B_lo
 constexpr uint32_t TMEM_COLS = 128;
-constexpr unsigned long long WAIT_NS = 2000000000ULL;  // 2 s per wait
 
 struct Ctl {
     unsigned long long full[STAGES];
@@ -46,56 +47,6 @@ struct Ctl {
 };
 
 constexpr size_t SMEM_BYTES = 1024 /*align slack*/ + STAGES * STAGE_BYTES + sizeof(Ctl) + 64;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long gtimer()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long* b, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(unsigned long long* b, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait on the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity)
-{
-    if (mbar_try(b, parity)) return true;
-    const unsigned long long t0 = gtimer();
-    while (!mbar_try(b, parity))
-        if (gtimer() - t0 > WAIT_NS) return false;
-    return true;
-}
-
-__device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-        ::"r"(smem_u32(dst)), "l"((unsigned long long)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
-        : "memory");
-}
 
 // UMMA shared-memory descriptor: K-major operand, 128-byte swizzle, rows of
 // 128 B in 8-row (1024 B) groups: LBO unused (1), SBO = 1024 B, version 1.
@@ -301,23 +252,6 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     tc_fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
-}
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn()
-{
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
-    }
-    return fn;
 }
 
 bool make_map(CUtensorMap* m, const __nv_bfloat16* base, int rows, int cols)

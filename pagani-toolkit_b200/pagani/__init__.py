@@ -30,6 +30,8 @@ EXPORTS = [
     "pg_degree", "pg_clustering", "pg_paths", "pg_betweenness", "pg_bfs_sigma", "pg_fw_paths",
     "pg_fw_batched", "pg_newman", "pg_newman_weighted", "pg_eigen_centrality", "pg_participation", "pg_maslov", "pg_maslov_round_size", "pg_smallworld",
     "pg_clustering_noalloc", "pg_clustering_noalloc_max_nodes",
+    "pg_cohort_create", "pg_cohort_add", "pg_cohort_graph", "pg_cohort_packed", "pg_cohort_info",
+    "pg_cohort_free",
 ]
 
 
@@ -111,6 +113,12 @@ def lib():
         L.pg_clustering_noalloc.argtypes = [vp, vp, i32, vp, vp, vp]
         L.pg_clustering_noalloc_max_nodes.argtypes = []
         L.pg_clustering_noalloc_max_nodes.restype = i64
+        L.pg_cohort_create.argtypes = [vp, i32, i32, i32, P(vp)]
+        L.pg_cohort_add.argtypes = [vp, vp, vp, i32, i32]
+        L.pg_cohort_graph.argtypes = [vp, vp, i32, dbl, P(vp), P(BuildInfo)]
+        L.pg_cohort_packed.argtypes = [vp, vp, vp]
+        L.pg_cohort_info.argtypes = [vp, P(i32), P(i32)]
+        L.pg_cohort_free.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -157,6 +165,54 @@ class Graph:
             self.free()
         except Exception:
             pass
+
+
+class Cohort:
+    """Subject-averaged correlation (CUCorMat's to_average modes) held on the
+    device: add() subjects, then graph() or packed()."""
+
+    def __init__(self, ctx, N, fisher=False, weighted=False):
+        self.ctx, self.N, self.weighted = ctx, N, weighted
+        h = ct.c_void_p()
+        ctx._check(lib().pg_cohort_create(ctx.h, N, int(fisher), int(weighted), ct.byref(h)))
+        self.h = h
+
+    def add(self, bold_TxN):
+        bold = np.ascontiguousarray(bold_TxN, np.float32)
+        T, N = bold.shape
+        if N != self.N:
+            raise ValueError(f"subject has {N} voxels, cohort has {self.N}")
+        self.ctx._check(lib().pg_cohort_add(self.ctx.h, self.h, _p(bold), T, 0))
+
+    @property
+    def subjects(self):
+        n, s = ct.c_int32(), ct.c_int32()
+        lib().pg_cohort_info(self.h, ct.byref(n), ct.byref(s))
+        return s.value
+
+    def graph(self, mode="r", value=0.3):
+        info = BuildInfo()
+        h = ct.c_void_p()
+        m = PG_THRESH_SPARSITY if mode in ("s", "sparsity") else PG_THRESH_R
+        self.ctx._check(lib().pg_cohort_graph(self.ctx.h, self.h, m, value, ct.byref(h), ct.byref(info)))
+        return Graph(self.ctx, h), info.as_dict()
+
+    def packed(self):
+        M1 = self.N * (self.N - 1) // 2
+        out = np.empty(max(M1, 1), np.float32)
+        self.ctx._check(lib().pg_cohort_packed(self.ctx.h, self.h, _p(out)))
+        return out[:M1]
+
+    def free(self):
+        if self.h:
+            lib().pg_cohort_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.free()
 
 
 class Context:
@@ -230,6 +286,10 @@ class Context:
         out = np.empty(max(N * (N - 1) // 2, 1), np.float32)
         self._check(lib().pg_correlation_packed(self.h, _p(bold), N, T, int(weighted), 0, _p(out)))
         return out[: N * (N - 1) // 2]
+
+    def cohort(self, N, fisher=False, weighted=False):
+        """Subject averaging (CUCorMat to_average yn/yf): a Cohort of N voxels."""
+        return Cohort(self, N, fisher, weighted)
 
     # ------------------------------------------------------------- metrics
     def degree(self, g):

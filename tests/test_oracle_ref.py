@@ -97,3 +97,25 @@ def test_participation_matches_reference_pc_cpu(tmp_path):
     pn_ref = np.fromfile(tmp_path / "d\\x_pc.nm_Normalized.nm", np.int32)[1:].view(np.float32)
     pc, pn, K = O.participation(R, C, V, mod)
     assert np.array_equal(pc, pc_ref) and np.array_equal(pn, pn_ref)
+
+
+@pytest.mark.parametrize("fisher", [False, True])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_cohort_average_matches_reference(ref, fisher, weighted):
+    """The averaging branch of CUCorMat (post_block with or without
+    fisher_trans, division by the subject count, inv_fisher_trans), run by the
+    reference's own functions over each subject's float r, against the FP64
+    cohort keys of the oracle; the r-threshold graphs agree away from the
+    threshold."""
+    N = 180
+    bolds = [synth.bold_series(N, T, 6, 700 + T) for T in (90, 70, 110)]
+    keys = O.cohort_keys(bolds, fisher=fisher, weighted=weighted)
+    rs = [O.corr_packed(O.zscore(b)[0], weighted=weighted).astype(np.float32) for b in bolds]
+    cm = ref.cohort(rs, N, fisher, weighted)
+    tol = 2e-6
+    assert np.max(np.abs(cm - keys)) < tol
+    thr = 0.2
+    R, C, _ = O.graph_r(keys, N, thr)
+    Rr, Cr = ref.graph_r(cm, N, np.float32(thr))
+    if not (np.abs(keys - thr) < tol).any():
+        assert np.array_equal(R, Rr) and np.array_equal(C, Cr)
