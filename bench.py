@@ -236,6 +236,7 @@ def main():
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-leg", action="store_true")
+    ap.add_argument("--no-cohort", action="store_true", help="skip the subject-average figure")
     ap.add_argument("--voxels", type=int, default=N_VOX,
                     help="profiling aid: a smaller subject for ncu captures (the metric is quoted at 58000)")
     args = ap.parse_args()
@@ -340,6 +341,36 @@ def main():
     eigen = {"ms": ec_t, "iterations": ec_it, "eigenvalue": ec_lam,
              "gteps": ec_nnz * ec_it / (ec_t / 1000.0) / 1e9}
 
+    # subject averaging (CUCorMat to_average yf) on the same series: the FP64
+    # Gram + Fisher accumulate of one subject, and the graph of the average
+    # (top 1%), CUDA events around each call after one warm-up add
+    cohort = None
+    if not args.no_cohort:
+        M1 = N_VOX * (N_VOX - 1) // 2
+        with ctx.cohort(N_VOX, fisher=True) as c:
+            c.add(device_ptr=(bold_dev.data_ptr(), (T_LEN, N_VOX)))
+            add_ms = []
+            for _ in range(2):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                c.add(device_ptr=(bold_dev.data_ptr(), (T_LEN, N_VOX)))
+                e1.record(stream)
+                torch.cuda.synchronize()
+                add_ms.append(e0.elapsed_time(e1))
+            g_c, _ = c.graph("s", SPARSITY)           # keys allocated on first use
+            g_c.free()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g_c, cinfo = c.graph("s", SPARSITY)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            g_c.free()
+        add_t = float(np.median(add_ms))
+        cohort = {"subjects": 3, "fisher": True, "ms_per_subject_add": add_t,
+                  "fp64_gram_tflops": 2.0 * M1 * T_LEN / (add_t / 1000.0) / 1e12,
+                  "flops_counted": "2 per pair and time point (FP64 product, FP64 sum)",
+                  "ms_graph_top1pct": e0.elapsed_time(e1), "edges": cinfo["edges"]}
+
     value = world * 60000.0 / ms_dev
     e2e = world * 60000.0 / ms_e2e
     tm = timings[-1]
@@ -375,6 +406,7 @@ def main():
                      "betweenness_and_paths": tm["bc_ms"], "newman": tm["newman_ms"]},
         "step_ms_all": all_ms,
         "eigen_centrality": eigen,
+        "subject_average": cohort,
         "clocks": clk,
     }
     if fp32:

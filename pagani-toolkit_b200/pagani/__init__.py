@@ -177,12 +177,18 @@ class Cohort:
         ctx._check(lib().pg_cohort_create(ctx.h, N, int(fisher), int(weighted), ct.byref(h)))
         self.h = h
 
-    def add(self, bold_TxN):
-        bold = np.ascontiguousarray(bold_TxN, np.float32)
-        T, N = bold.shape
+    def add(self, bold_TxN=None, device_ptr=None):
+        """One subject: (T, N) float32 on the host, or device_ptr = (ptr, (T, N))."""
+        if device_ptr is not None:
+            ptr, (T, N) = device_ptr
+            src, on_dev = ct.c_void_p(ptr), 1
+        else:
+            bold = np.ascontiguousarray(bold_TxN, np.float32)
+            T, N = bold.shape
+            src, on_dev = _p(bold), 0
         if N != self.N:
             raise ValueError(f"subject has {N} voxels, cohort has {self.N}")
-        self.ctx._check(lib().pg_cohort_add(self.ctx.h, self.h, _p(bold), T, 0))
+        self.ctx._check(lib().pg_cohort_add(self.ctx.h, self.h, src, T, on_dev))
 
     @property
     def subjects(self):

@@ -27,6 +27,15 @@ def test_cucormat_rejects_bad_threshold_type(tmp_path):
     assert p.returncode == 1 and "threshold type error" in p.stderr
 
 
+@pytest.mark.parametrize("avg", ["y", "b", "yx", "x", "q"])
+def test_cucormat_rejects_bad_average_mode(tmp_path, avg):
+    """to_average must be n, yf, yn, bf or bn (the reference silently leaves
+    the average at zero for y or b alone)."""
+    exe = os.path.join(BIN, "CUCorMat")
+    p = subprocess.run([exe, str(tmp_path), "0.5", avg, "n", "r", "0.3"], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 1 and "to_average must be" in p.stderr
+
+
 # ---------------------------------------------------------------- ConvertNII
 def _write_nm(path, x):
     with open(path, "wb") as f:

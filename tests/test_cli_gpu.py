@@ -214,3 +214,41 @@ def test_newman_weighted_tool(tmp_path):
     assert np.array_equal(read_nm(tmp_path / "w1_modu.nm"), lab.astype(np.float32))
     assert "Round:" in open(tmp_path / "w1_modu.txt").read()
     assert not (tmp_path / "b1_modu.nm").exists()
+
+
+@pytest.mark.parametrize("tool,avg,mode,thr", [("CUCorMat", "bf", "s", 2.0), ("CUCorMat_weighted", "yn", "r", 0.15)])
+def test_cucormat_subject_average(tmp_path, tool, avg, mode, thr):
+    """to_average: the averaged graph and .cormat (named after the directory,
+    with the subject count) equal the oracle's cohort average; bf also writes
+    every subject's own graph."""
+    N, shape = 500, (10, 10, 6)
+    d = tmp_path / "cohortdir"
+    d.mkdir()
+    mask = np.zeros(shape, np.uint8)
+    flat = np.zeros(np.prod(shape), np.uint8)
+    flat[:N] = 1
+    mask[:] = flat.reshape(shape[2], shape[1], shape[0]).transpose(2, 1, 0)
+    write_nifti(d / "mask.nii", mask, 2)
+    bolds = [synth.bold_series(N, T, 10, 5150 + T) for T in (120, 90)]
+    for k, b in enumerate(bolds):
+        write_nifti(d / f"s{k}.nii", volume_from_series(b, shape), 16)
+    run(tool, d, 0.5, avg, "y", mode, thr)
+    weighted = tool.endswith("weighted")
+    keys = O.cohort_keys(bolds, fisher=avg[1] == "f", weighted=weighted)
+    base = f"cohortdir_2_{N}"
+    cm = np.fromfile(d / f"{base}.cormat", np.float32)
+    assert np.frombuffer(open(d / f"{base}.cormat", "rb").read(4), np.int32)[0] == N * (N - 1) // 2
+    assert np.array_equal(cm[1:], keys.astype(np.float32))
+    if mode == "s":
+        Ro, Co, _, tau = O.graph_k(keys, N, O.sparsity_k(N, thr), weighted=weighted)
+        f = d / f"{base}_spa{thr:.3f}%_cor{np.float32(tau):.3f}.csr"
+    else:
+        Ro, Co, Vo = O.graph_r(keys, N, thr, weighted=weighted)
+        s = np.float32(100.0 * len(Co) / (N * (N - 1) // 2) / 2)
+        f = d / f"{base}_spa{s:.3f}%_cor{thr:.3f}.csr"
+    R, C, V = read_csr(f)
+    assert np.array_equal(R, Ro) and np.array_equal(C, Co)
+    if weighted:
+        assert np.array_equal(V, Vo)
+    per_subject = glob.glob(str(d / "s*_500_spa*.csr"))
+    assert len(per_subject) == (2 if avg[0] == "b" else 0)
