@@ -13,7 +13,8 @@
  * reference's own CPU sources compiled by oracle/Makefile into oracle/_ref/,
  * and tests/golden/ holds fixtures generated from that compiled reference.
  *
- * Build: gcc -O2 -ffp-contract=off (no fused multiply-add anywhere).
+ * Build: gcc -O2 -ffp-contract=off: no multiply-add is fused except where
+ * fma() is written out (the r accumulation).
  */
 #include "oracle.h"
 #include <math.h>
@@ -67,7 +68,7 @@ double or_pair_r(const double* z, int T, int i, int j, int weighted)
     const double* a = z + (int64_t)i * T;
     const double* b = z + (int64_t)j * T;
     double r = 0.0;
-    for (int t = 0; t < T; t++) r += a[t] * b[t];
+    for (int t = 0; t < T; t++) r = fma(a[t], b[t], r);
     return range_rule(r, weighted);
 }
 

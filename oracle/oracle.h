@@ -9,8 +9,10 @@
  *   - z-score in FP64: mean = (sum_t x_t) / T with sequential adds, then
  *     s = sqrt(sum_t (x_t - mean)^2) with each square rounded before the add,
  *     z_t = (x_t - mean) / s.  A zero-variance row becomes the zero vector.
- *   - r(i,j) = sum_t z_i[t] * z_j[t], t ascending, product rounded, then the
- *     add rounded (no fused multiply-add).  Compiled with -ffp-contract=off.
+ *   - r(i,j) = sum_t z_i[t] * z_j[t], t ascending, each term added with one
+ *     fused multiply-add (r = fma(z_i[t], z_j[t], r), a single rounding, as
+ *     the reference's SGEMM accumulates).  Everything else is compiled with
+ *     -ffp-contract=off, so no other multiply-add is fused.
  *   - the reference's range rule (post_block): an r outside [-1, 1]
  *     (unweighted) or outside (-1-1e-6, 1+1e-6) (weighted) is stored as 0.
  */

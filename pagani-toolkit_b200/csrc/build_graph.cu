@@ -64,15 +64,15 @@ __global__ void k_zwrite(const float* __restrict__ bold, int N, int T, int Tp, c
 }
 
 // --------------------------------------------------------- FP64 recheck
-// r(i,j) exactly as the oracle: sequential t, product rounded then sum
-// rounded; then the reference's range rule (post_block, CorMat.cpp:821 /
+// r(i,j) exactly as the oracle: sequential t, one fused multiply-add per
+// term; then the reference's range rule (post_block, CorMat.cpp:821 /
 // W CorMat.cpp:821).  Key = r or |r|.
 __device__ __forceinline__ double exact_r(const double* __restrict__ z64, int T, int i, int j, int weighted)
 {
     const double* a = z64 + (size_t)i * T;
     const double* b = z64 + (size_t)j * T;
     double r = 0.0;
-    for (int t = 0; t < T; t++) r = __dadd_rn(r, __dmul_rn(a[t], b[t]));
+    for (int t = 0; t < T; t++) r = __fma_rn(a[t], b[t], r);
     if (weighted) return (r > -1.0 - 1e-6 && r < 1.0 + 1e-6) ? r : 0.0;
     return (r >= -1.0 && r <= 1.0) ? r : 0.0;
 }

@@ -6,17 +6,21 @@
 // host array of M1 floats (post_block, CorMat.cpp:775-838), divides by the
 // subject count, applies inv_fisher_trans (:514-524) and thresholds once.
 // Here:
-//   - one FP64 accumulator of M1 doubles (packed upper triangle, the .cormat
-//     order) stays in HBM for the whole cohort: 13.5 GB at 58,000 voxels;
+//   - one FP64 accumulator stays in HBM for the whole cohort, tile-major:
+//     the 128 x 128 blocks (bi <= bj) of the pair matrix in row-major block
+//     order, each block contiguous (13.5 GB at 58,000 voxels; positions with
+//     j <= i or beyond N stay 0);
 //   - per subject, FP64 z-scores are written time-major (T x Np, the layout
 //     of the input series), then k_cohort_gram, a persistent FP64 Gram:
 //     thread 0 streams 16 time points x 128 voxels of both operands per
 //     stage with TMA into a 3-stage shared-memory ring (mbarrier waits
 //     bounded by the global timer), every thread keeps an 8 x 8 block of
-//     pair sums in registers -- product rounded, then sum rounded, t
+//     pair sums in registers -- one fused multiply-add per time point, t
 //     ascending, the oracle's order -- and the epilogue applies the range
-//     rule and the Fisher transform and adds the result into the
-//     accumulator.  The tensor cores are not used: the average needs every
+//     rule and the Fisher transform into a 128 KB shared-memory tile that
+//     one asynchronous bulk reduce-add (cp.reduce.async.bulk .add.f64) adds
+//     into the accumulator block while the next tile computes.  One add per
+//     element and launch, so the sum is the oracle's, in subject order.  The tensor cores are not used: the average needs every
 //     pair's exact FP64 r (no threshold separates decided pairs before all
 //     subjects are summed) and tcgen05 has no FP64 kind;
 //   - the graph: keys = order-preserving uint64 of acc / S (inverse Fisher
@@ -35,12 +39,15 @@
 struct pg_cohort {
     int device = 0;
     int N = 0;
+    int nb = 0;                            // 128-voxel blocks
+    long long ntiles = 0;                  // nb (nb + 1) / 2 upper-triangle blocks
+    long long nelem = 0;                   // ntiles * 128 * 128 accumulator entries
     int fisher = 0;
     int weighted = 0;
     int subjects = 0;
     long long M1 = 0;
-    double* acc = nullptr;                 // device, M1 doubles
-    unsigned long long* keys = nullptr;    // device, M1 keys (allocated on first use)
+    double* acc = nullptr;                 // device, nelem doubles (tile-major)
+    unsigned long long* keys = nullptr;    // device, nelem keys, 0 where no pair (allocated on first use)
     bool keys_valid = false;
     bool broken = false;                   // an add failed part-way: the sums are unusable
 };
@@ -136,8 +143,30 @@ __device__ __forceinline__ double range_rule(double r, int weighted)
     return (r >= -1.0 && r <= 1.0) ? r : 0.0;
 }
 
-// Offset of pair (i, j) in the packed upper triangle is row_base(i) + j.
-__device__ __forceinline__ long long row_base(long long i, long long N) { return i * N - i * (i + 1) / 2 - i - 1; }
+constexpr int CB = 128;          // voxels per block edge
+constexpr int CB2 = CB * CB;     // accumulator entries per block
+
+// Linear index of the first block of block row bi (blocks bi <= bj, row-major).
+__device__ __forceinline__ long long block_row_start(long long bi, long long nb) { return bi * nb - bi * (bi - 1) / 2; }
+
+// Block (bi, bj) of linear index L, by binary search over the row starts.
+__device__ __forceinline__ int2 block_of(long long L, int nb)
+{
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (block_row_start(mid, nb) <= L) lo = mid;
+        else hi = mid - 1;
+    }
+    return make_int2(lo, lo + (int)(L - block_row_start(lo, nb)));
+}
+
+// Accumulator position of pair (i, j), i < j.
+__device__ __forceinline__ long long acc_pos(int i, int j, int nb)
+{
+    const int bi = i / CB, bj = j / CB;
+    return (block_row_start(bi, nb) + (bj - bi)) * CB2 + (long long)(i % CB) * CB + (j % CB);
+}
 
 // ------------------------------------------------------------ z-scores
 // zT[t * Np + i] = (x - mean_i) / s_i with the operations of k_zwrite (the
@@ -157,13 +186,13 @@ __global__ void k_cohort_z(const float* __restrict__ bold, int N, int T, int Np,
 }
 
 // ------------------------------------------------------------ FP64 Gram
-constexpr int CB = 128;          // voxels per tile edge
 constexpr int CK = 16;           // time points per stage
 constexpr int CSTAGES = 3;
 constexpr int CTHREADS = 256;    // 16 x 16 threads, 8 x 8 pairs each
 constexpr uint32_t CTILE_BYTES = CB * CK * 8;
 constexpr uint32_t CSTAGE_BYTES = 2 * CTILE_BYTES;
-constexpr size_t CSMEM = 128 + CSTAGES * CSTAGE_BYTES + CSTAGES * 8 + 16;
+constexpr uint32_t COUT_BYTES = CB2 * 8;            // 128 KB epilogue tile
+constexpr size_t CSMEM = 128 + CSTAGES * CSTAGE_BYTES + COUT_BYTES + CSTAGES * 8 + 16;
 
 struct CohortArgs {
     int N, T, nb, nk;
@@ -173,7 +202,7 @@ struct CohortArgs {
     int* err;
 };
 
-// Tile cursor over the row-major upper triangle of nb x nb blocks: tile
+// Block cursor over the row-major upper triangle of nb x nb blocks: block
 // (bi, bi + rem).  Advances by `step` linear positions.
 __device__ __forceinline__ void tile_advance(int nb, int& bi, long long& rem, long long step)
 {
@@ -184,13 +213,21 @@ __device__ __forceinline__ void tile_advance(int nb, int& bi, long long& rem, lo
     }
 }
 
+__device__ __forceinline__ void bulk_reduce_add_f64(double* gdst, const void* ssrc, uint32_t bytes)
+{
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;"
+                 ::"l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
 template <bool FISHER>
 __global__ void __launch_bounds__(CTHREADS, 1)
 k_cohort_gram(const __grid_constant__ CUtensorMap zmap, const CohortArgs a)
 {
     extern __shared__ unsigned char smraw[];
     unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
-    unsigned long long* full = (unsigned long long*)(sm + CSTAGES * CSTAGE_BYTES);
+    double* out = (double*)(sm + CSTAGES * CSTAGE_BYTES);
+    unsigned long long* full = (unsigned long long*)(sm + CSTAGES * CSTAGE_BYTES + COUT_BYTES);
     volatile int* abort_flag = (volatile int*)(full + CSTAGES);
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const long long G = gridDim.x;
@@ -203,7 +240,7 @@ k_cohort_gram(const __grid_constant__ CUtensorMap zmap, const CohortArgs a)
     }
     __syncthreads();
 
-    // producer state (thread 0): tile of the next chunk to issue
+    // producer state (thread 0): block of the next chunk to issue
     int pbi = 0;
     long long prem = 0;
     tile_advance(a.nb, pbi, prem, blockIdx.x);
@@ -220,7 +257,7 @@ k_cohort_gram(const __grid_constant__ CUtensorMap zmap, const CohortArgs a)
         for (long long q = 0; q < total && q < CSTAGES; q++) issue(q);
 
     int cbi = 0;
-    long long crem = 0;
+    long long crem = 0, cL = blockIdx.x;
     tile_advance(a.nb, cbi, crem, blockIdx.x);
     double c[8][8];
     long long q = 0;
@@ -254,115 +291,128 @@ k_cohort_gram(const __grid_constant__ CUtensorMap zmap, const CohortArgs a)
 #pragma unroll
             for (int u = 0; u < 8; u++)
 #pragma unroll
-                for (int v = 0; v < 8; v++) c[u][v] = __dadd_rn(c[u][v], __dmul_rn(ra[u], rb[v]));
+                for (int v = 0; v < 8; v++) c[u][v] = __fma_rn(ra[u], rb[v], c[u][v]);
         }
-        __syncthreads();                       // every thread is done with stage s
+        if (kc == a.nk - 1 && tid == 0)
+            asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");   // the last block's reduce has read `out`
+        __syncthreads();                       // every thread is done with stage s (and `out` is free)
         if (*abort_flag) break;
         if (tid == 0 && q + CSTAGES < total) issue(q + CSTAGES);
         if (kc == a.nk - 1) {
             const int I0 = cbi * CB, J0 = (int)(cbi + crem) * CB;
 #pragma unroll
             for (int u = 0; u < 8; u++) {
-                const int i = I0 + 2 * ty + 32 * (u >> 1) + (u & 1);
-                const long long base = row_base(i, a.N);
+                const int r = 2 * ty + 32 * (u >> 1) + (u & 1);
+                const int i = I0 + r;
 #pragma unroll
-                for (int v = 0; v < 8; v++) {
-                    const int j = J0 + 2 * tx + 32 * (v >> 1) + (v & 1);
+                for (int v = 0; v < 8; v += 2) {
+                    const int cl = 2 * tx + 32 * (v >> 1);
+                    double2 f;
+                    f.x = f.y = 0.0;
+                    const int j = J0 + cl;
                     if (j > i && j < a.N) {
-                        const double r = range_rule(c[u][v], a.weighted);
-                        const double f = FISHER ? d_fisher(r) : r;
-                        double* p = a.acc + base + j;
-                        *p = __dadd_rn(*p, f);
+                        const double x = range_rule(c[u][v], a.weighted);
+                        f.x = FISHER ? d_fisher(x) : x;
                     }
+                    if (j + 1 > i && j + 1 < a.N) {
+                        const double x = range_rule(c[u][v + 1], a.weighted);
+                        f.y = FISHER ? d_fisher(x) : x;
+                    }
+                    *(double2*)(out + r * CB + cl) = f;
                 }
             }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // `out` visible to the bulk copy
+            __syncthreads();
+            if (tid == 0) bulk_reduce_add_f64(a.acc + cL * CB2, out, COUT_BYTES);
             tile_advance(a.nb, cbi, crem, G);
+            cL += G;
         }
     }
-    if (q < total && tid == 0) {
-        // a wait timed out: record it and drain this CTA's copies in flight
-        atomicExch(a.err, 1);
-        const long long last = total < q + CSTAGES ? total : q + CSTAGES;
-        for (long long w = q; w < last; w++)
-            mbar_wait(&full[w % CSTAGES], (uint32_t)((w / CSTAGES) & 1), WAIT_NS / 4);
+    if (tid == 0) {
+        if (q < total) {
+            // a wait timed out: record it and drain this CTA's loads in flight
+            atomicExch(a.err, 1);
+            const long long last = total < q + CSTAGES ? total : q + CSTAGES;
+            for (long long w = q; w < last; w++)
+                mbar_wait(&full[w % CSTAGES], (uint32_t)((w / CSTAGES) & 1), WAIT_NS / 4);
+        }
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");   // reduces complete before exit
     }
 }
 
 // ------------------------------------------------------ keys and graph
+// Kernels over the accumulator run one block of 256 threads per 128 x 128
+// accumulator block (grid-stride over blocks).
+
 template <bool FISHER>
-__global__ void k_cohort_keys(const double* __restrict__ acc, long long M1, double subjects,
+__global__ void k_cohort_keys(const double* __restrict__ acc, int N, int nb, long long ntiles, double subjects,
                               unsigned long long* __restrict__ keys)
 {
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < M1;
-         p += (long long)gridDim.x * blockDim.x) {
-        double k = __ddiv_rn(acc[p], subjects);
-        if (FISHER) k = d_inv_fisher(k);
-        keys[p] = dkey(k);
+    for (long long L = blockIdx.x; L < ntiles; L += gridDim.x) {
+        const int2 b = block_of(L, nb);
+        const double* src = acc + L * CB2;
+        unsigned long long* dst = keys + L * CB2;
+        for (int e = threadIdx.x; e < CB2; e += blockDim.x) {
+            const int i = b.x * CB + (e >> 7), j = b.y * CB + (e & 127);
+            unsigned long long k = 0;
+            if (j > i && j < N) {
+                double x = __ddiv_rn(src[e], subjects);
+                if (FISHER) x = d_inv_fisher(x);
+                k = dkey(x);
+            }
+            dst[e] = k;
+        }
     }
 }
 
-// Pairs (i < j) of row i, one warp per row: CMP 0 counts key > tkey, CMP 1
-// counts key == tkey.
+// CMP 0 counts keys > tkey, CMP 1 keys == tkey (tkey > 0: the 0 of an empty
+// position never counts).
 template <int CMP>
-__global__ void k_cohort_count(const unsigned long long* __restrict__ keys, int N, unsigned long long tkey,
+__global__ void k_cohort_count(const unsigned long long* __restrict__ keys, long long n, unsigned long long tkey,
                                unsigned long long* __restrict__ count)
 {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long local = 0;
-    for (int i = warp; i < N - 1; i += nw) {
-        const long long base = row_base(i, N);
-        for (int j0 = i + 1; j0 < N; j0 += 32) {
-            const int j = j0 + lane;
-            bool in = false;
-            if (j < N) {
-                const unsigned long long k = keys[base + j];
-                in = CMP == 0 ? k > tkey : k == tkey;
-            }
-            local += __popc(__ballot_sync(0xffffffffu, in));
-        }
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = keys[p];
+        local += CMP == 0 ? (k > tkey) : (k == tkey);
     }
-    if (lane == 0 && local) atomicAdd(count, local);
+    for (int o = 16; o; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
 }
 
 // Complemented lexicographic keys ~(i*N + j) of the pairs tied at tkey, so
 // that selecting the m-th largest yields the m-th smallest pair.
-__global__ void k_cohort_tie_keys(const unsigned long long* __restrict__ keys, int N, unsigned long long tkey,
-                                  unsigned long long* __restrict__ out, unsigned long long* __restrict__ n,
-                                  long long cap)
+__global__ void k_cohort_tie_keys(const unsigned long long* __restrict__ keys, int N, int nb, long long ntiles,
+                                  unsigned long long tkey, unsigned long long* __restrict__ out,
+                                  unsigned long long* __restrict__ n, long long cap)
 {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    for (int i = warp; i < N - 1; i += nw) {
-        const long long base = row_base(i, N);
-        for (int j0 = i + 1; j0 < N; j0 += 32) {
-            const int j = j0 + lane;
-            const bool in = j < N && keys[base + j] == tkey;
+    for (long long L = blockIdx.x; L < ntiles; L += gridDim.x) {
+        const int2 b = block_of(L, nb);
+        for (int e = threadIdx.x; e < CB2; e += blockDim.x) {
+            const bool in = keys[L * CB2 + e] == tkey;
             const long long s = warp_append(n, in);
-            if (s >= 0 && s < cap) out[s] = ~((unsigned long long)i * (unsigned long long)N + (unsigned long long)j);
+            if (s >= 0 && s < cap) {
+                const unsigned long long i = b.x * CB + (e >> 7), j = b.y * CB + (e & 127);
+                out[s] = ~(i * (unsigned long long)N + j);
+            }
         }
     }
 }
 
 // Edges: key > tkey, or key == tkey and (i, j) <= tie_cut lexicographically.
-__global__ void k_cohort_emit(const unsigned long long* __restrict__ keys, int N, unsigned long long tkey,
-                              int strict_only, unsigned long long tie_cut, int weighted, int2* __restrict__ pairs,
-                              float* __restrict__ w, unsigned long long* __restrict__ n, long long cap)
+__global__ void k_cohort_emit(const unsigned long long* __restrict__ keys, int N, int nb, long long ntiles,
+                              unsigned long long tkey, int strict_only, unsigned long long tie_cut, int weighted,
+                              int2* __restrict__ pairs, float* __restrict__ w, unsigned long long* __restrict__ n,
+                              long long cap)
 {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    for (int i = warp; i < N - 1; i += nw) {
-        const long long base = row_base(i, N);
-        for (int j0 = i + 1; j0 < N; j0 += 32) {
-            const int j = j0 + lane;
-            bool in = false;
-            unsigned long long k = 0;
-            if (j < N) {
-                k = keys[base + j];
-                in = k > tkey ||
-                     (!strict_only && k == tkey &&
-                      (unsigned long long)i * (unsigned long long)N + (unsigned long long)j <= tie_cut);
-            }
+    for (long long L = blockIdx.x; L < ntiles; L += gridDim.x) {
+        const int2 b = block_of(L, nb);
+        for (int e = threadIdx.x; e < CB2; e += blockDim.x) {
+            const unsigned long long k = keys[L * CB2 + e];
+            const int i = b.x * CB + (e >> 7), j = b.y * CB + (e & 127);
+            const bool in = k > tkey || (!strict_only && k == tkey &&
+                                         (unsigned long long)i * (unsigned long long)N + (unsigned long long)j <= tie_cut);
             const long long s = warp_append(n, in);
             if (s >= 0 && s < cap) {
                 pairs[s] = make_int2(i, j);
@@ -372,11 +422,19 @@ __global__ void k_cohort_emit(const unsigned long long* __restrict__ keys, int N
     }
 }
 
-__global__ void k_cohort_float(const unsigned long long* __restrict__ keys, long long n, float* __restrict__ out)
+// Packed upper triangle (the .cormat order) of rows [row0, row0 + rows):
+// one warp per row, lanes over j.
+__global__ void k_cohort_packed(const unsigned long long* __restrict__ keys, int N, int nb, long long row0,
+                                long long rows, float* __restrict__ out)
 {
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
-         p += (long long)gridDim.x * blockDim.x)
-        out[p] = (float)dkey_inv(keys[p]);
+    const long long base0 = row0 * N - row0 * (row0 + 1) / 2;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (long long ii = warp; ii < rows; ii += nw) {
+        const int i = (int)(row0 + ii);
+        const long long off = (long long)i * N - (long long)i * (i + 1) / 2 - base0;
+        for (int j = i + 1 + lane; j < N; j += 32) out[off + (j - i - 1)] = (float)dkey_inv(keys[acc_pos(i, j, nb)]);
+    }
 }
 
 bool make_zmap(CUtensorMap* m, const double* base, int Np, int Tp)
@@ -401,20 +459,21 @@ pg_status check_cohort(pg_ctx* ctx, const pg_cohort* c, const char* fn)
     return PG_OK;
 }
 
-// keys = dkey(finish(acc)), computed once after the last add.
+int block_grid(pg_ctx* ctx, long long ntiles) { return (int)std::max(1LL, std::min<long long>(ctx->sm_count * 8LL, ntiles)); }
+
+// keys = dkey(finish(acc)) (0 where there is no pair), computed once after
+// the last add.
 pg_status cohort_keys(pg_ctx* ctx, pg_cohort* c)
 {
     if (c->subjects < 1) return pg_fail(ctx, PG_ERR_INVALID, "cohort has no subjects");
     if (c->keys_valid) return PG_OK;
-    if (!c->keys) PG_CUDA(ctx, cudaMalloc(&c->keys, sizeof(unsigned long long) * (size_t)std::max(c->M1, 1LL)));
-    if (c->M1 > 0) {
-        const int grid = std::max(1, std::min(ctx->sm_count * 8, ceil_div(c->M1, 256)));
-        if (c->fisher)
-            k_cohort_keys<true><<<grid, 256, 0, ctx->stream>>>(c->acc, c->M1, (double)c->subjects, c->keys);
-        else
-            k_cohort_keys<false><<<grid, 256, 0, ctx->stream>>>(c->acc, c->M1, (double)c->subjects, c->keys);
-        PG_LAUNCHED(ctx);
-    }
+    if (!c->keys) PG_CUDA(ctx, cudaMalloc(&c->keys, sizeof(unsigned long long) * (size_t)c->nelem));
+    const int grid = block_grid(ctx, c->ntiles);
+    if (c->fisher)
+        k_cohort_keys<true><<<grid, 256, 0, ctx->stream>>>(c->acc, c->N, c->nb, c->ntiles, (double)c->subjects, c->keys);
+    else
+        k_cohort_keys<false><<<grid, 256, 0, ctx->stream>>>(c->acc, c->N, c->nb, c->ntiles, (double)c->subjects, c->keys);
+    PG_LAUNCHED(ctx);
     c->keys_valid = true;
     return PG_OK;
 }
@@ -425,20 +484,26 @@ extern "C" pg_status pg_cohort_create(pg_ctx* ctx, int32_t N, int32_t fisher, in
 {
     if (!ctx || !out || N < 1) return pg_fail(ctx, PG_ERR_INVALID, "pg_cohort_create: bad arguments (N=%d)", N);
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (ctx->smem_optin < CSMEM)
+        return pg_fail(ctx, PG_ERR_CUDA, "pg_cohort_create: %zu B of shared memory per block needed, %zu available",
+                       CSMEM, ctx->smem_optin);
     *out = nullptr;
     pg_cohort* c = new pg_cohort;
     c->device = ctx->device;
     c->N = N;
+    c->nb = (N + CB - 1) / CB;
+    c->ntiles = (long long)c->nb * (c->nb + 1) / 2;
+    c->nelem = c->ntiles * CB2;
     c->fisher = fisher != 0;
     c->weighted = weighted != 0;
     c->M1 = (long long)N * (N - 1) / 2;
-    cudaError_t e = cudaMalloc(&c->acc, sizeof(double) * (size_t)std::max(c->M1, 1LL));
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->acc, 0, sizeof(double) * (size_t)std::max(c->M1, 1LL), ctx->stream);
+    cudaError_t e = cudaMalloc(&c->acc, sizeof(double) * (size_t)c->nelem);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->acc, 0, sizeof(double) * (size_t)c->nelem, ctx->stream);
     if (e != cudaSuccess) {
-        const long long M1 = c->M1;
+        const long long nelem = c->nelem;
         pg_cohort_free(c);
         return pg_fail(ctx, e == cudaErrorMemoryAllocation ? PG_ERR_NOMEM : PG_ERR_CUDA,
-                       "pg_cohort_create: %lld-pair accumulator: %s", M1, cudaGetErrorString(e));
+                       "pg_cohort_create: %lld-entry accumulator: %s", nelem, cudaGetErrorString(e));
     }
     *out = c;
     return PG_OK;
@@ -449,7 +514,7 @@ extern "C" pg_status pg_cohort_add(pg_ctx* ctx, pg_cohort* c, const float* bold,
     PG_TRY(check_cohort(ctx, c, "pg_cohort_add"));
     if (!bold || T < 1) return pg_fail(ctx, PG_ERR_INVALID, "pg_cohort_add: bad arguments (T=%d)", T);
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    const int N = c->N, Np = (N + CB - 1) / CB * CB, Tp = (T + CK - 1) / CK * CK;
+    const int N = c->N, Np = c->nb * CB, Tp = (T + CK - 1) / CK * CK;
     const float* dbold = bold;
     if (!input_on_device) {
         float* tmp;
@@ -479,9 +544,9 @@ extern "C" pg_status pg_cohort_add(pg_ctx* ctx, pg_cohort* c, const float* bold,
     CohortArgs a;
     a.N = N;
     a.T = T;
-    a.nb = Np / CB;
+    a.nb = c->nb;
     a.nk = Tp / CK;
-    a.ntiles = (long long)a.nb * (a.nb + 1) / 2;
+    a.ntiles = c->ntiles;
     a.acc = c->acc;
     a.weighted = c->weighted;
     a.err = err;
@@ -524,7 +589,8 @@ extern "C" pg_status pg_cohort_graph(pg_ctx* ctx, pg_cohort* c, int32_t mode, do
     PG_CUDA(ctx, cudaEventRecord(ev[1], ctx->stream));
     const int N = c->N;
     const long long M1 = c->M1;
-    const int rgrid = std::max(1, std::min(ctx->sm_count * 8, ceil_div((long long)N * 32, 256)));
+    const int egrid = std::max(1, std::min(ctx->sm_count * 8, ceil_div(c->nelem, 256)));
+    const int bgrid = block_grid(ctx, c->ntiles);
     unsigned long long* counters;
     PG_TRY(pg_wst(ctx, "cohort.counters", 4, &counters));
     PG_CUDA(ctx, cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), ctx->stream));
@@ -535,10 +601,8 @@ extern "C" pg_status pg_cohort_graph(pg_ctx* ctx, pg_cohort* c, int32_t mode, do
     if (mode == PG_THRESH_R) {
         tau = value + 0.0;   // -0 threshold behaves as +0 (keys are never -0)
         tkey = dkey(tau);
-        if (M1 > 0) {
-            k_cohort_count<0><<<rgrid, 256, 0, ctx->stream>>>(c->keys, N, tkey, counters);
-            PG_LAUNCHED(ctx);
-        }
+        k_cohort_count<0><<<egrid, 256, 0, ctx->stream>>>(c->keys, c->nelem, tkey, counters);
+        PG_LAUNCHED(ctx);
         unsigned long long nh = 0;
         PG_TRY(pg_d2h(ctx, &nh, counters, sizeof nh));
         n_edges = (long long)nh;
@@ -553,13 +617,13 @@ extern "C" pg_status pg_cohort_graph(pg_ctx* ctx, pg_cohort* c, int32_t mode, do
             unsigned long long* hist;
             PG_TRY(pg_wst(ctx, "cohort.sel", 2, &st));
             PG_TRY(pg_wst(ctx, "cohort.hist", 256, &hist));
-            PG_TRY(pg_radix_select(ctx, c->keys, M1, k_edges, st, hist));
+            PG_TRY(pg_radix_select(ctx, c->keys, c->nelem, k_edges, st, hist));
             SelState sh;
             PG_TRY(pg_d2h(ctx, &sh, st, sizeof sh));
             tkey = sh.prefix;
             tau = dkey_inv(tkey);
             const long long need = sh.m;   // ties at tau still to take (>= 1)
-            k_cohort_count<1><<<rgrid, 256, 0, ctx->stream>>>(c->keys, N, tkey, counters + 1);
+            k_cohort_count<1><<<egrid, 256, 0, ctx->stream>>>(c->keys, c->nelem, tkey, counters + 1);
             PG_LAUNCHED(ctx);
             unsigned long long nt = 0;
             PG_TRY(pg_d2h(ctx, &nt, counters + 1, sizeof nt));
@@ -569,7 +633,8 @@ extern "C" pg_status pg_cohort_graph(pg_ctx* ctx, pg_cohort* c, int32_t mode, do
             } else {
                 unsigned long long* tk;
                 PG_TRY(pg_wst(ctx, "cohort.ties", (size_t)nt, &tk));
-                k_cohort_tie_keys<<<rgrid, 256, 0, ctx->stream>>>(c->keys, N, tkey, tk, counters + 2, (long long)nt);
+                k_cohort_tie_keys<<<bgrid, 256, 0, ctx->stream>>>(c->keys, N, c->nb, c->ntiles, tkey, tk, counters + 2,
+                                                                  (long long)nt);
                 PG_LAUNCHED(ctx);
                 PG_TRY(pg_radix_select(ctx, tk, (long long)nt, need, st, hist));
                 PG_TRY(pg_d2h(ctx, &sh, st, sizeof sh));
@@ -585,8 +650,8 @@ extern "C" pg_status pg_cohort_graph(pg_ctx* ctx, pg_cohort* c, int32_t mode, do
     PG_TRY(pg_wst(ctx, "b.pairs", (size_t)std::max(1LL, n_edges), &pairs));
     if (c->weighted) PG_TRY(pg_wst(ctx, "b.pw", (size_t)std::max(1LL, n_edges), &pw));
     if (n_edges > 0) {
-        k_cohort_emit<<<rgrid, 256, 0, ctx->stream>>>(c->keys, N, tkey, strict_only, tie_cut, c->weighted, pairs, pw,
-                                                      counters + 3, n_edges);
+        k_cohort_emit<<<bgrid, 256, 0, ctx->stream>>>(c->keys, N, c->nb, c->ntiles, tkey, strict_only, tie_cut,
+                                                      c->weighted, pairs, pw, counters + 3, n_edges);
         PG_LAUNCHED(ctx);
         unsigned long long ne = 0;
         PG_TRY(pg_d2h(ctx, &ne, counters + 3, sizeof ne));
@@ -619,15 +684,22 @@ extern "C" pg_status pg_cohort_packed(pg_ctx* ctx, pg_cohort* c, float* r_packed
     if (!r_packed) return pg_fail(ctx, PG_ERR_INVALID, "pg_cohort_packed: null output");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
     PG_TRY(cohort_keys(ctx, c));
-    const long long chunk = 64LL << 20;
+    const int N = c->N;
+    const long long chunk_elems = 64LL << 20;
     float* buf;
-    PG_TRY(pg_wst(ctx, "cormat.out", (size_t)std::min(std::max(c->M1, 1LL), chunk), &buf));
-    for (long long p0 = 0; p0 < c->M1; p0 += chunk) {
-        const long long n = std::min(chunk, c->M1 - p0);
-        const int grid = std::max(1, std::min(ctx->sm_count * 8, ceil_div(n, 256)));
-        k_cohort_float<<<grid, 256, 0, ctx->stream>>>(c->keys + p0, n, buf);
+    PG_TRY(pg_wst(ctx, "cormat.out", (size_t)std::min(std::max(c->M1, 1LL), chunk_elems + N), &buf));
+    long long row = 0;
+    while (row < N - 1) {
+        long long r1 = row, elems = 0;
+        while (r1 < N - 1 && elems + (N - 1 - r1) <= std::max(chunk_elems, (long long)N)) {
+            elems += N - 1 - r1;
+            r1++;
+        }
+        const long long off = row * N - row * (row + 1) / 2;
+        k_cohort_packed<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(c->keys, N, c->nb, row, r1 - row, buf);
         PG_LAUNCHED(ctx);
-        PG_TRY(pg_d2h(ctx, r_packed + p0, buf, sizeof(float) * (size_t)n));
+        PG_TRY(pg_d2h(ctx, r_packed + off, buf, sizeof(float) * (size_t)elems));
+        row = r1;
     }
     return PG_OK;
 }
