@@ -368,7 +368,7 @@ def main():
         add_t = float(np.median(add_ms))
         cohort = {"subjects": 3, "fisher": True, "ms_per_subject_add": add_t,
                   "fp64_gram_tflops": 2.0 * M1 * T_LEN / (add_t / 1000.0) / 1e12,
-                  "flops_counted": "2 per pair and time point (FP64 product, FP64 sum)",
+                  "flops_counted": "one FP64 fused multiply-add (2 flop) per pair and time point",
                   "ms_graph_top1pct": e0.elapsed_time(e1), "edges": cinfo["edges"]}
 
     value = world * 60000.0 / ms_dev
