@@ -44,7 +44,7 @@ constexpr double LAMBDA = 0.01;
 constexpr size_t SMEM_CAP = 220 * 1024;        // dynamic shared memory of a team CTA
 constexpr long long MEDIUM_EDGES = 1LL << 22;  // at most this many edges: one team per group
 constexpr int CLUSTER = 16;                    // largest team (CTAs of one cluster)
-constexpr long long MIN_CTA_EDGES = 16384;     // a team CTA keeps at least this many edges
+constexpr long long MIN_CTA_EDGES = 8192;      // a team CTA keeps at least this many edges
 
 // In-group degree of every member (label of neighbour == label of node).
 __global__ void k_nm_gdeg(const int32_t* __restrict__ R, const int32_t* __restrict__ C,
@@ -489,6 +489,7 @@ struct ClusterTeam {    // a cluster: rows of y meet in global memory
 };
 
 constexpr int TEAM_MAX_ROWS = 12288;   // rows of a team group (its vector fits shared memory)
+constexpr int TEAM_NPT = 8;            // vector entries per thread kept in registers during a step
 
 // First local row whose edge offset reaches rank * E / nb.
 __host__ __device__ inline int team_split(const int32_t* R, int n, int rank, int nb)
@@ -710,23 +711,55 @@ __device__ double team_lead_vector(const Team& tm, const Group& gg, int M, doubl
         double* ybuf = Kind::kCluster ? (yb ? gg.v0 : gg.v) : tm.oy;
         team_spmv<W>(tm, Kind::kCluster ? ybuf + tm.r0 : ybuf, c, beta, lane, wid, nwarp);
         Kind::barrier();
-        x1[0] = 0.0;
-        for (int p = tid; p < n; p += nthr) {
-            const double y = ybuf[p];
-            x1[0] += y * y;
-        }
-        block_sum(ps, x1, ph);
-        vnorm = sqrt(x1[0]);
         double x3[3] = {0.0, 0.0, 0.0};
-        for (int p = tid; p < n; p += nthr) {
-            const double vold = tm.rep[p];
-            const double vp = ybuf[p] / vnorm;
-            const double d1 = vp - vold, d2 = vp + vold;
-            x3[0] += d1 * d1;
-            x3[1] += d2 * d2;
-            x3[2] += vp * (double)tm.kd[p];
-            if ((unsigned)(p - tm.r0) < (unsigned)tm.nown) tm.oprev[p - tm.r0] = vold;
-            tm.rep[p] = vp;
+        if (n <= TEAM_NPT * nthr) {
+            // at most TEAM_NPT entries per thread: y is loaded once, all loads
+            // and divisions of a thread issued together; the per-thread sums
+            // run over p = tid, tid + nthr, ... as in the loops below
+            double yv[TEAM_NPT];
+            x1[0] = 0.0;
+#pragma unroll
+            for (int k = 0; k < TEAM_NPT; k++) {
+                const int p = tid + k * nthr;
+                yv[k] = p < n ? ybuf[p] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < TEAM_NPT; k++)
+                if (tid + k * nthr < n) x1[0] += yv[k] * yv[k];
+            block_sum(ps, x1, ph);
+            vnorm = sqrt(x1[0]);
+#pragma unroll
+            for (int k = 0; k < TEAM_NPT; k++) {
+                const int p = tid + k * nthr;
+                if (p < n) {
+                    const double vold = tm.rep[p];
+                    const double vp = yv[k] / vnorm;
+                    const double d1 = vp - vold, d2 = vp + vold;
+                    x3[0] += d1 * d1;
+                    x3[1] += d2 * d2;
+                    x3[2] += vp * (double)tm.kd[p];
+                    if ((unsigned)(p - tm.r0) < (unsigned)tm.nown) tm.oprev[p - tm.r0] = vold;
+                    tm.rep[p] = vp;
+                }
+            }
+        } else {
+            x1[0] = 0.0;
+            for (int p = tid; p < n; p += nthr) {
+                const double y = ybuf[p];
+                x1[0] += y * y;
+            }
+            block_sum(ps, x1, ph);
+            vnorm = sqrt(x1[0]);
+            for (int p = tid; p < n; p += nthr) {
+                const double vold = tm.rep[p];
+                const double vp = ybuf[p] / vnorm;
+                const double d1 = vp - vold, d2 = vp + vold;
+                x3[0] += d1 * d1;
+                x3[1] += d2 * d2;
+                x3[2] += vp * (double)tm.kd[p];
+                if ((unsigned)(p - tm.r0) < (unsigned)tm.nown) tm.oprev[p - tm.r0] = vold;
+                tm.rep[p] = vp;
+            }
         }
         block_sum(ps, x3, ph);
         s1 = x3[0];
