@@ -23,7 +23,9 @@
 // barriers (no host round trip per level).  The forward pass also yields the
 // hop path length (sum of 1/d per node), returned by pg_betweenness on request.
 #include "pg_internal.cuh"
+#include "bc_dense.cuh"
 #include <cooperative_groups.h>
+#include <climits>
 #include <algorithm>
 
 namespace cg = cooperative_groups;
@@ -125,8 +127,12 @@ __device__ __forceinline__ ulonglong2 lane_mask(const bool (&f)[SL])
 }
 
 // four CTAs per SM (64 registers): occupancy hides the L2 latency of the row gathers
+// Batches [batch_first, batch_last); the forward sweep runs levels
+// fwd_first..fwd_last.  fwd_first > 1 resumes a batch whose earlier levels
+// were computed elsewhere (the dense tensor-core levels); fwd_last < INT_MAX
+// stops after that level, before the backward sweep (one batch per launch).
 __global__ void __launch_bounds__(THREADS, 4)
-k_brandes(BCArgs a, int batch_first, int batch_last)
+k_brandes(BCArgs a, int batch_first, int batch_last, int fwd_first, int fwd_last)
 {
     cg::grid_group grid = cg::this_grid();
     const int lane = threadIdx.x & 31;
@@ -139,17 +145,18 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
         const int ns = min(S, a.nsrc - s0);
         const ulonglong2 full = make_ulonglong2(ns >= 64 ? ~0ULL : ((1ULL << ns) - 1ULL),
                                                 ns >= 128 ? ~0ULL : ns > 64 ? ((1ULL << (ns - 64)) - 1ULL) : 0ULL);
+        const bool init = fwd_first <= 1;
         // ---- init: levels -1, frontier = sources
-        for (size_t q = gt; q < (size_t)n * S; q += gstride) a.dist[q] = -1;
-        for (size_t v = gt; v < (size_t)n; v += gstride) {
+        for (size_t q = gt; init && q < (size_t)n * S; q += gstride) a.dist[q] = -1;
+        for (size_t v = gt; init && v < (size_t)n; v += gstride) {
             a.front[v] = make_ulonglong2(0ULL, 0ULL);
             a.seen[v] = make_ulonglong2(0ULL, 0ULL);
             a.fhist[v] = make_ulonglong2(0ULL, 0ULL);
         }
-        for (size_t q = gt; q < (size_t)WORK_SLOTS; q += gstride) a.work[q] = 0;
-        if (gt < 3) a.flags[gt] = 0;
+        for (size_t q = gt; init && q < (size_t)WORK_SLOTS; q += gstride) a.work[q] = 0;
+        if (init && gt < 3) a.flags[gt] = 0;
         grid.sync();
-        if (gt < (size_t)ns) {
+        if (init && gt < (size_t)ns) {
             int s = a.sources ? a.sources[s0 + gt] : s0 + (int)gt;
             a.dist[(size_t)s * S + gt] = 0;
             a.sigma[(size_t)s * S + gt] = 1ULL;
@@ -160,10 +167,15 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
             atomicOr(gt < 64 ? &a.fhist[s].x : &a.fhist[s].y, bit);
         }
         grid.sync();
-        // ---- forward
-        int d = 1;
-        ulonglong2* cur = a.front;
-        ulonglong2* nxt = a.front + n;
+        // ---- forward: level d reads the frontier buffer (d - 1) & 1 and writes d & 1
+        int d = init ? 1 : fwd_first;
+        ulonglong2* cur = a.front + (size_t)((d - 1) & 1) * n;
+        ulonglong2* nxt = a.front + (size_t)(d & 1) * n;
+        if (!init) {
+            if (gt == 0) a.flags[d % 3] = 0;
+            grid.sync();
+        }
+        bool stopped = false;
         for (;; d++) {
             if (gt == 0) a.flags[(d + 1) % 3] = 0;
             int found = 0;
@@ -260,8 +272,13 @@ k_brandes(BCArgs a, int batch_first, int batch_last)
             grid.sync();
             const int any = a.flags[d % 3];
             ulonglong2* t = cur; cur = nxt; nxt = t;
+            if (d >= fwd_last) {
+                stopped = true;
+                break;
+            }
             if (!any) break;
         }
+        if (stopped) continue;   // the caller computes the next levels
         const int maxd = d - 1;  // deepest level reached
         if (a.out_dist) {
             for (size_t q = gt; q < (size_t)ns * n; q += gstride) {
@@ -415,7 +432,7 @@ __global__ void k_sum_inv(const double* __restrict__ x, int32_t n, double* __res
     }
 }
 
-pg_status alloc_state(pg_ctx* ctx, int n, BCArgs& a)
+pg_status alloc_state(pg_ctx* ctx, int n, BCArgs& a, int* max_deg = nullptr)
 {
     PG_TRY(pg_wst(ctx, "bc.dist", (size_t)n * S + S, &a.dist));
     PG_TRY(pg_wst(ctx, "bc.sigma", (size_t)n * S + S, &a.sigma));
@@ -430,6 +447,7 @@ pg_status alloc_state(pg_ctx* ctx, int n, BCArgs& a)
     PG_TRY(pg_d2h(ctx, hR.data(), a.R, sizeof(int32_t) * (n + 1)));
     for (int i = 0; i < n; i++) ord[i] = i;
     std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return hR[x + 1] - hR[x] > hR[y + 1] - hR[y]; });
+    if (max_deg) *max_deg = n > 0 ? hR[ord[0] + 1] - hR[ord[0]] : 0;
     int32_t* dord;
     PG_TRY(pg_wst(ctx, "bc.order", (size_t)n + 1, &dord));
     PG_TRY(pg_h2d(ctx, dord, ord.data(), sizeof(int32_t) * n));
@@ -437,16 +455,52 @@ pg_status alloc_state(pg_ctx* ctx, int n, BCArgs& a)
     return PG_OK;
 }
 
-pg_status launch_brandes(pg_ctx* ctx, BCArgs& a, int batch_first, int batch_last)
+pg_status launch_brandes(pg_ctx* ctx, BCArgs& a, int batch_first, int batch_last, int fwd_first = 1,
+                         int fwd_last = INT_MAX)
 {
     int per_sm = 0;
     PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_brandes, THREADS, 0));
     if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "brandes kernel cannot be resident");
     int grid = per_sm * ctx->sm_count;
-    void* args[] = {(void*)&a, (void*)&batch_first, (void*)&batch_last};
+    void* args[] = {(void*)&a, (void*)&batch_first, (void*)&batch_last, (void*)&fwd_first, (void*)&fwd_last};
     PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_brandes, dim3(grid), dim3(THREADS), args, 0, ctx->stream));
     PG_LAUNCHED(ctx);
     return PG_OK;
+}
+
+// Levels 2 and 3 of every batch on the tensor cores (dense graphs): level 1
+// by the gather kernel, 2 and 3 as exact integer GEMMs, the rest (and the
+// backward sweep) by the gather kernel again.
+constexpr int DENSE_FIRST = 2, DENSE_LAST = 3;
+
+pg_status dense_batch(pg_ctx* ctx, BCArgs& a, int b, BCDense& dn)
+{
+    PG_TRY(launch_brandes(ctx, a, b, b + 1, 1, DENSE_FIRST - 1));
+    for (int d = DENSE_FIRST; d <= DENSE_LAST; d++) {
+        BCLevel lv;
+        lv.sigma = a.sigma;
+        lv.dist = a.dist;
+        lv.seen = a.seen;
+        lv.nxt = a.front + (size_t)(d & 1) * a.n;
+        lv.fprev = a.front + (size_t)((d - 1) & 1) * a.n;
+        lv.fhist = d < LCAP ? a.fhist + (size_t)d * a.n : nullptr;
+        lv.inv = a.inv;
+        lv.flag = nullptr;
+        lv.d = d;
+        PG_TRY(bc_dense_level(ctx, dn, lv));
+    }
+    return launch_brandes(ctx, a, b, b + 1, DENSE_LAST + 1, INT_MAX);
+}
+
+pg_status run_batches(pg_ctx* ctx, BCArgs& a, int nb, BCDense* dn)
+{
+    if (!dn) {
+        const int per_launch = 16;   // a bounded number of batches per launch keeps every launch short
+        for (int b = 0; b < nb; b += per_launch) PG_TRY(launch_brandes(ctx, a, b, std::min(nb, b + per_launch)));
+        return PG_OK;
+    }
+    for (int b = 0; b < nb; b++) PG_TRY(dense_batch(ctx, a, b, *dn));
+    return bc_dense_check(ctx, *dn);
 }
 }  // namespace
 
@@ -461,17 +515,17 @@ extern "C" pg_status pg_betweenness(pg_ctx* ctx, const pg_graph* g, float* bc, d
     a.n = n;
     a.nsrc = n;
     a.do_backward = 1;
-    PG_TRY(alloc_state(ctx, n, a));
+    BCDense dn;
+    PG_TRY(alloc_state(ctx, n, a, &dn.max_deg));
+    const bool dense = bc_dense_eligible(ctx, n, g->nnz, dn.max_deg);
+    if (dense) PG_TRY(bc_dense_setup(ctx, g->R, g->C, n, dn));
     PG_TRY(pg_wst(ctx, "bc.bc", (size_t)n + 1, &a.bc));
     PG_CUDA(ctx, cudaMemsetAsync(a.bc, 0, sizeof(double) * (n + 1), ctx->stream));
     if (eff || lp) {
         PG_TRY(pg_wst(ctx, "bc.inv", (size_t)n + 1, &a.inv));
         PG_CUDA(ctx, cudaMemsetAsync(a.inv, 0, sizeof(double) * (n + 1), ctx->stream));
     }
-    const int nb = (n + S - 1) / S;
-    // a bounded number of batches per launch keeps every launch short
-    const int per_launch = 16;
-    for (int b = 0; b < nb; b += per_launch) PG_TRY(launch_brandes(ctx, a, b, std::min(nb, b + per_launch)));
+    PG_TRY(run_batches(ctx, a, (n + S - 1) / S, dense ? &dn : nullptr));
     float *dbc, *deff = nullptr;
     PG_TRY(pg_wst(ctx, "bc.bcf", (size_t)n + 1, &dbc));
     if (eff) PG_TRY(pg_wst(ctx, "bc.eff", (size_t)n + 1, &deff));
@@ -506,7 +560,10 @@ extern "C" pg_status pg_bfs_sigma(pg_ctx* ctx, const pg_graph* g, const int32_t*
     a.C = g->C;
     a.n = n;
     a.nsrc = ns;
-    PG_TRY(alloc_state(ctx, n, a));
+    BCDense dn;
+    PG_TRY(alloc_state(ctx, n, a, &dn.max_deg));
+    const bool dense = bc_dense_eligible(ctx, n, g->nnz, dn.max_deg);
+    if (dense) PG_TRY(bc_dense_setup(ctx, g->R, g->C, n, dn));
     int32_t* dsrc;
     PG_TRY(pg_wst(ctx, "bc.src", (size_t)ns + 1, &dsrc));
     PG_CUDA(ctx, cudaMemcpyAsync(dsrc, sources, sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream));
@@ -514,7 +571,12 @@ extern "C" pg_status pg_bfs_sigma(pg_ctx* ctx, const pg_graph* g, const int32_t*
     PG_TRY(pg_wst(ctx, "bc.odist", (size_t)S * n, &a.out_dist));
     PG_TRY(pg_wst(ctx, "bc.osigma", (size_t)S * n, &a.out_sigma));
     for (int b = 0; b < (ns + S - 1) / S; b++) {
-        PG_TRY(launch_brandes(ctx, a, b, b + 1));
+        if (dense) {
+            PG_TRY(dense_batch(ctx, a, b, dn));
+            PG_TRY(bc_dense_check(ctx, dn));
+        } else {
+            PG_TRY(launch_brandes(ctx, a, b, b + 1));
+        }
         int cnt = std::min(S, ns - b * S);
         PG_TRY(pg_d2h(ctx, dist + (size_t)b * S * n, a.out_dist, sizeof(int32_t) * (size_t)cnt * n));
         PG_TRY(pg_d2h(ctx, sigma + (size_t)b * S * n, a.out_sigma, sizeof(int64_t) * (size_t)cnt * n));

@@ -69,3 +69,22 @@ def random_weighted(n, p, seed):
 def bench_like(seed=7):
     """A denser synthetic voxel graph with community structure."""
     return from_bold(1500, 120, 0.3, seed)
+
+
+def communities(sizes, p_in, p_link, seed):
+    """Dense random communities in a chain: G(size, p_in) inside each block,
+    G(p_link) between consecutive blocks only, so BFS depth grows with the
+    number of blocks while rows stay long."""
+    rng = np.random.default_rng(seed)
+    n = int(sum(sizes))
+    off = np.cumsum([0] + list(sizes))
+    edges = []
+    for k, sz in enumerate(sizes):
+        a = int(off[k])
+        m = np.triu(rng.random((sz, sz)) < p_in, 1)
+        edges += [(a + int(i), a + int(j)) for i, j in zip(*np.nonzero(m))]
+        if k + 1 < len(sizes):
+            b = int(off[k + 1])
+            m = rng.random((sz, sizes[k + 1])) < p_link
+            edges += [(a + int(i), b + int(j)) for i, j in zip(*np.nonzero(m))]
+    return csr_from_edges(n, edges)

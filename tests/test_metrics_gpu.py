@@ -15,6 +15,10 @@ CASES = {
     "complete30": G.complete(30),
     "bold700": G.from_bold(700, 200, 0.3, 11),
     "bold1500": G.bench_like(),
+    # dense enough for the tensor-core Brandes levels (>= 64 neighbours per
+    # row): max degree 104 (one 8-bit limb) and 325 (two limbs), depth 6 and 4
+    "dense_chain": G.communities([130] * 6, 0.6, 0.03, 1),
+    "dense_blocks": G.communities([420, 420, 420], 0.7, 0.004, 2),
 }
 
 
