@@ -40,10 +40,10 @@ import numpy as np  # noqa: E402
 
 N_VOX, T_LEN, N_SIG, SPARSITY = 58000, 240, 20, 1.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one-pass ncu
-# capture) of one k_brandes launch -- 16 batches of 128 sources -- on the
-# 58000-voxel subject; the workload is deterministic, so it holds for every run
-BRANDES_DRAM_BYTES_PER_LAUNCH_58K = 28.74e9
-BRANDES_SOURCES_PER_LAUNCH = 16 * 128
+# capture) of the k_brandes launches of one 128-source batch (the level-1
+# launch and the resumed launch) on the 58000-voxel subject; the workload is
+# deterministic, so it holds for every run
+BRANDES_DRAM_BYTES_PER_BATCH_58K = 1.127e9
 WORKLOAD = "subject-58k: N=58000 voxels, T=240, 20 latent signals, top 1% |r| -> binary CSR; " \
            "degree, Cp (triangles), Lp/efficiency, Brandes BC all sources, Newman modularity"
 
@@ -288,9 +288,12 @@ def main():
                             "build": info, "nnz": g.info[1], "lp": lp, "Q": Q, "modules": nmod})
         g.free()
 
-    def timed(precision, on_device, steps, warmup, timings=None):
+    def timed(precision, on_device, steps, warmup, timings=None, prof=None):
         for _ in range(warmup):
             subject(precision, on_device)
+        if prof is not None:        # per-kernel events inside the timed steps
+            ctx.profile(True)
+            ctx.profile_reset()
         ms = []
         for _ in range(steps):
             flush.fill_(1)          # evict L2 between timed steps
@@ -306,13 +309,18 @@ def main():
             if world > 1:
                 t = reduce_max_ms(t, f"cuda:{local}")
             ms.append(t)
+        if prof is not None:
+            for k in ("k_brandes", "k_bc_dense"):
+                prof[k] = ctx.kernel_time(k)
+            ctx.profile(False)
         return float(np.mean(ms)), ms
 
     launches0 = ctx.launches
     clocks = ClockSampler(local)
     clocks.start()
     timings = []
-    ms_dev, all_ms = timed(args.precision, True, args.steps, args.warmup, timings)
+    kprof = {}
+    ms_dev, all_ms = timed(args.precision, True, args.steps, args.warmup, timings, prof=kprof)
     clk = clocks.stop()
     launches = (ctx.launches - launches0) // max(1, args.steps + args.warmup)
     ms_e2e, _ = timed(args.precision, False, args.steps, 1)
@@ -375,14 +383,33 @@ def main():
     e2e = world * 60000.0 / ms_e2e
     tm = timings[-1]
     nnz = tm["nnz"]
-    # roofline of the dominant kernel (Brandes sweep, HBM/L2 graph traffic):
-    # algorithmic bytes per source = 2 passes x (nnz*4 col + (N+1)*4 rowptr)
-    # + N * (4 dist + 8 sigma + 8 delta) * 2
-    per_src = 2 * (nnz * 4 + (N_VOX + 1) * 4) + N_VOX * (4 + 8 + 8) * 2
-    bc_bytes = per_src * N_VOX
+    # roofline of the dominant kernel, k_brandes (the gather sweeps of every
+    # 128-source batch: level 1, the levels after the tensor-core ones and the
+    # whole backward sweep), timed with CUDA events around its launches during
+    # the timed steps.  Algorithmic bytes per batch: those of the backward
+    # sweep alone -- per source nnz*4 col + (N+1)*4 rowptr + N*(4 dist +
+    # 8 sigma + 8 delta) -- so the figure leaves out the forward levels the
+    # kernel also runs (conservative).
+    n_batches = (N_VOX + 127) // 128
+    kb_launches, kb_ms = kprof["k_brandes"]
+    kb_ms_batch = kb_ms / max(1, args.steps * n_batches)
+    per_src_bwd = nnz * 4 + (N_VOX + 1) * 4 + N_VOX * (4 + 8 + 8)
+    bytes_batch = per_src_bwd * 128
+    achieved = bytes_batch / (kb_ms_batch / 1000.0) / 1e9 if kb_ms_batch > 0 else None
     bc_s = tm["bc_ms"] / 1000.0
-    achieved = bc_bytes / bc_s / 1e9
     gteps = N_VOX * nnz / bc_s / 1e9
+    # the tensor-core levels (k_bc_dense): one pass over the dense 0/1
+    # adjacency per launch, HBM-bound
+    kd_launches, kd_ms = kprof["k_bc_dense"]
+    np_pad = (N_VOX + 127) // 128 * 128
+    tensor_levels = None
+    if kd_launches:
+        kd_ms_launch = kd_ms / kd_launches
+        tensor_levels = {"kernel": "k_bc_dense", "launches_per_step": kd_launches / args.steps,
+                         "ms_per_launch": kd_ms_launch, "bytes_per_launch": np_pad * np_pad,
+                         "achieved_gbs": np_pad * np_pad / (kd_ms_launch / 1000.0) / 1e9,
+                         "frac": np_pad * np_pad / (kd_ms_launch / 1000.0) / 1e9 / hbm_peak,
+                         "ms_per_step": kd_ms / args.steps}
     line = {
         "metric": "cohort subjects/min @58k voxels", "value": value, "unit": "subjects/min",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev,
@@ -396,11 +423,14 @@ def main():
                 "d2h_bytes_per_step": d2h_bytes},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": "k_brandes", "achieved": achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "traffic": BRANDES_DRAM_BYTES_PER_LAUNCH_58K if N_VOX == 58000 else None,
-                     "algorithmic_bytes_per_launch": per_src * BRANDES_SOURCES_PER_LAUNCH,
-                     "per_launch": "16 batches of 128 sources",
+                     "unit": "GB/s", "frac": achieved / hbm_peak if achieved else None,
+                     "traffic": BRANDES_DRAM_BYTES_PER_BATCH_58K if N_VOX == 58000 else None,
+                     "algorithmic_bytes_per_launch": bytes_batch,
+                     "per_launch": "one 128-source batch (its k_brandes launches); algorithmic bytes of the "
+                                   "backward sweep only",
+                     "ms_per_batch": kb_ms_batch, "launches_per_step": kb_launches / args.steps,
                      "peak_source": peak_kind},
+        "tensor_levels": tensor_levels,
         "bc_gteps": gteps, "bc_mteps_reference_formula": nnz * N_VOX / (tm["bc_ms"]) / 1024 ** 2,
         "stage_ms": {"build": {k: tm["build"][k] for k in ("ms_zscore", "ms_hist", "ms_emit", "ms_select", "ms_csr")},
                      "betweenness_and_paths": tm["bc_ms"], "newman": tm["newman_ms"]},

@@ -57,6 +57,15 @@ pg_status   pg_synchronize(pg_ctx* ctx);
 void*       pg_stream(pg_ctx* ctx);
 /* Number of kernel launches issued by this context so far. */
 int64_t     pg_launch_count(const pg_ctx* ctx);
+/* Per-kernel device time, for measurement harnesses (no counterpart in the
+ * reference).  With profiling on, the library records CUDA events on the
+ * context stream around every launch of its dominant kernels ("k_brandes",
+ * "k_bc_dense"); pg_profile_get returns the launches and summed milliseconds
+ * of one kernel since the last reset (it synchronises the stream).  Off by
+ * default; the events cost a few microseconds per launch. */
+pg_status   pg_profile_enable(pg_ctx* ctx, int32_t on);
+pg_status   pg_profile_reset(pg_ctx* ctx);
+pg_status   pg_profile_get(pg_ctx* ctx, const char* kernel, int64_t* launches, double* ms);
 
 /* ------------------------------------------------------------- graphs */
 /* Replaces the .csr reads of every metric tool (e.g. U/Cp/Cp/Cp_main.cpp:107-116,

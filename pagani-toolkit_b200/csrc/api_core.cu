@@ -76,6 +76,11 @@ extern "C" pg_status pg_destroy(pg_ctx* ctx)
     for (auto& kv : ctx->ws) cudaFree(kv.second.p);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     for (auto& e : ctx->ev) cudaEventDestroy(e);
+    for (auto& sp : ctx->prof_open) {
+        cudaEventDestroy(sp.a);
+        cudaEventDestroy(sp.b);
+    }
+    for (auto& e : ctx->prof_free) cudaEventDestroy(e);
     for (auto& st : ctx->side)
         if (st) cudaStreamDestroy(st);
     cudaStreamDestroy(ctx->stream);
@@ -91,6 +96,85 @@ extern "C" pg_status pg_synchronize(pg_ctx* ctx)
 }
 
 extern "C" void* pg_stream(pg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+// ---------------------------------------------------------------- profiling
+static cudaEvent_t prof_event(pg_ctx* ctx)
+{
+    if (!ctx->prof_free.empty()) {
+        cudaEvent_t e = ctx->prof_free.back();
+        ctx->prof_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+
+int pg_prof_begin(pg_ctx* ctx, const char* name)
+{
+    if (!ctx->prof) return -1;
+    cudaEvent_t a = prof_event(ctx), b = prof_event(ctx);
+    if (!a || !b) return -1;
+    cudaEventRecord(a, ctx->stream);
+    ctx->prof_open.push_back({name, a, b});
+    return (int)ctx->prof_open.size() - 1;
+}
+
+void pg_prof_end(pg_ctx* ctx, int handle)
+{
+    if (handle < 0 || handle >= (int)ctx->prof_open.size()) return;
+    cudaEventRecord(ctx->prof_open[handle].b, ctx->stream);
+}
+
+// Folds the recorded spans into the per-kernel sums (synchronises the stream).
+static pg_status prof_resolve(pg_ctx* ctx)
+{
+    if (ctx->prof_open.empty()) return PG_OK;
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (auto& sp : ctx->prof_open) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) {
+            auto& acc = ctx->prof_sum[sp.name];
+            acc.first++;
+            acc.second += ms;
+        } else {
+            cudaGetLastError();
+        }
+        ctx->prof_free.push_back(sp.a);
+        ctx->prof_free.push_back(sp.b);
+    }
+    ctx->prof_open.clear();
+    return PG_OK;
+}
+
+extern "C" pg_status pg_profile_enable(pg_ctx* ctx, int32_t on)
+{
+    if (!ctx) return PG_ERR_INVALID;
+    PG_TRY(prof_resolve(ctx));
+    ctx->prof = on != 0;
+    return PG_OK;
+}
+
+extern "C" pg_status pg_profile_reset(pg_ctx* ctx)
+{
+    if (!ctx) return PG_ERR_INVALID;
+    PG_TRY(prof_resolve(ctx));
+    ctx->prof_sum.clear();
+    return PG_OK;
+}
+
+extern "C" pg_status pg_profile_get(pg_ctx* ctx, const char* kernel, int64_t* launches, double* ms)
+{
+    if (!ctx || !kernel) return pg_fail(ctx, PG_ERR_INVALID, "pg_profile_get: null argument");
+    PG_TRY(prof_resolve(ctx));
+    auto it = ctx->prof_sum.find(kernel);
+    if (launches) *launches = it == ctx->prof_sum.end() ? 0 : it->second.first;
+    if (ms) *ms = it == ctx->prof_sum.end() ? 0.0 : it->second.second;
+    return PG_OK;
+}
 extern "C" int64_t pg_launch_count(const pg_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 // --------------------------------------------------------------- workspace

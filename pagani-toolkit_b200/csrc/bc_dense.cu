@@ -16,12 +16,13 @@
 //
 // Kernel structure: one persistent CTA of 6 warps per SM over 128-row
 // tiles.  Warp 0 streams K in 128-byte chunks with TMA (128B swizzle) into a
-// 4-stage ring (A tile + one X^T tile per limb) guarded by mbarriers; warp 1
-// issues 4 UMMA (M=128, N=128, K=32) per limb and chunk into one of two TMEM
-// accumulator buffers; warps 2-5 read their 32 TMEM lanes (rows) of the
-// finished buffer and update the batch state while the next tile's MMAs run.  Every mbarrier wait is bounded by the global timer; on
-// expiry the kernel records an error, drains its own copies and MMAs, frees
-// TMEM and returns.
+// ring of 6 (one limb) or 4 (two limbs) stages -- an A tile and one X^T tile
+// per limb -- guarded by mbarriers; warp 1 issues 4 UMMA (M=128, N=128,
+// K=32) per limb and chunk into one of two TMEM accumulator buffers; warps
+// 2-5 read their 32 TMEM lanes (rows) of the finished buffer and update the
+// batch state while the next tile's MMAs run.  Every mbarrier wait is
+// bounded by the global timer; on expiry the kernel records an error, drains
+// its own copies and MMAs, frees TMEM and returns.
 #include "bc_dense.cuh"
 #include "tma.cuh"
 #include <algorithm>
@@ -40,15 +41,15 @@ constexpr uint32_t IDESC_I8 = (2u << 4) | ((uint32_t)(DS >> 3) << 17) | ((uint32
 
 template <int LIMBS>   // 1 or 2 limbs: path counts below 2^16 (max degree < 65536)
 struct DCfg {
-    static constexpr int STAGES = 4;
+    static constexpr int STAGES = LIMBS == 1 ? 6 : 4;   // 192 KB of stages either way
     static constexpr uint32_t STAGE = DTILE * (1 + LIMBS);
     static constexpr uint32_t ACC_COLS = LIMBS * DS;                 // one accumulator buffer
     static constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;              // two buffers: 256 or 512
 };
 
 struct DCtl {
-    u64 full[4];        // stage loaded (TMA complete_tx)
-    u64 empty[4];       // stage consumed (MMA commit)
+    u64 full[6];        // stage loaded (TMA complete_tx)
+    u64 empty[6];       // stage consumed (MMA commit)
     u64 tfull[2];       // accumulator buffer ready (MMA commit)
     u64 tempty[2];      // accumulator buffer read (one arrive per epilogue warp)
     u64 drainbar;
@@ -335,8 +336,10 @@ pg_status launch_level(pg_ctx* ctx, BCDense& d, const BCLevel& lv, int* err)
     const size_t smem = dsmem<LIMBS>();
     PG_CUDA(ctx, cudaFuncSetAttribute(k_bc_dense<LIMBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = std::min(ctx->sm_count, nb);
+    const int prof = pg_prof_begin(ctx, "k_bc_dense");
     k_bc_dense<LIMBS><<<grid, DWARPS * 32, smem, ctx->stream>>>(d.map_adj, map_b, nb, d.np / DKC, a, err);
     PG_LAUNCHED(ctx);
+    pg_prof_end(ctx, prof);
     return PG_OK;
 }
 }  // namespace

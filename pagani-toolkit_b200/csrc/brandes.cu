@@ -463,8 +463,10 @@ pg_status launch_brandes(pg_ctx* ctx, BCArgs& a, int batch_first, int batch_last
     if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "brandes kernel cannot be resident");
     int grid = per_sm * ctx->sm_count;
     void* args[] = {(void*)&a, (void*)&batch_first, (void*)&batch_last, (void*)&fwd_first, (void*)&fwd_last};
+    const int prof = pg_prof_begin(ctx, "k_brandes");
     PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_brandes, dim3(grid), dim3(THREADS), args, 0, ctx->stream));
     PG_LAUNCHED(ctx);
+    pg_prof_end(ctx, prof);
     return PG_OK;
 }
 

@@ -26,6 +26,13 @@ struct pg_ctx {
     // Pinned host staging for small D2H/H2D transfers.
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // Optional per-kernel device time (pg_profile_enable): event pairs around
+    // the launches of named kernels, resolved when read.
+    bool prof = false;
+    struct ProfSpan { const char* name; cudaEvent_t a, b; };
+    std::vector<ProfSpan> prof_open;
+    std::map<std::string, std::pair<int64_t, double>> prof_sum;
+    std::vector<cudaEvent_t> prof_free;
 };
 
 struct pg_graph {
@@ -67,6 +74,13 @@ pg_status pg_fail(pg_ctx* ctx, pg_status s, const char* fmt, ...);
             return pg_fail((ctx), PG_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__,   \
                            cudaGetErrorString(e_));                                     \
     } while (0)
+
+// ------------------------------------------------------------- profiling
+// With profiling on, pg_prof_begin records an event on the context stream
+// before a launch of kernel `name` and returns a handle for pg_prof_end
+// (after the launch); both are no-ops (handle -1) when profiling is off.
+int pg_prof_begin(pg_ctx* ctx, const char* name);
+void pg_prof_end(pg_ctx* ctx, int handle);
 
 // ------------------------------------------------------------- workspace
 // Device buffer named `key`, at least `bytes` long (contents undefined).

@@ -31,7 +31,7 @@ EXPORTS = [
     "pg_fw_batched", "pg_newman", "pg_newman_weighted", "pg_eigen_centrality", "pg_participation", "pg_maslov", "pg_maslov_round_size", "pg_smallworld",
     "pg_clustering_noalloc", "pg_clustering_noalloc_max_nodes",
     "pg_cohort_create", "pg_cohort_add", "pg_cohort_graph", "pg_cohort_packed", "pg_cohort_info",
-    "pg_cohort_free",
+    "pg_cohort_free", "pg_profile_enable", "pg_profile_reset", "pg_profile_get",
 ]
 
 
@@ -119,6 +119,9 @@ def lib():
         L.pg_cohort_packed.argtypes = [vp, vp, vp]
         L.pg_cohort_info.argtypes = [vp, P(i32), P(i32)]
         L.pg_cohort_free.argtypes = [vp]
+        L.pg_profile_enable.argtypes = [vp, i32]
+        L.pg_profile_reset.argtypes = [vp]
+        L.pg_profile_get.argtypes = [vp, ct.c_char_p, P(i64), P(dbl)]
         _lib = L
     return _lib
 
@@ -247,6 +250,19 @@ class Context:
     @property
     def launches(self):
         return int(lib().pg_launch_count(self.h))
+
+    def profile(self, on=True):
+        """Per-kernel event timing on (or off); see kernel_time()."""
+        self._check(lib().pg_profile_enable(self.h, int(on)))
+
+    def profile_reset(self):
+        self._check(lib().pg_profile_reset(self.h))
+
+    def kernel_time(self, name):
+        """(launches, summed ms) of one profiled kernel since the last reset."""
+        n, ms = ct.c_int64(), ct.c_double()
+        self._check(lib().pg_profile_get(self.h, name.encode(), ct.byref(n), ct.byref(ms)))
+        return n.value, ms.value
 
     def synchronize(self):
         self._check(lib().pg_synchronize(self.h))
