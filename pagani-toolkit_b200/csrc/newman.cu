@@ -821,7 +821,10 @@ __device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int3
     for (int i = tid; i < nown; i += nthr) key[i] &= 0xffffu;   // now the row order
     __syncthreads();
     // cost of lanes-per-row L = 2^t: warp 0 takes the first slice of every
-    // round, the longest, so its total bounds the step
+    // round, the longest, so its total bounds the step; a slice costs its
+    // gathers plus a fixed 16 (loop, shuffle tree and row store: measured on
+    // 16-CTA teams of the 58k graphs, where a smaller constant picked L = 16
+    // for some CTAs and made them 20 % slower than their L = 8 neighbours)
     __shared__ long long cost[6], size[6];
     if (tid < 6) {
         const int L = 1 << tid, RPS = 32 / L, ns = (nown + RPS - 1) / RPS, nw = nthr >> 5;
@@ -830,7 +833,7 @@ __device__ int team_slice(Team& tm, const Group& gg, int e0, uint32_t* key, int3
             const int first = (int)key[s * RPS];
             const int it = (tm.oR[first + 1] - tm.oR[first] + L - 1) / L;
             sz += 32LL * it;
-            if (s % nw == 0) c += it + 3 + tid;
+            if (s % nw == 0) c += it + 16 + tid;
         }
         cost[tid] = c;
         size[tid] = sz;
