@@ -289,11 +289,12 @@ def main():
         g.free()
 
     def timed(precision, on_device, steps, warmup, timings=None, prof=None):
+        if prof is not None:        # per-kernel events; the warm-up steps fill the event pool
+            ctx.profile(True)
         for _ in range(warmup):
             subject(precision, on_device)
-        if prof is not None:        # per-kernel events inside the timed steps
-            ctx.profile(True)
-            ctx.profile_reset()
+        if prof is not None:
+            ctx.profile_reset()     # only the timed steps count
         ms = []
         for _ in range(steps):
             flush.fill_(1)          # evict L2 between timed steps
