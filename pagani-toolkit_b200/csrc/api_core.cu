@@ -64,6 +64,14 @@ extern "C" pg_status pg_create(pg_ctx** out, int device)
         return PG_ERR_CUDA;
     }
     for (auto& e : ctx->ev) cudaEventCreate(&e);
+    // graphs come from the device's stream-ordered pool; keeping freed
+    // blocks in the pool makes the per-subject graph allocation cheap
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     *out = ctx;
     return PG_OK;
 }
@@ -239,9 +247,12 @@ pg_status pg_graph_alloc(pg_ctx* ctx, int32_t n, int64_t nnz, bool weighted, pg_
     g->device = ctx->device;
     g->n = n;
     g->nnz = nnz;
-    cudaError_t e = cudaMalloc(&g->R, sizeof(int32_t) * ((size_t)n + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&g->C, sizeof(int32_t) * (size_t)(nnz > 0 ? nnz : 1));
-    if (e == cudaSuccess && weighted) e = cudaMalloc(&g->V, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));
+    // stream-ordered on the context stream (pg_graph_free's cudaFree waits for
+    // the device before the blocks return to the pool)
+    cudaError_t e = cudaMallocAsync((void**)&g->R, sizeof(int32_t) * ((size_t)n + 1), ctx->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&g->C, sizeof(int32_t) * (size_t)(nnz > 0 ? nnz : 1), ctx->stream);
+    if (e == cudaSuccess && weighted)
+        e = cudaMallocAsync((void**)&g->V, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1), ctx->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(g->R); cudaFree(g->C); cudaFree(g->V);

@@ -295,3 +295,26 @@ def test_newman_whole_grid_groups(ctx):
     labels, Q, nm = ctx.newman_weighted(g, gpu_rule_above=5000)
     lab_or, Q_or, nm_or = O.newman_weighted(R, C, V, gpu_rule_above=5000)
     assert nm == nm_or and np.array_equal(labels, lab_or)
+
+
+def test_dense_brandes_levels_take_the_tensor_core_path(ctx):
+    """Per-kernel profiling shows where Brandes ran: a dense graph takes two
+    tensor-core launches (levels 2 and 3) and two gather launches per
+    128-source batch, a sparse graph only the gather kernel."""
+    R, C, _ = CASES["dense_blocks"]
+    g = ctx.graph(R, C)
+    batches = (len(R) - 1 + 127) // 128
+    ctx.profile(True)
+    ctx.profile_reset()
+    try:
+        ctx.betweenness(g)
+        nd, msd = ctx.kernel_time("k_bc_dense")
+        nb, _ = ctx.kernel_time("k_brandes")
+        assert nd == 2 * batches and nb == 2 * batches and msd > 0
+        ctx.profile_reset()
+        R2, C2, _ = CASES["bold700"]
+        ctx.betweenness(ctx.graph(R2, C2))
+        assert ctx.kernel_time("k_bc_dense")[0] == 0
+        assert ctx.kernel_time("k_brandes")[0] >= 1
+    finally:
+        ctx.profile(False)
