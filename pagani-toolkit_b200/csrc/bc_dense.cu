@@ -87,15 +87,81 @@ struct DArgs {
     int* flag;
 };
 
+// Work units of one launch: tiles [0, nreg) whole (the full rounds of the
+// persistent grid); each remaining tail tile split into `spl` parts along K,
+// whose int32 partial sums are added (exactly, in any order) into `tail`,
+// [tail tile][row][limb column]; k_bc_dense_tail then updates those rows.
+struct DUnits {
+    int ntiles, nk, nreg, spl;
+    int32_t* tail;
+    __device__ __forceinline__ int count() const { return nreg + (ntiles - nreg) * spl; }
+    // tile of unit u, its chunk range, and its tail index (-1: a whole tile)
+    __device__ __forceinline__ void get(int u, int& tile, int& c0, int& c1, int& ti) const
+    {
+        if (u < nreg) {
+            tile = u;
+            c0 = 0;
+            c1 = nk;
+            ti = -1;
+            return;
+        }
+        const int j = u - nreg, part = j % spl;
+        ti = j / spl;
+        tile = nreg + ti;
+        c0 = (int)((long long)nk * part / spl);
+        c1 = (int)((long long)nk * (part + 1) / spl);
+    }
+};
+
+// Level-d update of row v from its path counts: load(cb, r) fills the limb
+// values of sources 32 cb .. 32 cb + 31.  Returns true if a source reached v.
+template <int LIMBS, class Load>
+__device__ __forceinline__ bool update_row(const DArgs& a, int v, Load load)
+{
+    const bool valid = v < a.n;
+    const ulonglong2 sv = valid ? a.seen[v] : make_ulonglong2(0ULL, 0ULL);
+    u64 nb0 = 0ULL, nb1 = 0ULL;
+#pragma unroll 1
+    for (int cb = 0; cb < DS / 32; cb++) {
+        uint32_t r[LIMBS][32];
+        load(cb, r);
+        const u64 seenw = cb < 2 ? sv.x : sv.y;
+        const int sh = (cb & 1) * 32;
+        uint32_t bits = 0u;
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+            u64 sg = r[0][c];
+            if (LIMBS > 1) sg += (u64)r[1][c] << 8;
+            const bool nw = sg != 0ULL && !((seenw >> (sh + c)) & 1ULL);
+            if (nw && valid) {
+                const size_t at = (size_t)v * DS + cb * 32 + c;
+                a.sigma[at] = sg;
+                a.dist[at] = a.d;
+            }
+            bits |= (uint32_t)nw << c;
+        }
+        if (cb < 2) nb0 |= (u64)bits << sh;
+        else nb1 |= (u64)bits << sh;
+    }
+    if (!valid) return false;
+    const ulonglong2 nb = make_ulonglong2(nb0, nb1);
+    a.nxt[v] = nb;
+    a.seen[v] = make_ulonglong2(sv.x | nb.x, sv.y | nb.y);
+    if (a.fhist) a.fhist[v] = nb;
+    if (!(nb.x | nb.y)) return false;
+    if (a.inv) a.inv[v] += (double)(__popcll(nb.x) + __popcll(nb.y)) / (double)a.d;
+    return true;
+}
+
 // Warp roles: warp 0 lane 0 streams the operand tiles with TMA, warp 1 lane
 // 0 issues the MMAs, warps 2-5 run the epilogue (warp w reads TMEM lanes
 // 32 (w % 4) .. + 31).  The accumulator is double-buffered in TMEM, so the
-// MMAs of the next row tile overlap the epilogue of this one.
+// MMAs of the next unit overlap the epilogue of this one.
 constexpr int DWARPS = 6;
 
 template <int LIMBS>
 __global__ void __launch_bounds__(DWARPS * 32, 1)
-k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, int ntiles, int nk,
+k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, DUnits un,
            DArgs a, int* __restrict__ err)
 {
     using Cfg = DCfg<LIMBS>;
@@ -105,6 +171,7 @@ k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CU
     DCtl* ctl = (DCtl*)(smem + ST * Cfg::STAGE);
     volatile int* abort_flag = &ctl->abort;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int units = un.count();
     if (t == 0) {
         for (int s = 0; s < ST; s++) {
             mbar_init(&ctl->full[s], 1);
@@ -135,8 +202,10 @@ k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CU
         // ---- producer
         if (lane == 0) {
             long long q = 0;
-            for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x)
-                for (int c = 0; c < nk; c++) {
+            for (int u = blockIdx.x; u < units && !*abort_flag; u += gridDim.x) {
+                int tile, c0, c1, ti;
+                un.get(u, tile, c0, c1, ti);
+                for (int c = c0; c < c1; c++) {
                     const int s = (int)(q % ST);
                     if (!mbar_wait(&ctl->empty[s], (uint32_t)((q / ST) & 1) ^ 1u) || *abort_flag) {
                         *abort_flag = 1;
@@ -151,19 +220,22 @@ k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CU
                     q++;
                     ctl->issued = q;
                 }
+            }
         }
     } else if (warp == 1) {
         // ---- MMA issuer
         if (lane == 0) {
             long long q = 0;
             int tl = 0;
-            for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, tl++) {
+            for (int u = blockIdx.x; u < units && !*abort_flag; u += gridDim.x, tl++) {
+                int tile, c0, c1, ti;
+                un.get(u, tile, c0, c1, ti);
                 const int buf = tl & 1;
                 if (!mbar_wait(&ctl->tempty[buf], (uint32_t)((tl >> 1) & 1) ^ 1u)) { *abort_flag = 1; break; }
                 tc_fence_after();
                 const uint32_t dst = tmem + (uint32_t)(buf * Cfg::ACC_COLS);
                 bool ok = true;
-                for (int c = 0; c < nk; c++) {
+                for (int c = c0; c < c1; c++) {
                     const int s = (int)(q % ST);
                     if (!mbar_wait(&ctl->full[s], (uint32_t)((q / ST) & 1)) || *abort_flag) { ok = false; break; }
                     tc_fence_after();
@@ -174,7 +246,8 @@ k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CU
                         const u64 o = (u64)(kk * 32) >> 4;   // 32 B per K=32 step
 #pragma unroll
                         for (int l = 0; l < LIMBS; l++)
-                            umma_i8(dst + (uint32_t)(l * DS), ad + o, sdesc(st + DTILE * (1 + l)) + o, (c | kk) != 0);
+                            umma_i8(dst + (uint32_t)(l * DS), ad + o, sdesc(st + DTILE * (1 + l)) + o,
+                                    (c != c0) | (kk != 0));
                     }
                     umma_commit(&ctl->empty[s]);
                     q++;
@@ -185,11 +258,13 @@ k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CU
             }
         }
     } else {
-        // ---- epilogue: row 32 (warp % 4) + lane of the tile, 32 sources at a time
+        // ---- epilogue: row 32 (warp % 4) + lane of the unit's tile
         const int quarter = warp & 3;
         bool found = false;
         int tl = 0;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, tl++) {
+        for (int u = blockIdx.x; u < units; u += gridDim.x, tl++) {
+            int tile, c0, c1, ti;
+            un.get(u, tile, c0, c1, ti);
             const int buf = tl & 1;
             const bool ok = mbar_wait(&ctl->tfull[buf], (uint32_t)((tl >> 1) & 1)) && !*abort_flag;
             if (!ok) {
@@ -197,48 +272,31 @@ k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CU
                 break;
             }
             tc_fence_after();
-            const int v = tile * DM + quarter * 32 + lane;
-            const bool valid = v < a.n;
-            const ulonglong2 sv = valid ? a.seen[v] : make_ulonglong2(0ULL, 0ULL);
-            u64 nb0 = 0ULL, nb1 = 0ULL;
+            const int row = quarter * 32 + lane;
             const uint32_t src = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * Cfg::ACC_COLS);
+            if (ti < 0) {
+                found |= update_row<LIMBS>(a, tile * DM + row, [&](int cb, uint32_t (&r)[LIMBS][32]) {
+#pragma unroll
+                    for (int l = 0; l < LIMBS; l++) tmem_ld32(src + (uint32_t)(l * DS + cb * 32), r[l]);
+                });
+            } else {
+                // a part of a tail tile: add its partial sums (exact int32)
+                int32_t* dst = un.tail + ((size_t)ti * DM + row) * (LIMBS * DS);
 #pragma unroll 1
-            for (int cb = 0; cb < DS / 32; cb++) {
-                uint32_t r[LIMBS][32];
+                for (int l = 0; l < LIMBS; l++)
+#pragma unroll 1
+                    for (int cb = 0; cb < DS / 32; cb++) {
+                        uint32_t r[32];
+                        tmem_ld32(src + (uint32_t)(l * DS + cb * 32), r);
 #pragma unroll
-                for (int l = 0; l < LIMBS; l++) tmem_ld32(src + (uint32_t)(l * DS + cb * 32), r[l]);
-                const u64 seenw = cb < 2 ? sv.x : sv.y;
-                const int sh = (cb & 1) * 32;
-                uint32_t bits = 0u;
-#pragma unroll
-                for (int c = 0; c < 32; c++) {
-                    u64 sg = r[0][c];
-                    if (LIMBS > 1) sg += (u64)r[1][c] << 8;
-                    const bool nw = sg != 0ULL && !((seenw >> (sh + c)) & 1ULL);
-                    if (nw && valid) {
-                        const size_t at = (size_t)v * DS + cb * 32 + c;
-                        a.sigma[at] = sg;
-                        a.dist[at] = a.d;
+                        for (int c = 0; c < 32; c++)
+                            if (r[c]) atomicAdd(dst + l * DS + cb * 32 + c, (int32_t)r[c]);
                     }
-                    bits |= (uint32_t)nw << c;
-                }
-                if (cb < 2) nb0 |= (u64)bits << sh;
-                else nb1 |= (u64)bits << sh;
             }
             // the accumulator buffer may be overwritten once every epilogue warp has read it
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl->tempty[buf]);
-            if (valid) {
-                const ulonglong2 nb = make_ulonglong2(nb0, nb1);
-                a.nxt[v] = nb;
-                a.seen[v] = make_ulonglong2(sv.x | nb.x, sv.y | nb.y);
-                if (a.fhist) a.fhist[v] = nb;
-                if (nb.x | nb.y) {
-                    if (a.inv) a.inv[v] += (double)(__popcll(nb.x) + __popcll(nb.y)) / (double)a.d;
-                    found = true;
-                }
-            }
         }
         if (found) ctl->found = 1;
     }
@@ -255,6 +313,24 @@ k_bc_dense(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CU
     __syncthreads();
     if (t == 0 && ctl->found && a.flag) atomicExch(a.flag, 1);
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
+}
+
+// The rows of the split tail tiles, from their summed partial counts.
+template <int LIMBS>
+__global__ void k_bc_dense_tail(DUnits un, DArgs a)
+{
+    const int ntail = un.ntiles - un.nreg;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ntail * DM; g += gridDim.x * blockDim.x) {
+        const int ti = g / DM, row = g % DM;
+        const int32_t* srcp = un.tail + ((size_t)ti * DM + row) * (LIMBS * DS);
+        const bool f = update_row<LIMBS>(a, (un.nreg + ti) * DM + row, [&](int cb, uint32_t (&r)[LIMBS][32]) {
+#pragma unroll
+            for (int l = 0; l < LIMBS; l++)
+#pragma unroll
+                for (int c = 0; c < 32; c++) r[l][c] = (uint32_t)srcp[l * DS + cb * 32 + c];
+        });
+        if (f && a.flag) atomicExch(a.flag, 1);
+    }
 }
 
 // X^T for level d: row l * 128 + s holds limb l of sigma[u][s] for u on
@@ -317,7 +393,7 @@ bool make_map_u8(CUtensorMap* m, const uint8_t* base, int rows, int cols)
 template <int LIMBS>
 pg_status launch_level(pg_ctx* ctx, BCDense& d, const BCLevel& lv, int* err)
 {
-    const int nb = d.np / DM;
+    const int nb = d.np / DM, nk = d.np / DKC;
     k_bc_xt<LIMBS><<<d.np / 64, 256, 0, ctx->stream>>>(lv.sigma, lv.fprev, d.n, d.np, d.xt);
     PG_LAUNCHED(ctx);
     CUtensorMap map_b;
@@ -333,12 +409,28 @@ pg_status launch_level(pg_ctx* ctx, BCDense& d, const BCLevel& lv, int* err)
     a.fhist = lv.fhist;
     a.inv = lv.inv;
     a.flag = lv.flag;
+    const int grid = std::min(ctx->sm_count, nb);
+    // whole tiles for the full rounds of the grid; the last partial round's
+    // tiles split along K over the idle CTAs (at least 8 chunks per part)
+    DUnits un;
+    un.ntiles = nb;
+    un.nk = nk;
+    un.nreg = nb / grid * grid;
+    un.spl = 1;
+    un.tail = d.tail;
+    const int ntail = nb - un.nreg;
+    if (un.nreg > 0 && ntail > 0) un.spl = std::max(1, std::min(grid / ntail, nk / 8));
+    if (un.spl == 1) un.nreg = nb;   // no split: every tile whole
+    else PG_CUDA(ctx, cudaMemsetAsync(d.tail, 0, sizeof(int32_t) * (size_t)ntail * DM * LIMBS * DS, ctx->stream));
     const size_t smem = dsmem<LIMBS>();
     PG_CUDA(ctx, cudaFuncSetAttribute(k_bc_dense<LIMBS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = std::min(ctx->sm_count, nb);
     const int prof = pg_prof_begin(ctx, "k_bc_dense");
-    k_bc_dense<LIMBS><<<grid, DWARPS * 32, smem, ctx->stream>>>(d.map_adj, map_b, nb, d.np / DKC, a, err);
+    k_bc_dense<LIMBS><<<grid, DWARPS * 32, smem, ctx->stream>>>(d.map_adj, map_b, un, a, err);
     PG_LAUNCHED(ctx);
+    if (un.nreg < nb) {
+        k_bc_dense_tail<LIMBS><<<ceil_div((long long)ntail * DM, 128), 128, 0, ctx->stream>>>(un, a);
+        PG_LAUNCHED(ctx);
+    }
     pg_prof_end(ctx, prof);
     return PG_OK;
 }
@@ -368,6 +460,8 @@ pg_status bc_dense_setup(pg_ctx* ctx, const int32_t* R, const int32_t* C, int n,
     PG_TRY(pg_wst(ctx, "bc.adj", np * np, &d.adj));
     PG_TRY(pg_wst(ctx, "bc.xt", 2 * DS * np, &d.xt));
     PG_TRY(pg_wst(ctx, "bc.dense_err", 1, &d.err));
+    // partial sums of tail tiles: fewer tail tiles than SMs, two limbs at most
+    PG_TRY(pg_wst(ctx, "bc.dense_tail", (size_t)std::max(ctx->sm_count, 1) * DM * 2 * DS, &d.tail));
     PG_CUDA(ctx, cudaMemsetAsync(d.err, 0, sizeof(int), ctx->stream));
     PG_CUDA(ctx, cudaMemsetAsync(d.adj, 0, np * np, ctx->stream));
     k_bc_adj<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(R, C, n, d.np, d.adj);

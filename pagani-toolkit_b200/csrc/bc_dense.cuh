@@ -13,6 +13,7 @@ struct BCDense {
     uint8_t* adj = nullptr;      // np x np, adj[v * np + u] = 1 for an edge
     uint8_t* xt = nullptr;       // limbs (<= 2) x 128 x np: level-(d-1) path counts, transposed
     int* err = nullptr;          // set when a pipeline wait timed out
+    int32_t* tail = nullptr;     // partial sums of the K-split tail tiles
     CUtensorMap map_adj;
 };
 

@@ -318,3 +318,27 @@ def test_dense_brandes_levels_take_the_tensor_core_path(ctx):
         assert ctx.kernel_time("k_brandes")[0] >= 1
     finally:
         ctx.profile(False)
+
+
+def test_dense_levels_with_split_tail_tiles(ctx):
+    """A 20,000-node dense graph has more 128-row tiles (157) than SMs: the
+    tiles of the last partial round are split along K and their partial
+    path counts summed; sigma and levels stay exact."""
+    from pagani import synth
+    N = 20000
+    bold = synth.bold_series(N, 120, 10, 77)
+    g, _ = ctx.build_graph(bold, mode="s", value=2.0, sign="abs")
+    R, C, _ = g.to_csr()
+    assert R[-1] >= 64 * N                       # dense: the tensor-core levels run
+    src = np.random.default_rng(9).integers(0, N, size=40).astype(np.int32)
+    ctx.profile(True)
+    ctx.profile_reset()
+    try:
+        dist, sigma = ctx.bfs_sigma(g, src)
+        assert ctx.kernel_time("k_bc_dense")[0] == 2
+    finally:
+        ctx.profile(False)
+    for q, s in enumerate(src):
+        d_or, s_or = O.bfs_source(R, C, int(s))
+        assert np.array_equal(dist[q], d_or)
+        assert np.array_equal(sigma[q], s_or)
