@@ -277,6 +277,48 @@ pg_status pg_smallworld(double cp, const double* cp_rand, int32_t n_cp, double l
                         const double* lp_rand, int32_t n_lp, double* gamma, double* lambda,
                         double* sigma);
 
+/* ------------------------------------------------------ batched subjects */
+/* A cohort through the whole path in one call: the reference runs CUCorMat,
+ * Degree, Cp, BFS_MulCPU / CUBC, Newman_Modularity, Maslov and
+ * SmallWorldProperty as separate programs over a directory
+ * (main() of U/CorMat/CUCorMat/CUCORMAT/CorMat.cpp:51,
+ * U/Degree/Degree/Degree.cpp:12, U/Cp/Cp/Cp_main.cpp:28,
+ * U/BC/CUBC/CUBC_main.cpp:15, U/cuda_EC/cuda_EC/modularity_GPU.cu:532 and
+ * W/SmallWorldProperty/SmallWorldProperty.cpp:14); here each subject's graph stays on the device
+ * while every requested metric runs.  Subjects may differ in N and T.
+ * Output arrays are host buffers of N entries; NULL skips the metric.  With
+ * bc set, eff and lp come from the Brandes sweep, else from pg_paths; cp uses
+ * Onnela's formula when build.weighted is set.  n_random > 0 adds that many
+ * Maslov surrogates per subject (swaps_per_edge x edges attempts, seed
+ * pg_surrogate_seed(seed, subject, r)) and their clustering and hop path
+ * length for gamma, lambda and sigma. */
+typedef struct {
+    const float* bold;       /* T x N float32 (device pointer with build.input_on_device) */
+    int32_t N, T;
+    float* degree;           /* pg_degree */
+    float* cp;               /* pg_clustering */
+    float* eff;              /* nodal efficiency */
+    float* bc;               /* pg_betweenness */
+    int32_t* modules;        /* pg_newman labels */
+    int64_t edges;           /* results */
+    double tau, cp_mean, lp, Q;
+    int32_t n_modules;
+    double gamma, lambda, sigma;
+} pg_subject;
+
+typedef struct {
+    pg_build_opts build;
+    int32_t n_random;
+    int64_t swaps_per_edge;
+    uint64_t seed;
+} pg_run_opts;
+
+/* Defaults: pg_build_opts_default, no surrogates, 2 swap attempts per edge
+ * (U/cuda_EC/cuda_EC/Maslov.cpp:19 tries 2M), seed 1. */
+void      pg_run_opts_default(pg_run_opts* o);
+uint64_t  pg_surrogate_seed(uint64_t base, int32_t subject, int32_t r);
+pg_status pg_run_subjects(pg_ctx* ctx, pg_subject* subjects, int32_t n, const pg_run_opts* opts);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,7 @@ EXPORTS = [
     "pg_clustering_noalloc", "pg_clustering_noalloc_max_nodes",
     "pg_cohort_create", "pg_cohort_add", "pg_cohort_graph", "pg_cohort_packed", "pg_cohort_info",
     "pg_cohort_free", "pg_profile_enable", "pg_profile_reset", "pg_profile_get",
+    "pg_run_opts_default", "pg_surrogate_seed", "pg_run_subjects",
 ]
 
 
@@ -59,6 +60,19 @@ class BuildInfo(ct.Structure):
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Subject(ct.Structure):
+    _fields_ = [("bold", ct.c_void_p), ("N", ct.c_int32), ("T", ct.c_int32), ("degree", ct.c_void_p),
+                ("cp", ct.c_void_p), ("eff", ct.c_void_p), ("bc", ct.c_void_p), ("modules", ct.c_void_p),
+                ("edges", ct.c_int64), ("tau", ct.c_double), ("cp_mean", ct.c_double), ("lp", ct.c_double),
+                ("Q", ct.c_double), ("n_modules", ct.c_int32), ("gamma", ct.c_double), ("lambda_", ct.c_double),
+                ("sigma", ct.c_double)]
+
+
+class RunOpts(ct.Structure):
+    _fields_ = [("build", BuildOpts), ("n_random", ct.c_int32), ("swaps_per_edge", ct.c_int64),
+                ("seed", ct.c_uint64)]
 
 
 LOG_FN = ct.CFUNCTYPE(None, ct.c_char_p, ct.c_void_p)
@@ -122,6 +136,11 @@ def lib():
         L.pg_profile_enable.argtypes = [vp, i32]
         L.pg_profile_reset.argtypes = [vp]
         L.pg_profile_get.argtypes = [vp, ct.c_char_p, P(i64), P(dbl)]
+        L.pg_run_opts_default.argtypes = [P(RunOpts)]
+        L.pg_run_opts_default.restype = None
+        L.pg_surrogate_seed.argtypes = [ct.c_uint64, i32, i32]
+        L.pg_surrogate_seed.restype = ct.c_uint64
+        L.pg_run_subjects.argtypes = [vp, P(Subject), i32, P(RunOpts)]
         _lib = L
     return _lib
 
@@ -312,6 +331,36 @@ class Context:
     def cohort(self, N, fisher=False, weighted=False):
         """Subject averaging (CUCorMat to_average yn/yf): a Cohort of N voxels."""
         return Cohort(self, N, fisher, weighted)
+
+    def run_subjects(self, bolds, mode="s", value=1.0, sign="abs", n_random=0, swaps_per_edge=2, seed=1,
+                     metrics=("degree", "cp", "eff", "bc", "modules")):
+        """pg_run_subjects over (T, N) float32 series: one dict per subject with
+        the requested per-node arrays and the scalar results."""
+        o = RunOpts()
+        lib().pg_run_opts_default(ct.byref(o))
+        o.build.mode = PG_THRESH_SPARSITY if mode in ("s", "sparsity") else PG_THRESH_R
+        o.build.value = value
+        o.build.sign = PG_ABS if sign == "abs" else PG_SIGNED
+        o.n_random, o.swaps_per_edge, o.seed = n_random, swaps_per_edge, seed
+        keep, subs = [], (Subject * max(1, len(bolds)))()
+        outs = []
+        for k, b in enumerate(bolds):
+            b = np.ascontiguousarray(b, np.float32)
+            T, N = b.shape
+            arrs = {m: np.zeros(N, np.int32 if m == "modules" else np.float32) for m in metrics}
+            keep += [b] + list(arrs.values())
+            subs[k].bold, subs[k].N, subs[k].T = b.ctypes.data, N, T
+            for m, a in arrs.items():
+                setattr(subs[k], m, a.ctypes.data)
+            outs.append(arrs)
+        self._check(lib().pg_run_subjects(self.h, subs, len(bolds), ct.byref(o)))
+        res = []
+        for k, arrs in enumerate(outs):
+            d = dict(arrs)
+            for f in ("edges", "tau", "cp_mean", "lp", "Q", "n_modules", "gamma", "lambda_", "sigma"):
+                d[f.rstrip("_")] = getattr(subs[k], f)
+            res.append(d)
+        return res
 
     # ------------------------------------------------------------- metrics
     def degree(self, g):
