@@ -14,6 +14,14 @@ sweep) and Newman leading-eigenvector modularity.
   e2e    -- the same through the C ABI with the series in pinned host memory:
             the host->device copy of the series and the device->host copy of
             every per-node result are inside the timed region.
+  roofline -- the dominant kernel, k_brandes (Brandes gather sweeps), timed
+            with CUDA events around its launches during the timed steps
+            (pg_profile_*), against the algorithmic bytes of its backward sweep
+            and the measured HBM copy peak; tensor_levels gives the same for
+            k_bc_dense (Brandes levels 2-3 as int8 tensor-core GEMMs, one pass
+            over the dense adjacency per launch).
+  extras -- eigenvector centrality and subject averaging (FP64 cohort Gram
+            with the Fisher transform) on the same subject, outside the step.
 
 --impl reference times the reference's own CPU code of the path (compiled
 from its sources into oracle/_ref/) on the host cores; see cpu_baseline().
