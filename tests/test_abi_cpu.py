@@ -62,3 +62,16 @@ def test_no_gpu_fails_loudly():
         pytest.skip("a GPU is present")
     with pytest.raises(pagani.PaganiError):
         pagani.Context(0)
+
+
+def test_run_opts_defaults_and_surrogate_seeds():
+    lib = pagani.lib()
+    o = pagani.RunOpts()
+    lib.pg_run_opts_default(ct.byref(o))
+    b = pagani.BuildOpts()
+    lib.pg_build_opts_default(ct.byref(b))
+    assert bytes(o.build) == bytes(b)
+    assert (o.n_random, o.swaps_per_edge, o.seed) == (0, 2, 1)
+    seeds = {lib.pg_surrogate_seed(7, s, r) for s in range(50) for r in range(20)}
+    assert len(seeds) == 1000                      # one stream per (subject, surrogate)
+    assert lib.pg_surrogate_seed(7, 3, 4) == lib.pg_surrogate_seed(7, 3, 4)
