@@ -134,6 +134,29 @@ def reduce_max_ms(t_ms, device):
     return float(tt.item())
 
 
+def _free_port():
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _spawned(local, world, port, fn, fn_args):
+    os.environ.update(RANK=str(local), LOCAL_RANK=str(local), WORLD_SIZE=str(world),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    fn(*fn_args)
+
+
+def spawn_ranks(world, fn, *fn_args):
+    """Start `world` ranks of fn(*fn_args) on this node, one process each, with
+    RANK / LOCAL_RANK / WORLD_SIZE / MASTER_ADDR / MASTER_PORT set as torchrun
+    sets them (used when bench.py --gpus N is started without torchrun)."""
+    import torch.multiprocessing as mp
+    mp.spawn(_spawned, args=(world, _free_port(), fn, fn_args), nprocs=world, join=True)
+
+
 def rank_subject_seed(rank):
     """Every replica processes its own subject stream."""
     from pagani import synth
@@ -248,9 +271,16 @@ def main():
     ap.add_argument("--voxels", type=int, default=N_VOX,
                     help="profiling aid: a smaller subject for ncu captures (the metric is quoted at 58000)")
     args = ap.parse_args()
+    if args.gpus > 1 and "RANK" not in os.environ:
+        spawn_ranks(args.gpus, run, args)   # started without torchrun
+        return
+    run(args)
+
+
+def run(args):
     set_voxels(args.voxels)
     rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -176,11 +176,16 @@ pg_status pg_clustering(pg_ctx* ctx, const pg_graph* g, int32_t kind, int32_t fl
  * triangles (int64[n], may be NULL) are DEVICE pointers owned by the caller;
  * work is issued on `stream` (a cudaStream_t, NULL = legacy default stream)
  * and is not waited for.  Scratch is a 16 MiB static device array inside the
- * library: n is limited to pg_clustering_noalloc_max_nodes() (larger n returns
- * PG_ERR_TOO_LARGE), every GPU that loads the library holds the array until
- * exit, and calls that overlap on the GPU race on it.  The first call on a
- * device resolves the array's device address (with that device current);
- * make that first call before any stream capture.  No cudaMalloc/cudaFree. */
+ * library, and the neighbour bitmap of a node (n bits) lives in shared memory:
+ * n is limited to pg_clustering_noalloc_max_nodes(), the smaller of the
+ * array's 2,097,150 nodes and the bitmap's limit on the current device
+ * (1,826,816 nodes on a B200); larger n returns PG_ERR_TOO_LARGE.  Every GPU
+ * that loads the library holds the array until exit, and calls that overlap
+ * on the GPU race on it.  The first call on a device (and the first call after
+ * cudaDeviceReset gives the device a new context) resolves the array's device
+ * address and caches the SM count and shared-memory limit, with that device
+ * current; make that first call before any stream capture.  No
+ * cudaMalloc/cudaFree. */
 pg_status pg_clustering_noalloc(const int32_t* R, const int32_t* C, int32_t n, float* cp, int64_t* triangles,
                                 void* stream);
 int64_t   pg_clustering_noalloc_max_nodes(void);

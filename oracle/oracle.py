@@ -29,7 +29,10 @@ _vp = ct.c_void_p
 def build(ref: bool | None = None) -> None:
     """Compile liboracle.so (and the reference groups when the tree exists)."""
     targets = ["all"]
-    ref_root = os.environ.get("PAGANI_REF_ROOT", "/root/reference")
+    # the reference checkout: PAGANI_REF_ROOT, else a "reference" directory
+    # beside the repository
+    ref_root = os.environ.get("PAGANI_REF_ROOT", os.path.join(os.path.dirname(HERE), "..", "reference"))
+    ref_root = os.path.abspath(ref_root)
     if ref is None:
         ref = os.path.isdir(ref_root)
     if ref:

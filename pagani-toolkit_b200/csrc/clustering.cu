@@ -10,6 +10,8 @@
 // which halves the work (each triangle is then counted twice at each of its
 // three nodes).
 #include "pg_internal.cuh"
+#include <cuda.h>
+#include <algorithm>
 #include <cmath>
 
 namespace {
@@ -321,44 +323,91 @@ namespace {
 constexpr int64_t NOALLOC_SCRATCH_WORDS = (16LL << 20) / 8;   // 16 MiB: n + 2 counters
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
 constexpr int NOALLOC_MAX_DEVICES = 64;
-static unsigned long long* g_noalloc_ptr[NOALLOC_MAX_DEVICES];   // device address, per device
+constexpr int NOALLOC_SMEM_SLACK = 4096;   // static shared memory of k_triangles and margin
+
+// Set-up state per device, filled by the first call with that device
+// current: the array's device address (the host-side symbol is only a
+// stand-in), the SM count and the opt-in shared memory per block, and the id
+// of the CUDA context they belong to.  A new context on the device (after
+// cudaDeviceReset) has a new id, and the next call resolves the address again.
+struct NoallocDevice {
+    unsigned long long* scratch;
+    unsigned long long ctx_id;
+    int sm_count;
+    int smem_optin;
+};
+static NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
 
 __global__ void k_noalloc_clear(unsigned long long* __restrict__ w, int64_t count)
 {
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x)
         w[q] = 0ULL;
 }
+
+// Largest n whose neighbour bitmap (n bits) fits the opt-in shared memory.
+int64_t noalloc_smem_nodes(int smem_optin) { return (int64_t)(smem_optin - NOALLOC_SMEM_SLACK) / 4 * 32; }
+
+bool current_ctx_id(unsigned long long* id)
+{
+    CUcontext c = nullptr;
+    if (cuCtxGetCurrent(&c) != CUDA_SUCCESS || !c) return false;
+    return cuCtxGetId(c, id) == CUDA_SUCCESS;
+}
+
+pg_status noalloc_setup(int dev, NoallocDevice** out)
+{
+    NoallocDevice& d = g_noalloc_dev[dev];
+    unsigned long long id = 0;
+    if (d.scratch && current_ctx_id(&id) && id == d.ctx_id) {
+        *out = &d;
+        return PG_OK;
+    }
+    void* p = nullptr;   // resolving the symbol also initialises the device's context
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PG_ERR_CUDA;
+    int sms = 0, optin = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+        return PG_ERR_CUDA;
+    if (!current_ctx_id(&id)) return PG_ERR_CUDA;
+    d.scratch = (unsigned long long*)p;
+    d.ctx_id = id;
+    d.sm_count = sms;
+    d.smem_optin = optin;
+    *out = &d;
+    return PG_OK;
+}
 }  // namespace
 
-extern "C" int64_t pg_clustering_noalloc_max_nodes(void) { return NOALLOC_SCRATCH_WORDS - 2; }
+extern "C" int64_t pg_clustering_noalloc_max_nodes(void)
+{
+    int64_t lim = NOALLOC_SCRATCH_WORDS - 2;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess)
+        lim = std::min(lim, noalloc_smem_nodes(optin));
+    return lim;
+}
 
 extern "C" pg_status pg_clustering_noalloc(const int32_t* R, const int32_t* C, int32_t n, float* cp, int64_t* triangles,
                                            void* stream)
 {
     if (!R || !cp || n < 0) return PG_ERR_INVALID;
-    if ((int64_t)n > pg_clustering_noalloc_max_nodes()) return PG_ERR_TOO_LARGE;
+    if ((int64_t)n > NOALLOC_SCRATCH_WORDS - 2) return PG_ERR_TOO_LARGE;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PG_ERR_NO_DEVICE;
-    // First call on this device: resolve the array's device address with the
-    // device current (the host-side symbol is not a device address).
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PG_ERR_CUDA;
-        g_noalloc_ptr[dev] = (unsigned long long*)p;
-    }
+    NoallocDevice* d = nullptr;
+    if (pg_status st = noalloc_setup(dev, &d); st != PG_OK) return st;
     if (n == 0) return PG_OK;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return PG_ERR_CUDA;
-    size_t smem = (size_t)((n + 31) / 32) * 4;
-    if (smem > prop.sharedMemPerBlockOptin - 4096) return PG_ERR_TOO_LARGE;
+    if ((int64_t)n > noalloc_smem_nodes(d->smem_optin)) return PG_ERR_TOO_LARGE;
+    const size_t smem = (size_t)((n + 31) / 32) * 4;
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(k_triangles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return PG_ERR_CUDA;
     cudaStream_t st = (cudaStream_t)stream;
-    unsigned long long* tri2 = g_noalloc_ptr[dev];
+    unsigned long long* tri2 = d->scratch;
     int* next_node = (int*)(tri2 + (n + 1));
-    k_noalloc_clear<<<prop.multiProcessorCount, 256, 0, st>>>(tri2, (int64_t)n + 2);
-    k_triangles<<<prop.multiProcessorCount * 4, THREADS, smem, st>>>(R, C, n, tri2, next_node);
-    k_cp_binary<<<prop.multiProcessorCount * 4, 256, 0, st>>>(R, n, tri2, cp, (long long*)triangles);
+    k_noalloc_clear<<<d->sm_count, 256, 0, st>>>(tri2, (int64_t)n + 2);
+    k_triangles<<<d->sm_count * 4, THREADS, smem, st>>>(R, C, n, tri2, next_node);
+    k_cp_binary<<<d->sm_count * 4, 256, 0, st>>>(R, n, tri2, cp, (long long*)triangles);
     return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_CUDA;
 }

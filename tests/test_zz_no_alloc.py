@@ -44,3 +44,58 @@ def test_noalloc_rejects_too_many_nodes():
     R = torch.zeros(4, dtype=torch.int32, device="cuda")
     out = torch.zeros(4, dtype=torch.float32, device="cuda")
     assert lib.pg_clustering_noalloc(R.data_ptr(), R.data_ptr(), big, out.data_ptr(), None, None) == 4  # PG_ERR_TOO_LARGE
+
+
+def _ring_lattice(n, k, extra, seed):
+    """n nodes, each joined to its k nearest neighbours on either side (so
+    every node is in triangles), plus `extra` random chords; CSR built with
+    numpy so that graphs of millions of nodes take seconds."""
+    rng = np.random.default_rng(seed)
+    src = np.repeat(np.arange(n, dtype=np.int64), k)
+    dst = (src + np.tile(np.arange(1, k + 1), n)) % n
+    a = rng.integers(0, n, extra)
+    b = rng.integers(0, n, extra)
+    src = np.concatenate([src, a])
+    dst = np.concatenate([dst, b])
+    keep = src != dst
+    u = np.concatenate([src[keep], dst[keep]])
+    v = np.concatenate([dst[keep], src[keep]])
+    key = np.unique(u * n + v)
+    rows = key // n
+    C = (key % n).astype(np.int32)
+    R = np.zeros(n + 1, np.int64)
+    np.add.at(R, rows + 1, 1)
+    return np.cumsum(R).astype(np.int32), C
+
+
+def test_noalloc_large_shared_memory_path():
+    """n above 393,216 needs more than 48 KB of dynamic shared memory for the
+    neighbour bitmap (the opt-in path); two calls in a row."""
+    import torch
+    lib = pagani.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    R, C = _ring_lattice(450_000, 3, 200_000, 63)
+    with pagani.Context(0) as ctx:
+        cp_ref, tri_ref, _ = ctx.clustering(ctx.graph(R, C))
+    for _ in range(2):
+        st, cp, tri = _call(lib, torch, R, C, stream)
+        assert st == 0
+        assert np.array_equal(tri, tri_ref)
+        assert np.array_equal(cp, cp_ref)
+
+
+def test_noalloc_limit_is_reachable():
+    """A graph of exactly the advertised number of nodes is accepted (the
+    rejection of one node more is the test above)."""
+    import torch
+    lib = pagani.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    nmax = int(lib.pg_clustering_noalloc_max_nodes())
+    assert 0 < nmax <= 2_097_150
+    R, C = _ring_lattice(nmax, 2, 0, 64)
+    st, cp, tri = _call(lib, torch, R, C, stream)
+    assert st == 0
+    # a ring lattice with two neighbours a side: every node sits in exactly 3
+    # triangles among its 4 neighbours, Cp = 3 / 6
+    assert np.all(tri == 3)
+    assert np.all(cp == np.float32(0.5))
