@@ -99,6 +99,8 @@ typedef struct {
     int32_t zero_variance;   /* voxels with zero variance (their r is 0) */
     double  sparsity_percent;/* 100 * edges / M1 */
     double  ms_zscore, ms_hist, ms_emit, ms_select, ms_csr; /* device time per stage */
+    double  band_err_max;    /* max |r_tile - r| over the band pairs (r: FP64 recheck) */
+    double  band_err_mean;   /* mean of the same */
 } pg_build_info;
 
 /* Defaults: r mode 0.3, signed, split-BF16, binary, guard 2e-3, host input. */

@@ -206,6 +206,67 @@ def brandes(R, C):
     return bc
 
 
+# ------------------------------------------- subject-size restatements
+_big = None
+
+
+def big_lib():
+    """liboracle_big.so (oracle_big.c): threaded, vectorised restatements with
+    the results of the functions above, for subjects of tens of thousands of
+    voxels."""
+    global _big
+    if _big is None:
+        path = os.path.join(HERE, "liboracle_big.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-s", "-C", HERE, "big"], check=True)
+        L = _load(path)
+        L.or_big_topk.argtypes = [_f64p, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int64, ct.c_int,
+                                  _f64p, _i32p, _i32p]
+        L.or_big_topk.restype = ct.c_int64
+        L.or_brandes_mt.argtypes = [_i32p, _i32p, ct.c_int, ct.c_int, _f64p, _vp]
+        _big = L
+    return _big
+
+
+def big_topk(z, kmax, abs_mode=False, weighted=False, threads=None):
+    """The kmax pairs of largest key (r or |r|) in (key desc, i asc, j asc)
+    order; the first k of them are graph_k's edge set for k edges and
+    keys[k-1] its tau."""
+    z = np.ascontiguousarray(z, np.float64)
+    N, T = z.shape
+    kmax = min(int(kmax), N * (N - 1) // 2)
+    keys = np.empty(max(kmax, 1), np.float64)
+    ii = np.empty(max(kmax, 1), np.int32)
+    jj = np.empty(max(kmax, 1), np.int32)
+    n = big_lib().or_big_topk(z, N, T, int(abs_mode), int(weighted), kmax, threads or os.cpu_count() or 1,
+                              keys, ii, jj)
+    if n < 0:
+        raise MemoryError("or_big_topk ran out of memory")
+    return keys[:n], ii[:n], jj[:n]
+
+
+def csr_from_pairs(N, ii, jj):
+    """Binary CSR (both directions, ascending columns) of undirected pairs."""
+    u = np.concatenate([ii, jj]).astype(np.int64)
+    v = np.concatenate([jj, ii]).astype(np.int64)
+    order = np.argsort(u * N + v, kind="stable")
+    C = v[order].astype(np.int32)
+    R = np.zeros(N + 1, np.int64)
+    np.add.at(R, u + 1, 1)
+    return np.cumsum(R).astype(np.int32), C
+
+
+def brandes_mt(R, C, threads=None, with_inv_sum=False):
+    """or_brandes with the sources split over threads; with_inv_sum also
+    returns sum_v 1/d(s, v) per source (or_bfs_paths' inv_sum)."""
+    N = len(R) - 1
+    bc = np.empty(N, np.float64)
+    inv = np.empty(N, np.float64) if with_inv_sum else None
+    big_lib().or_brandes_mt(np.ascontiguousarray(R, np.int32), np.ascontiguousarray(C, np.int32), N,
+                            threads or os.cpu_count() or 1, bc, _ptr(inv))
+    return (bc, inv) if with_inv_sum else bc
+
+
 def fw_dense(d):
     d = np.ascontiguousarray(d, dtype=np.float32).copy()
     lib().or_fw_dense(d, d.shape[0])

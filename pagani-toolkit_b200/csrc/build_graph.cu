@@ -77,14 +77,35 @@ __device__ __forceinline__ double exact_r(const double* __restrict__ z64, int T,
     return (r >= -1.0 && r <= 1.0) ? r : 0.0;
 }
 
-__global__ void k_recheck(const int2* __restrict__ band, long long nband, const double* __restrict__ z64, int T,
-                          int weighted, int abs_mode, double* __restrict__ key64)
+// FP64 r of every band pair, and the error of the tile's r against it:
+// err[0] = bits of max |r_tile - r| (non-negative doubles order as their
+// bits), err[1] = sum of |r_tile - r| (r before the range rule).
+__global__ void k_recheck(const int2* __restrict__ band, const float* __restrict__ band_r, long long nband,
+                          const double* __restrict__ z64, int T, int weighted, int abs_mode,
+                          double* __restrict__ key64, unsigned long long* __restrict__ err)
 {
+    double emax = 0.0, esum = 0.0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nband;
          q += (long long)gridDim.x * blockDim.x) {
         int2 e = band[q];
-        double r = exact_r(z64, T, e.x, e.y, weighted);
+        const double* a = z64 + (long long)e.x * T;
+        const double* b = z64 + (long long)e.y * T;
+        double r = 0.0;
+        for (int t = 0; t < T; t++) r = __fma_rn(a[t], b[t], r);
+        const double d = fabs((double)band_r[q] - r);
+        emax = fmax(emax, d);
+        esum += d;
+        if (weighted) r = (r > -1.0 - 1e-6 && r < 1.0 + 1e-6) ? r : 0.0;
+        else r = (r >= -1.0 && r <= 1.0) ? r : 0.0;
         key64[q] = abs_mode ? fabs(r) : r;
+    }
+    for (int o = 16; o; o >>= 1) {
+        emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+        esum += __shfl_xor_sync(0xffffffffu, esum, o);
+    }
+    if ((threadIdx.x & 31) == 0 && esum > 0.0) {
+        atomicMax(&err[0], (unsigned long long)__double_as_longlong(emax));
+        atomicAdd((double*)&err[1], esum);
     }
 }
 
@@ -422,11 +443,13 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
     // ---- emit pass
     int2 *pairs, *band;
     float* pw = nullptr;
+    float* band_r;
     unsigned long long* counters;
     const long long cap_total = cap_pairs + cap_band;
     PG_TRY(pg_wst(ctx, "b.pairs", (size_t)std::max(1LL, cap_total), &pairs));
     if (o.weighted) PG_TRY(pg_wst(ctx, "b.pw", (size_t)std::max(1LL, cap_total), &pw));
     PG_TRY(pg_wst(ctx, "b.band", (size_t)std::max(1LL, cap_band), &band));
+    PG_TRY(pg_wst(ctx, "b.band_r", (size_t)std::max(1LL, cap_band), &band_r));
     PG_TRY(pg_wst(ctx, "b.counters", 4, &counters));
     PG_CUDA(ctx, cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), ctx->stream));
     p.lo_cut = lo_cut;
@@ -436,6 +459,7 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
     p.n_pairs = counters;
     p.cap_pairs = cap_pairs;
     p.band = band;
+    p.band_r = band_r;
     p.n_band = counters + 1;
     p.cap_band = cap_band;
     if (M1 > 0 && cap_total > 0) PG_TRY(run_gram(ctx, z, o.precision, EPI_EMIT, p));
@@ -455,7 +479,8 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
     if (n_band > 0) {
         PG_TRY(pg_wst(ctx, "b.key64", (size_t)n_band, &key64));
         int grid = std::max(1, std::min(ctx->sm_count * 16, ceil_div(n_band, 128)));
-        k_recheck<<<grid, 128, 0, ctx->stream>>>(band, n_band, z.z64, T, p.weighted, p.abs_mode, key64);
+        k_recheck<<<grid, 128, 0, ctx->stream>>>(band, band_r, n_band, z.z64, T, p.weighted, p.abs_mode, key64,
+                                                 counters + 2);
         PG_LAUNCHED(ctx);
     }
     int strict_only = 1;
@@ -529,6 +554,15 @@ extern "C" pg_status pg_build_graph(pg_ctx* ctx, const float* bold, int32_t N, i
     cudaEventElapsedTime(&ms, ev[2], ev[3]); inf.ms_emit = ms;
     cudaEventElapsedTime(&ms, ev[3], ev[4]); inf.ms_select = ms;
     cudaEventElapsedTime(&ms, ev[4], ev[5]); inf.ms_csr = ms;
+    if (n_band > 0) {
+        unsigned long long err[2];
+        PG_TRY(pg_d2h(ctx, err, counters + 2, sizeof err));
+        double emax, esum;
+        memcpy(&emax, &err[0], 8);
+        memcpy(&esum, &err[1], 8);
+        inf.band_err_max = emax;
+        inf.band_err_mean = esum / (double)n_band;
+    }
     inf.tau = tau;
     inf.edges = n_edges;
     inf.sparsity_percent = M1 > 0 ? 100.0 * (double)n_edges / (double)M1 : 0.0;

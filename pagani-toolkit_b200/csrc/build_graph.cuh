@@ -41,6 +41,7 @@ struct EpiParams {
     unsigned long long* n_pairs;
     long long cap_pairs;
     int2* band;                    // band pairs (i < j)
+    float* band_r;                 // the tile's r of every band pair
     unsigned long long* n_band;
     long long cap_band;
 };
@@ -129,7 +130,10 @@ __device__ __forceinline__ void epi_emit_masks(unsigned int m1, unsigned int m2,
                 }
                 s1++;
             } else {
-                if (s2 < p.cap_band) p.band[s2] = make_int2(i, j);
+                if (s2 < p.cap_band) {
+                    p.band[s2] = make_int2(i, j);
+                    p.band_r[s2] = r;
+                }
                 s2++;
             }
         }

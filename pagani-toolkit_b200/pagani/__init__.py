@@ -56,7 +56,8 @@ class BuildInfo(ct.Structure):
     _fields_ = [("tau", ct.c_double), ("edges", ct.c_int64), ("band_pairs", ct.c_int64),
                 ("above_pairs", ct.c_int64), ("zero_variance", ct.c_int32),
                 ("sparsity_percent", ct.c_double), ("ms_zscore", ct.c_double), ("ms_hist", ct.c_double),
-                ("ms_emit", ct.c_double), ("ms_select", ct.c_double), ("ms_csr", ct.c_double)]
+                ("ms_emit", ct.c_double), ("ms_select", ct.c_double), ("ms_csr", ct.c_double),
+                ("band_err_max", ct.c_double), ("band_err_mean", ct.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from pagani import synth
 
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_small.npz"))
 N = GOLD["bold"].shape[1]
@@ -105,3 +106,39 @@ def test_sparsity_count_formula_matches_reference_float_arithmetic():
     assert O.sparsity_k(58000, 1.0) == 16819709
     assert O.sparsity_k(58000, 0.5) == 8409855
     assert O.sparsity_k(5000, 1.0) == 124975
+
+
+def test_oracle_matches_reference_at_config1_size():
+    """The restatement against the reference's own pipeline on the
+    5,000-voxel configuration (tests/golden/config1_5000.npz): edge set equal
+    except on the listed pairs within 1e-6 of the threshold, and on the
+    reference's CSR identical Cp floats and Newman labels, betweenness and
+    efficiency within the reference's float accumulation."""
+    import os as _os
+    fx = np.load(_os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "golden", "config1_5000.npz"))
+    N = int(fx["N"])
+    bold = synth.bold_series(N, int(fx["T"]), int(fx["signals"]), int(fx["seed"]))
+    z, _ = O.zscore(bold)
+    r = O.corr_packed(z)
+    iu = np.triu_indices(N, 1)
+    keep = r > float(fx["thr"])
+    near = np.zeros(len(r), bool)
+    near_idx = fx["near_i"].astype(np.int64) * N - fx["near_i"].astype(np.int64) * (fx["near_i"] + 1) // 2 \
+        + fx["near_j"] - fx["near_i"] - 1
+    near[near_idx] = True
+    assert np.array_equal(r[near_idx], fx["near_r64"])
+    keep[near_idx] = fx["near_ref_keep"].astype(bool)          # the reference's decision there
+    R, C = O.csr_from_pairs(N, iu[0][keep].astype(np.int32), iu[1][keep].astype(np.int32))
+    import hashlib
+    h = hashlib.sha256()
+    h.update(R.tobytes())
+    h.update(C.tobytes())
+    assert h.hexdigest() == str(fx["csr_sha256"])
+    tri, cp, _ = O.cp_binary(R, C)
+    assert np.array_equal(cp, fx["cp"])
+    labels, _, _, _ = O.newman(R, C)
+    assert np.array_equal(labels, fx["labels"])
+    bc, inv = O.brandes_mt(R, C, with_inv_sum=True)
+    np.testing.assert_allclose(bc, fx["bc"], rtol=1e-4, atol=1e-2)
+    # APSP_BFS sums 1/d over ~5,000 targets in float: up to ~3e-5 relative here
+    np.testing.assert_allclose(inv / (N - 1), fx["li"], rtol=1e-4)
