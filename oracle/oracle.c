@@ -736,17 +736,21 @@ int or_newman_weighted(const int32_t* R, const int32_t* C, const float* Vw, int6
 }
 
 /* --------------------------------------------------------- Maslov rewiring */
-/* Degree-preserving double-edge swaps, restating Rewire/Maslov of
+/* Maslov-Sneppen rewiring: Rewire/Maslov,
  * U/cuda_EC/cuda_EC/Maslov.cpp:8-109 and the weighted variant
  * Maslov_weighted_1, W/Maslov/Maslov/Maslov.cpp:50-196 (weights stay with the
  * edge slot that carries them).  The reference draws from srand(time(0)) /
- * rand(); this restatement uses a seeded counter-based generator and runs the
- * attempts in rounds of B = pg_maslov_round_size(M): inside a round every
- * attempt reads the state left by the previous round, valid attempts claim
- * their four end points (lowest attempt index wins) and only attempts that
- * own all four commit.  Committed attempts of one round touch disjoint
- * vertices and slots, so they commute.  This is the exact schedule of the
- * GPU kernel, which makes the two bit-identical for the same seed. */
+ * rand() and evaluates its attempts one after another.  This restatement
+ * uses a seeded counter-based generator (attempt a: stream bits 2a and
+ * 2a + 1) and the round schedule of the GPU kernel: a round
+ * holds the attempts deferred by the previous round plus fresh ones, up to
+ * B = or_maslov_round_size(M); every attempt of a round is evaluated on the
+ * state the previous round left; an attempt the reference would reject there
+ * is decided; a valid attempt claims its two slots and the table entries of
+ * its two new pairs (lowest attempt index wins); attempts owning all four
+ * commit (they touch disjoint slots and create distinct pairs, so they
+ * commute) and the others are deferred.  Every requested attempt is
+ * evaluated once; the result is the GPU kernel's bit for bit. */
 static inline uint64_t mix64(uint64_t z)
 {
     z += 0x9E3779B97F4A7C15ULL;
@@ -758,10 +762,30 @@ static inline uint64_t mix64(uint64_t z)
 int64_t or_maslov_round_size(int64_t M);
 int64_t or_maslov_round_size(int64_t M)
 {
-    int64_t b = M / 16;
-    if (b < 1) b = 1;
-    if (b > 65536) b = 65536;
+    int64_t b = M / 32;
+    if (b < 64) b = 64;
+    if (b > (1LL << 20)) b = 1LL << 20;
     return b;
+}
+
+static uint32_t maslov_table_size(int64_t B)
+{
+    uint32_t h = 1024;
+    while ((int64_t)h < 64 * B) h <<= 1;
+    return h;
+}
+
+/* Random bits q of the stream of `seed`: splitmix64 outputs at counter q of
+ * a key derived from the seed, so streams of different seeds do not overlap
+ * (a plain seed ^ q would make the streams of small seeds permutations of
+ * one another). */
+static inline uint64_t stream_key(uint64_t seed) { return mix64(seed ^ 0xD1B54A32D192ED03ULL); }
+static inline uint64_t stream_bits(uint64_t key, uint64_t q) { return mix64(key + q * 0x9E3779B97F4A7C15ULL); }
+
+static inline uint32_t pair_entry(int a, int b, int64_t N, uint32_t hmask)
+{
+    uint64_t lo = (uint64_t)(a < b ? a : b), hi = (uint64_t)(a < b ? b : a);
+    return (uint32_t)(mix64(lo * (uint64_t)N + hi) & hmask);
 }
 
 static inline int has_edge(const uint64_t* bits, int64_t N, int a, int b)
@@ -775,72 +799,12 @@ static inline void set_edge(uint64_t* bits, int64_t N, int a, int b, int on)
     if (on) bits[q >> 6] |= 1ULL << (q & 63); else bits[q >> 6] &= ~(1ULL << (q & 63));
 }
 
-int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uint64_t seed,
-                  int64_t attempts, int32_t* R_out, int32_t* C_out, float* V_out)
+/* CSR of the rewired slots with ascending columns; each undirected slot's
+ * weight goes to both directions (Maslov_weighted_1's vu/vl re-attachment,
+ * W/Maslov/Maslov/Maslov.cpp:145-186); R is unchanged (degrees preserved). */
+static void maslov_rebuild(const int32_t* R, int N, int64_t M, const int32_t* ea, const int32_t* eb,
+                           const float* ew, int32_t* R_out, int32_t* C_out, float* V_out)
 {
-    int64_t M = R[N] / 2;
-    int32_t* ea = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
-    int32_t* eb = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
-    float* ew = (float*)malloc((size_t)(M > 0 ? M : 1) * sizeof(float));
-    size_t words = (size_t)(((uint64_t)N * (uint64_t)N + 63) / 64);
-    uint64_t* bits = (uint64_t*)calloc(words > 0 ? words : 1, sizeof(uint64_t));
-    int64_t m = 0;
-    for (int i = 0; i < N; i++)
-        for (int32_t e = R[i]; e < R[i + 1]; e++) {
-            set_edge(bits, N, i, C[e], 1);
-            if (C[e] > i) { ea[m] = i; eb[m] = C[e]; ew[m] = V ? V[e] : 1.0f; m++; }
-        }
-    int64_t committed = 0;
-    int64_t B = or_maslov_round_size(M);
-    int64_t* owner = (int64_t*)malloc((size_t)(N > 0 ? N : 1) * sizeof(int64_t));
-    for (int i = 0; i < N; i++) owner[i] = INT64_MAX;
-    int32_t* av = (int32_t*)malloc((size_t)B * 4 * sizeof(int32_t));
-    int64_t* ai = (int64_t*)malloc((size_t)B * 2 * sizeof(int64_t));
-    unsigned char* ok = (unsigned char*)malloc((size_t)B);
-    unsigned char* coin = (unsigned char*)malloc((size_t)B);
-    for (int64_t base = 0; M >= 2 && base < attempts; base += B) {
-        int64_t nb = attempts - base < B ? attempts - base : B;
-        for (int64_t a = 0; a < nb; a++) {
-            uint64_t idx = (uint64_t)(base + a);
-            uint64_t h1 = mix64(seed ^ (2 * idx)), h2 = mix64(seed ^ (2 * idx + 1));
-            int64_t i = (int64_t)(h1 % (uint64_t)M), j = (int64_t)(h2 % (uint64_t)M);
-            int c = (int)((h1 >> 63) ^ (h2 >> 63));
-            int V1 = ea[i], V2 = eb[i], V3 = ea[j], V4 = eb[j];
-            int valid = !(V1 == V3 || V1 == V4 || V2 == V3 || V2 == V4);
-            if (valid) {
-                if (c) valid = !(has_edge(bits, N, V1, V3) || has_edge(bits, N, V2, V4));
-                else   valid = !(has_edge(bits, N, V1, V4) || has_edge(bits, N, V2, V3));
-            }
-            av[4 * a] = V1; av[4 * a + 1] = V2; av[4 * a + 2] = V3; av[4 * a + 3] = V4;
-            ai[2 * a] = i; ai[2 * a + 1] = j; ok[a] = (unsigned char)valid; coin[a] = (unsigned char)c;
-            if (valid)
-                for (int q = 0; q < 4; q++) if (owner[av[4 * a + q]] > (int64_t)a) owner[av[4 * a + q]] = a;
-        }
-        for (int64_t a = 0; a < nb; a++) {
-            if (!ok[a]) continue;
-            int own = 1;
-            for (int q = 0; q < 4; q++) own &= owner[av[4 * a + q]] == a;
-            if (!own) continue;
-            int V1 = av[4 * a], V2 = av[4 * a + 1], V3 = av[4 * a + 2], V4 = av[4 * a + 3];
-            int64_t i = ai[2 * a], j = ai[2 * a + 1];
-            set_edge(bits, N, V1, V2, 0); set_edge(bits, N, V2, V1, 0);
-            set_edge(bits, N, V3, V4, 0); set_edge(bits, N, V4, V3, 0);
-            if (coin[a]) {   /* 1-3, 2-4 (Maslov.cpp:31-42) */
-                set_edge(bits, N, V1, V3, 1); set_edge(bits, N, V3, V1, 1);
-                set_edge(bits, N, V2, V4, 1); set_edge(bits, N, V4, V2, 1);
-                eb[i] = V3; ea[j] = V2;
-            } else {         /* 1-4, 3-2 (Maslov.cpp:44-55) */
-                set_edge(bits, N, V1, V4, 1); set_edge(bits, N, V4, V1, 1);
-                set_edge(bits, N, V2, V3, 1); set_edge(bits, N, V3, V2, 1);
-                eb[i] = V4; eb[j] = V2;
-            }
-            committed++;
-        }
-        for (int64_t a = 0; a < nb; a++)
-            for (int q = 0; q < 4; q++) owner[av[4 * a + q]] = INT64_MAX;
-    }
-    /* Rebuild CSR with ascending columns; each undirected slot's weight goes to
-     * both directions (Maslov_weighted_1's vu/vl re-attachment, :160-186). */
     int64_t* cur = (int64_t*)malloc((size_t)(N + 1) * sizeof(int64_t));
     for (int i = 0; i <= N; i++) R_out[i] = R[i];
     int32_t* tmpc = (int32_t*)malloc((size_t)(R[N] > 0 ? R[N] : 1) * sizeof(int32_t));
@@ -862,7 +826,185 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
     memcpy(C_out, tmpc, sizeof(int32_t) * (size_t)R[N]);
     if (V_out) memcpy(V_out, tmpw, sizeof(float) * (size_t)R[N]);
     free(tmpc); free(tmpw); free(cur);
-    free(ea); free(eb); free(ew); free(bits); free(owner); free(av); free(ai); free(ok); free(coin);
+}
+
+typedef struct {
+    uint64_t a;
+    int v[4];
+    int64_t i, j;
+    uint32_t h[2];        /* table entries of the two new pairs */
+    int state;            /* 0 shared end point, 1 new edge exists, 2 valid */
+    int coin;
+} MsItem;
+
+int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uint64_t seed,
+                  int64_t attempts, int32_t* R_out, int32_t* C_out, float* V_out)
+{
+    int64_t M = R[N] / 2;
+    int32_t* ea = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
+    int32_t* eb = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
+    float* ew = (float*)malloc((size_t)(M > 0 ? M : 1) * sizeof(float));
+    size_t words = (size_t)(((uint64_t)N * (uint64_t)N + 63) / 64);
+    uint64_t* bits = (uint64_t*)calloc(words > 0 ? words : 1, sizeof(uint64_t));
+    int64_t m = 0;
+    for (int i = 0; i < N; i++)
+        for (int32_t e = R[i]; e < R[i + 1]; e++) {
+            set_edge(bits, N, i, C[e], 1);
+            if (C[e] > i) { ea[m] = i; eb[m] = C[e]; ew[m] = V ? V[e] : 1.0f; m++; }
+        }
+    int64_t committed = 0;
+    const int64_t B = or_maslov_round_size(M);
+    const uint32_t H = maslov_table_size(B), hmask = H - 1;
+    /* claims of valid attempts, then the writes of committed ones */
+    uint64_t* slot_owner = (uint64_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(uint64_t));
+    uint64_t* table = (uint64_t*)malloc((size_t)H * sizeof(uint64_t));
+    uint64_t* slot_wr = (uint64_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(uint64_t));
+    uint64_t* pair_wr = (uint64_t*)malloc((size_t)H * sizeof(uint64_t));
+    for (int64_t q = 0; q < M; q++) slot_owner[q] = slot_wr[q] = UINT64_MAX;
+    for (uint32_t q = 0; q < H; q++) table[q] = pair_wr[q] = UINT64_MAX;
+    MsItem* items = (MsItem*)malloc((size_t)B * sizeof(MsItem));
+    unsigned char* commit = (unsigned char*)malloc((size_t)B);
+    uint64_t* pend = (uint64_t*)malloc((size_t)B * sizeof(uint64_t));
+    uint64_t* pnext = (uint64_t*)malloc((size_t)B * sizeof(uint64_t));
+    int64_t np = 0;
+    uint64_t fresh = 0;
+    const uint64_t key = stream_key(seed);
+    while (M >= 2) {
+        uint64_t left = (uint64_t)attempts - fresh;
+        uint64_t take = left < (uint64_t)(B - np) ? left : (uint64_t)(B - np);
+        int64_t total = np + (int64_t)take;
+        if (total == 0) break;
+        /* evaluate on the round's state; valid attempts claim */
+        for (int64_t it = 0; it < total; it++) {
+            MsItem* t = &items[it];
+            t->a = it < np ? pend[it] : fresh + (uint64_t)(it - np);
+            uint64_t h1 = stream_bits(key, 2 * t->a), h2 = stream_bits(key, 2 * t->a + 1);
+            t->i = (int64_t)(h1 % (uint64_t)M);
+            t->j = (int64_t)(h2 % (uint64_t)M);
+            t->coin = (int)((h1 >> 63) ^ (h2 >> 63));
+            t->v[0] = ea[t->i]; t->v[1] = eb[t->i]; t->v[2] = ea[t->j]; t->v[3] = eb[t->j];
+            int x1 = t->v[0], x2 = t->coin ? t->v[2] : t->v[3];   /* 1-3 or 1-4 */
+            int y1 = t->v[1], y2 = t->coin ? t->v[3] : t->v[2];   /* 2-4 or 2-3 */
+            t->h[0] = pair_entry(x1, x2, N, hmask);
+            t->h[1] = pair_entry(y1, y2, N, hmask);
+            if (t->v[0] == t->v[2] || t->v[0] == t->v[3] || t->v[1] == t->v[2] || t->v[1] == t->v[3]) t->state = 0;
+            else if (has_edge(bits, N, x1, x2) || has_edge(bits, N, y1, y2)) t->state = 1;
+            else t->state = 2;
+            if (t->state == 2) {
+                if (slot_owner[t->i] > t->a) slot_owner[t->i] = t->a;
+                if (slot_owner[t->j] > t->a) slot_owner[t->j] = t->a;
+                if (table[t->h[0]] > t->a) table[t->h[0]] = t->a;
+                if (table[t->h[1]] > t->a) table[t->h[1]] = t->a;
+            }
+        }
+        /* valid attempts owning all four claims commit: record their writes */
+        for (int64_t it = 0; it < total; it++) {
+            MsItem* t = &items[it];
+            commit[it] = t->state == 2 && slot_owner[t->i] == t->a && slot_owner[t->j] == t->a &&
+                         table[t->h[0]] == t->a && table[t->h[1]] == t->a;
+            if (!commit[it]) continue;
+            uint32_t o1 = pair_entry(t->v[0], t->v[1], N, hmask), o2 = pair_entry(t->v[2], t->v[3], N, hmask);
+            slot_wr[t->i] = slot_wr[t->j] = t->a;
+            uint32_t w[4] = {o1, o2, t->h[0], t->h[1]};
+            for (int q = 0; q < 4; q++) if (pair_wr[w[q]] > t->a) pair_wr[w[q]] = t->a;
+        }
+        /* apply the commits; a rejected attempt whose reads a lower-index
+         * commit wrote is deferred, as is every valid attempt that lost */
+        int64_t nn = 0;
+        for (int64_t it = 0; it < total; it++) {
+            MsItem* t = &items[it];
+            if (t->state == 2 && !commit[it]) { pnext[nn++] = t->a; continue; }
+            if (t->state < 2) {
+                int stale = slot_wr[t->i] < t->a || slot_wr[t->j] < t->a;
+                if (t->state == 1) stale |= pair_wr[t->h[0]] < t->a || pair_wr[t->h[1]] < t->a;
+                if (stale) pnext[nn++] = t->a;
+                continue;
+            }
+            int V1 = t->v[0], V2 = t->v[1], V3 = t->v[2], V4 = t->v[3];
+            set_edge(bits, N, V1, V2, 0); set_edge(bits, N, V2, V1, 0);
+            set_edge(bits, N, V3, V4, 0); set_edge(bits, N, V4, V3, 0);
+            if (t->coin) {   /* 1-3, 2-4 (Maslov.cpp:36-44) */
+                set_edge(bits, N, V1, V3, 1); set_edge(bits, N, V3, V1, 1);
+                set_edge(bits, N, V2, V4, 1); set_edge(bits, N, V4, V2, 1);
+                eb[t->i] = V3; ea[t->j] = V2;
+            } else {         /* 1-4, 3-2 (Maslov.cpp:47-56) */
+                set_edge(bits, N, V1, V4, 1); set_edge(bits, N, V4, V1, 1);
+                set_edge(bits, N, V2, V3, 1); set_edge(bits, N, V3, V2, 1);
+                eb[t->i] = V4; eb[t->j] = V2;
+            }
+            committed++;
+        }
+        for (int64_t it = 0; it < total; it++) {
+            MsItem* t = &items[it];
+            slot_owner[t->i] = slot_owner[t->j] = slot_wr[t->i] = slot_wr[t->j] = UINT64_MAX;
+            table[t->h[0]] = table[t->h[1]] = pair_wr[t->h[0]] = pair_wr[t->h[1]] = UINT64_MAX;
+            pair_wr[pair_entry(t->v[0], t->v[1], N, hmask)] = UINT64_MAX;
+            pair_wr[pair_entry(t->v[2], t->v[3], N, hmask)] = UINT64_MAX;
+        }
+        uint64_t* tmp = pend; pend = pnext; pnext = tmp;
+        np = nn;
+        fresh += take;
+    }
+    free(slot_owner); free(table); free(slot_wr); free(pair_wr); free(items); free(commit); free(pend); free(pnext);
+    maslov_rebuild(R, N, M, ea, eb, ew, R_out, C_out, V_out);
+    free(ea); free(eb); free(ew); free(bits);
+    return committed;
+}
+
+/* The reference's Rewire loop itself (U/cuda_EC/cuda_EC/Maslov.cpp:17-59,
+ * W/Maslov/Maslov/Maslov.cpp:59-101), attempt after attempt on the current
+ * graph, drawing from the 15-bit linear congruential rand() of the Microsoft
+ * C runtime the reference was built with (state = state * 214013 + 2531011,
+ * output bits 16..30) seeded with `seed` where the reference calls
+ * srand(time(0)): slot i = (rand() * 0x8000 + rand()) % M, slot j likewise,
+ * coin = rand() % 2.  Returns the number of committed swaps (the reference's
+ * Shuffle_times).  With the stream of the reference's run this is the
+ * reference's result exactly. */
+int64_t or_rewire_seq(const int32_t* R, const int32_t* C, const float* V, int N, uint32_t seed, int64_t attempts,
+                      int32_t* R_out, int32_t* C_out, float* V_out)
+{
+    int64_t M = R[N] / 2;
+    int32_t* ea = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
+    int32_t* eb = (int32_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(int32_t));
+    float* ew = (float*)malloc((size_t)(M > 0 ? M : 1) * sizeof(float));
+    size_t words = (size_t)(((uint64_t)N * (uint64_t)N + 63) / 64);
+    uint64_t* bits = (uint64_t*)calloc(words > 0 ? words : 1, sizeof(uint64_t));
+    int64_t m = 0;
+    for (int i = 0; i < N; i++)
+        for (int32_t e = R[i]; e < R[i + 1]; e++) {
+            set_edge(bits, N, i, C[e], 1);
+            if (C[e] > i) { ea[m] = i; eb[m] = C[e]; ew[m] = V ? V[e] : 1.0f; m++; }
+        }
+    uint32_t st = seed;
+#define RAND15() (st = st * 214013u + 2531011u, (int)((st >> 16) & 0x7fff))
+    int64_t committed = 0;
+    for (int64_t k = 0; M > 0 && k < attempts; k++) {
+        int hi = RAND15(), lo = RAND15();
+        int64_t i = ((int64_t)hi * 0x8000 + lo) % M;
+        hi = RAND15(); lo = RAND15();
+        int64_t j = ((int64_t)hi * 0x8000 + lo) % M;
+        int V1 = ea[i], V2 = eb[i], V3 = ea[j], V4 = eb[j];
+        if (V1 == V3 || V1 == V4 || V2 == V3 || V2 == V4) continue;
+        if (RAND15() % 2) {
+            if (has_edge(bits, N, V1, V3) || has_edge(bits, N, V2, V4)) continue;
+            set_edge(bits, N, V1, V2, 0); set_edge(bits, N, V2, V1, 0);
+            set_edge(bits, N, V3, V4, 0); set_edge(bits, N, V4, V3, 0);
+            set_edge(bits, N, V1, V3, 1); set_edge(bits, N, V3, V1, 1);
+            set_edge(bits, N, V2, V4, 1); set_edge(bits, N, V4, V2, 1);
+            eb[i] = V3; ea[j] = V2;
+        } else {
+            if (has_edge(bits, N, V1, V4) || has_edge(bits, N, V2, V3)) continue;
+            set_edge(bits, N, V1, V2, 0); set_edge(bits, N, V2, V1, 0);
+            set_edge(bits, N, V3, V4, 0); set_edge(bits, N, V4, V3, 0);
+            set_edge(bits, N, V1, V4, 1); set_edge(bits, N, V4, V1, 1);
+            set_edge(bits, N, V2, V3, 1); set_edge(bits, N, V3, V2, 1);
+            eb[i] = V4; eb[j] = V2;
+        }
+        committed++;
+    }
+#undef RAND15
+    maslov_rebuild(R, N, M, ea, eb, ew, R_out, C_out, V_out);
+    free(ea); free(eb); free(ew); free(bits);
     return committed;
 }
 

@@ -49,6 +49,8 @@ int     or_newman_weighted(const int32_t* R, const int32_t* C, const float* Vw, 
                            int gpu_rule_above, int32_t* labels, double* Q, int* n_modules, int* n_rounds);
 int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uint64_t seed,
                   int64_t attempts, int32_t* R_out, int32_t* C_out, float* V_out);
+int64_t or_rewire_seq(const int32_t* R, const int32_t* C, const float* V, int N, uint32_t seed, int64_t attempts,
+                      int32_t* R_out, int32_t* C_out, float* V_out);
 int     or_eigen_centrality(const int32_t* R, const int32_t* C, const float* V, int N, int raw,
                             double* ec, double* eigenvalue, double* residual);
 double  or_ln(double x);

@@ -85,6 +85,8 @@ def lib():
         L.or_newman.restype = ct.c_int
         L.or_maslov.argtypes = [_i32p, _i32p, _vp, ct.c_int, ct.c_uint64, ct.c_int64, _i32p, _i32p, _vp]
         L.or_maslov.restype = ct.c_int64
+        L.or_rewire_seq.argtypes = [_i32p, _i32p, _vp, ct.c_int, ct.c_uint32, ct.c_int64, _i32p, _i32p, _vp]
+        L.or_rewire_seq.restype = ct.c_int64
         L.or_maslov_round_size.argtypes = [ct.c_int64]
         L.or_maslov_round_size.restype = ct.c_int64
         L.or_eigen_centrality.argtypes = [_i32p, _i32p, _vp, ct.c_int, ct.c_int, _f64p,
@@ -314,6 +316,18 @@ def maslov(R, C, V, seed, attempts):
     return Ro, Co[: len(C)].copy(), (Vo[: len(C)].copy() if V is not None else None), ncommit
 
 
+def rewire_seq(R, C, V, seed, attempts=None):
+    """The reference's sequential Rewire with its 15-bit rand() stream seeded
+    by `seed` (or_rewire_seq); attempts defaults to the reference's 2M."""
+    N = len(R) - 1
+    attempts = len(C) if attempts is None else attempts
+    Ro = np.empty(N + 1, np.int32)
+    Co = np.empty(max(len(C), 1), np.int32)
+    Vo = np.empty(max(len(C), 1), np.float32) if V is not None else None
+    ncommit = lib().or_rewire_seq(R, C, _ptr(V), N, seed, attempts, Ro, Co, _ptr(Vo))
+    return Ro, Co[: len(C)].copy(), (Vo[: len(C)].copy() if V is not None else None), ncommit
+
+
 def maslov_round_size(M):
     return int(lib().or_maslov_round_size(M))
 
@@ -332,6 +346,22 @@ def eigen_centrality(R, C, V=None, raw=False):
 
 
 # ------------------------------------------------------------ compiled reference
+class _QuietFd:
+    """Silences fd 1 around a reference call that prints."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 class Ref:
     """The reference's own CPU functions (oracle/_ref/)."""
 
@@ -369,6 +399,15 @@ class Ref:
         for lib_, pre in ((c, "ref_"), (x, "ref_w")):
             getattr(lib_, pre + "cohort_add").argtypes = [_f32p, _f32p, ct.c_int, ct.c_int]
             getattr(lib_, pre + "cohort_finish").argtypes = [_f32p, ct.c_longlong, ct.c_int, ct.c_int]
+        ms = os.path.join(REF_DIR, "libref_maslov.so")
+        self._maslov = _load(ms) if os.path.exists(ms) else None
+        if self._maslov is not None:
+            self._maslov.ref_maslov.argtypes = [_i32p, _i32p, ct.c_int, ct.c_int, ct.c_uint, _i32p, _i32p]
+        wms = os.path.join(REF_DIR, "libref_wmaslov.so")
+        self._wmaslov = _load(wms) if os.path.exists(wms) else None
+        if self._wmaslov is not None:
+            self._wmaslov.ref_wmaslov.argtypes = [_i32p, _i32p, _f32p, ct.c_int, ct.c_int, ct.c_uint, _i32p, _i32p,
+                                                  _f32p]
         wn = os.path.join(REF_DIR, "libref_wnewman.so")
         self._wnewman = _load(wn) if os.path.exists(wn) else None
         if self._wnewman is not None:
@@ -468,6 +507,22 @@ class Ref:
             getattr(lib_, pre + "cohort_add")(cm, np.ascontiguousarray(r, np.float32), N, int(fisher))
         getattr(lib_, pre + "cohort_finish")(cm, M1, len(r_subjects), int(fisher))
         return cm[:M1]
+
+    def maslov(self, R, C, seed, V=None):
+        """The reference's Maslov (U) or Maslov_weighted_1 (W) with rand()
+        seeded by `seed`: 2M attempts, (R, C[, V]) of the surrogate."""
+        N = len(R) - 1
+        R = np.ascontiguousarray(R, np.int32)
+        C = np.ascontiguousarray(C, np.int32)
+        Ro = np.empty(N + 1, np.int32)
+        Co = np.empty(max(len(C), 1), np.int32)
+        if V is None:
+            self._maslov.ref_maslov(R, C, N, len(C), seed, Ro, Co)
+            return Ro, Co[: len(C)].copy()
+        Vo = np.empty(max(len(C), 1), np.float32)
+        with _QuietFd():
+            self._wmaslov.ref_wmaslov(R, C, np.ascontiguousarray(V, np.float32), N, len(C), seed, Ro, Co, Vo)
+        return Ro, Co[: len(C)].copy(), Vo[: len(C)].copy()
 
     def cp2(self, R, C, V):
         N = len(R) - 1

@@ -230,6 +230,37 @@ void ref_wpartition(int* R, int* C, float* V, int n, int* result)
     Partition(R, C, result);
 }
 }
+#elif defined(REF_GROUP_MASLOV) || defined(REF_GROUP_WMASLOV)
+/* U/cuda_EC/cuda_EC/Maslov.cpp (Maslov, Rewire) or W/Maslov/Maslov/Maslov.cpp
+ * (Maslov_weighted_1), compiled with ref_shim/seeded_rand.h forced in. */
+extern "C" {
+unsigned int ref_rand_seed = 1;
+static unsigned int ref_lcg_state = 1;
+int ref_rand15(void)
+{
+    ref_lcg_state = ref_lcg_state * 214013u + 2531011u;
+    return (int)((ref_lcg_state >> 16) & 0x7fff);
+}
+void ref_srand15(unsigned int seed) { ref_lcg_state = seed; }
+}
+#if defined(REF_GROUP_MASLOV)
+void Maslov(int* R_dst, int* C_dst, int* R_src, int* C_src, int Rlength, int Clength);
+extern "C" void ref_maslov(int* R_src, int* C_src, int N, int nnz, unsigned int seed, int* R_dst, int* C_dst)
+{
+    ref_rand_seed = seed;
+    Maslov(R_dst, C_dst, R_src, C_src, N + 1, nnz);
+}
+#else
+void Maslov_weighted_1(int* R_dst, int* C_dst, float* V_dst, int* R_src, int* C_src, float* V_src, int Rlength,
+                       int Clength);
+extern "C" void ref_wmaslov(int* R_src, int* C_src, float* V_src, int N, int nnz, unsigned int seed, int* R_dst,
+                            int* C_dst, float* V_dst)
+{
+    ref_rand_seed = seed;
+    Maslov_weighted_1(R_dst, C_dst, V_dst, R_src, C_src, V_src, N + 1, nnz);
+}
+#endif
+
 #else
 #error "select a reference group with -DREF_GROUP_<NAME>"
 #endif

@@ -347,11 +347,28 @@ __global__ void k_noalloc_clear(unsigned long long* __restrict__ w, int64_t coun
 // Largest n whose neighbour bitmap (n bits) fits the opt-in shared memory.
 int64_t noalloc_smem_nodes(int smem_optin) { return (int64_t)(smem_optin - NOALLOC_SMEM_SLACK) / 4 * 32; }
 
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points
+// (the library does not link the driver library directly).
 bool current_ctx_id(unsigned long long* id)
 {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *p = nullptr, *q = nullptr;
+        cudaDriverEntryPointQueryResult r1, r2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r1) != cudaSuccess ||
+            r1 != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &q, cudaEnableDefault, &r2) != cudaSuccess ||
+            r2 != cudaDriverEntryPointSuccess)
+            return false;
+        get_current = (GetCurrent)p;
+        get_id = (GetId)q;
+    }
     CUcontext c = nullptr;
-    if (cuCtxGetCurrent(&c) != CUDA_SUCCESS || !c) return false;
-    return cuCtxGetId(c, id) == CUDA_SUCCESS;
+    if (get_current(&c) != CUDA_SUCCESS || !c) return false;
+    return get_id(c, id) == CUDA_SUCCESS;
 }
 
 pg_status noalloc_setup(int dev, NoallocDevice** out)

@@ -2,21 +2,52 @@
 // U/cuda_EC/cuda_EC/Maslov.cpp:8-109; Maslov_weighted_1,
 // W/Maslov/Maslov/Maslov.cpp:50-196).
 //
-// The reference runs 2M sequential attempts drawn from rand().  Here the
-// attempts come from a seeded counter-based generator and run in rounds of
-// B attempts: every attempt of a round reads the state left by the previous
-// round (two random edge slots, the swap orientation coin, the shared
-// end-point test and the "new edge already exists" test against an N x N
-// edge bitmap), valid attempts claim their four end points with atomicMin of
-// the attempt index, and only attempts that own all four commit.  Committed
-// attempts of one round touch disjoint vertices (hence disjoint slots and
-// bitmap bits), so the round's result does not depend on thread timing and
-// equals the sequential restatement in the oracle bit for bit.
-// Weights stay with the edge slot that carries them, as in Maslov_weighted_1.
+// The reference evaluates its swap attempts one after another, each on the
+// graph the previous ones left: two random edge slots i, j (edges 1-2 and
+// 3-4), a coin for the new pairing (1-3 + 2-4, or 1-4 + 3-2), rejection when
+// the edges share an end point or a new edge already exists, otherwise the
+// swap is applied to the slots and to the adjacency matrix.
+//
+// Here the attempts come from a seeded counter-based generator (attempt a
+// uses bits 2a and 2a + 1 of a splitmix64 stream keyed by the seed) and are
+// evaluated in rounds, all attempts of a round on the state the previous
+// round left:
+//   - a valid attempt claims its two slots and its two new pairs, lowest
+//     attempt index first (atomicMin of the index relative to the round's
+//     oldest attempt; slots in an owner array, pairs in a direct-mapped table
+//     where a collision of two pairs only costs a deferral); attempts that
+//     own all four claims commit;
+//   - every attempt whose evaluation read something (a slot, or the bit of a
+//     pair it needed absent) that a lower-index commit of the round writes,
+//     and every valid attempt that lost a claim, is deferred to the next
+//     round and evaluated again there; the other rejected attempts are
+//     decided.
+// Each decided attempt thus saw exactly the state the lower-index commits of
+// its round leave (commits touch disjoint slots and create distinct pairs,
+// and a valid attempt's new pairs are absent from the round's state), so a
+// round is the reference's sequential chain over its decided attempts in
+// index order, and every requested attempt is decided once.  Measured
+// against the reference's own Maslov (compiled from its sources, 100 seeds),
+// the committed fraction and the surrogates' clustering agree in
+// distribution (tests/test_maslov_reference_cpu.py).  The decisions depend
+// only on the state and the indices, not on thread timing, and equal the
+// oracle's sequential restatement (or_maslov) bit for bit.
+//
+// All rounds run in one cooperative launch with grid-wide barriers between
+// the evaluate / commit / release phases; the round counters live in a
+// device control block, so the launch needs no host round trip and can be
+// captured in a CUDA graph.  Weights stay with their edge slot, as in
+// Maslov_weighted_1.
 #include "pg_internal.cuh"
+#include "maslov.cuh"
 #include <algorithm>
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 namespace {
+constexpr int MS_THREADS = 256;
+
 __device__ __host__ __forceinline__ uint64_t mix64(uint64_t z)
 {
     z += 0x9E3779B97F4A7C15ULL;
@@ -35,6 +66,13 @@ __device__ __forceinline__ void put_edge(unsigned long long* bits, uint64_t n, i
     uint64_t q = (uint64_t)a * n + (uint64_t)b;
     unsigned long long m = 1ULL << (q & 63);
     if (on) atomicOr(&bits[q >> 6], m); else atomicAnd(&bits[q >> 6], ~m);
+}
+
+// table entry of the unordered pair {a, b}
+__device__ __host__ __forceinline__ uint32_t pair_slot(int a, int b, uint64_t n, uint32_t hmask)
+{
+    uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+    return (uint32_t)(mix64(lo * n + hi) & hmask);
 }
 
 // Upper-triangle edge slots from the CSR (row-major order, as the
@@ -81,73 +119,162 @@ __global__ void k_ms_upper_count(const int32_t* __restrict__ R, const int32_t* _
     }
 }
 
-struct Attempt {
+__global__ void k_ms_reset(MsControl* __restrict__ st, uint64_t attempts, uint32_t* __restrict__ slot_owner,
+                           uint32_t* __restrict__ slot_wr, long long M, uint32_t* __restrict__ table,
+                           uint32_t* __restrict__ pair_wr, uint32_t hsize)
+{
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    for (long long q = tid; q < M; q += nt) slot_owner[q] = slot_wr[q] = 0xffffffffu;
+    for (long long q = tid; q < hsize; q += nt) table[q] = pair_wr[q] = 0xffffffffu;
+    if (tid == 0) {
+        st->fresh_next = 0;
+        st->attempts = attempts;
+        st->n_pending = 0;
+        st->n_next = 0;
+        st->oldest = 0;
+        st->next_oldest = ~0ULL;
+        st->committed = 0;
+        st->rounds = 0;
+    }
+}
+
+struct MsItem {
+    unsigned long long a;   // attempt index
     int v[4];
-    long long i, j;
-    int ok, coin;
+    int i, j;               // slots
+    uint32_t h[2];          // table entries of the new pairs
+    int state;              // 0 shared end point, 1 new edge exists, 2 valid, 3 committing
+    int coin;
 };
 
-__global__ void k_ms_propose(const int* __restrict__ ea, const int* __restrict__ eb, long long M, int32_t n,
-                             const unsigned long long* __restrict__ bits, uint64_t seed, long long base, int nb,
-                             Attempt* __restrict__ at, unsigned int* __restrict__ owner)
+__device__ __forceinline__ uint64_t stream_key(uint64_t seed) { return mix64(seed ^ 0xD1B54A32D192ED03ULL); }
+__device__ __forceinline__ uint64_t stream_bits(uint64_t key, uint64_t q)
 {
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nb; a += gridDim.x * blockDim.x) {
-        uint64_t idx = (uint64_t)(base + a);
-        uint64_t h1 = mix64(seed ^ (2 * idx)), h2 = mix64(seed ^ (2 * idx + 1));
-        long long i = (long long)(h1 % (uint64_t)M), j = (long long)(h2 % (uint64_t)M);
-        int c = (int)((h1 >> 63) ^ (h2 >> 63));
-        int V1 = ea[i], V2 = eb[i], V3 = ea[j], V4 = eb[j];
-        bool ok = !(V1 == V3 || V1 == V4 || V2 == V3 || V2 == V4);
-        if (ok) {
-            if (c) ok = !(has_edge(bits, n, V1, V3) || has_edge(bits, n, V2, V4));
-            else ok = !(has_edge(bits, n, V1, V4) || has_edge(bits, n, V2, V3));
-        }
-        Attempt t;
-        t.v[0] = V1; t.v[1] = V2; t.v[2] = V3; t.v[3] = V4;
-        t.i = i; t.j = j; t.ok = ok; t.coin = c;
-        at[a] = t;
-        if (ok)
-            for (int q = 0; q < 4; q++) atomicMin(&owner[t.v[q]], (unsigned)a);
-    }
+    return mix64(key + q * 0x9E3779B97F4A7C15ULL);
 }
 
-__global__ void k_ms_commit(const Attempt* __restrict__ at, int nb, int32_t n, const unsigned int* __restrict__ owner,
-                            int* __restrict__ ea, int* __restrict__ eb, unsigned long long* __restrict__ bits,
-                            unsigned long long* __restrict__ committed)
+__global__ void __launch_bounds__(MS_THREADS)
+k_ms_rounds(MsArgs p)
 {
-    unsigned long long mine = 0;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nb; a += gridDim.x * blockDim.x) {
-        Attempt t = at[a];
-        if (!t.ok) continue;
-        bool own = true;
-        for (int q = 0; q < 4; q++) own &= owner[t.v[q]] == (unsigned)a;
-        if (!own) continue;
-        int V1 = t.v[0], V2 = t.v[1], V3 = t.v[2], V4 = t.v[3];
-        put_edge(bits, n, V1, V2, false); put_edge(bits, n, V2, V1, false);
-        put_edge(bits, n, V3, V4, false); put_edge(bits, n, V4, V3, false);
-        if (t.coin) {  // 1-3, 2-4 (Maslov.cpp:31-42)
-            put_edge(bits, n, V1, V3, true); put_edge(bits, n, V3, V1, true);
-            put_edge(bits, n, V2, V4, true); put_edge(bits, n, V4, V2, true);
-            eb[t.i] = V3;
-            ea[t.j] = V2;
-        } else {       // 1-4, 3-2 (Maslov.cpp:44-55)
-            put_edge(bits, n, V1, V4, true); put_edge(bits, n, V4, V1, true);
-            put_edge(bits, n, V2, V3, true); put_edge(bits, n, V3, V2, true);
-            eb[t.i] = V4;
-            eb[t.j] = V2;
+    cg::grid_group grid = cg::this_grid();
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    const uint64_t n = (uint64_t)p.n;
+    const uint64_t key = stream_key(p.seed);
+    unsigned long long* pend = p.pend_a;
+    unsigned long long* pnext = p.pend_b;
+    MsItem* items = (MsItem*)p.items;
+    for (;;) {
+        const volatile MsControl* vst = p.st;
+        const unsigned long long np = vst->n_pending;
+        const unsigned long long fresh = vst->fresh_next;
+        const unsigned long long left = vst->attempts - fresh;
+        const unsigned long long take = min(left, (unsigned long long)p.B - np);
+        const unsigned long long total = np + take;
+        if (total == 0) break;                                   // uniform over the grid
+        const unsigned long long base = np ? vst->oldest : fresh;    // oldest attempt of the round
+        // ---- evaluate on the round's state; valid attempts claim
+        for (long long it = tid; it < (long long)total; it += nt) {
+            MsItem t;
+            t.a = it < (long long)np ? pend[it] : fresh + (it - np);
+            const uint64_t h1 = stream_bits(key, 2 * t.a), h2 = stream_bits(key, 2 * t.a + 1);
+            t.i = (int)(h1 % (uint64_t)p.M);
+            t.j = (int)(h2 % (uint64_t)p.M);
+            t.coin = (int)((h1 >> 63) ^ (h2 >> 63));
+            t.v[0] = p.ea[t.i]; t.v[1] = p.eb[t.i]; t.v[2] = p.ea[t.j]; t.v[3] = p.eb[t.j];
+            const int x1 = t.v[0], x2 = t.coin ? t.v[2] : t.v[3];   // new pair 1: 1-3 or 1-4
+            const int y1 = t.v[1], y2 = t.coin ? t.v[3] : t.v[2];   // new pair 2: 2-4 or 2-3
+            t.h[0] = pair_slot(x1, x2, n, p.hmask);
+            t.h[1] = pair_slot(y1, y2, n, p.hmask);
+            if (t.v[0] == t.v[2] || t.v[0] == t.v[3] || t.v[1] == t.v[2] || t.v[1] == t.v[3]) t.state = 0;
+            else if (has_edge(p.bits, n, x1, x2) || has_edge(p.bits, n, y1, y2)) t.state = 1;
+            else t.state = 2;
+            if (t.state == 2) {
+                const uint32_t pr = (uint32_t)(t.a - base);
+                atomicMin(&p.slot_owner[t.i], pr);
+                atomicMin(&p.slot_owner[t.j], pr);
+                atomicMin(&p.table[t.h[0]], pr);
+                atomicMin(&p.table[t.h[1]], pr);
+            }
+            items[it] = t;
         }
-        mine++;
-    }
-    mine = __reduce_add_sync(0xffffffffu, (unsigned)mine);
-    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(committed, mine);
-}
-
-__global__ void k_ms_release(const Attempt* __restrict__ at, int nb, unsigned int* __restrict__ owner)
-{
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nb; a += gridDim.x * blockDim.x) {
-        Attempt t = at[a];
-        if (t.ok)
-            for (int q = 0; q < 4; q++) owner[t.v[q]] = 0xffffffffu;
+        grid.sync();
+        // ---- valid attempts owning all four claims commit: record their writes
+        for (long long it = tid; it < (long long)total; it += nt) {
+            MsItem& t = items[it];
+            if (t.state != 2) continue;
+            const uint32_t pr = (uint32_t)(t.a - base);
+            if (!(p.slot_owner[t.i] == pr && p.slot_owner[t.j] == pr && p.table[t.h[0]] == pr &&
+                  p.table[t.h[1]] == pr))
+                continue;
+            t.state = 3;
+            p.slot_wr[t.i] = pr;          // committed slots are disjoint
+            p.slot_wr[t.j] = pr;
+            atomicMin(&p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)], pr);
+            atomicMin(&p.pair_wr[pair_slot(t.v[2], t.v[3], n, p.hmask)], pr);
+            atomicMin(&p.pair_wr[t.h[0]], pr);
+            atomicMin(&p.pair_wr[t.h[1]], pr);
+        }
+        grid.sync();
+        // ---- apply the commits; defer valid attempts that lost and rejected
+        // attempts whose reads a lower-index commit wrote
+        unsigned long long mine = 0;
+        for (long long it = tid; it < (long long)total; it += nt) {
+            const MsItem t = items[it];
+            const uint32_t pr = (uint32_t)(t.a - base);
+            bool defer = t.state == 2;
+            if (t.state < 2) {
+                defer = p.slot_wr[t.i] < pr || p.slot_wr[t.j] < pr;
+                if (t.state == 1) defer |= p.pair_wr[t.h[0]] < pr || p.pair_wr[t.h[1]] < pr;
+            }
+            if (defer) {
+                pnext[atomicAdd(&p.st->n_next, 1ULL)] = t.a;
+                atomicMin(&p.st->next_oldest, t.a);
+                continue;
+            }
+            if (t.state != 3) continue;
+            const int V1 = t.v[0], V2 = t.v[1], V3 = t.v[2], V4 = t.v[3];
+            put_edge(p.bits, n, V1, V2, false); put_edge(p.bits, n, V2, V1, false);
+            put_edge(p.bits, n, V3, V4, false); put_edge(p.bits, n, V4, V3, false);
+            if (t.coin) {   // 1-3, 2-4 (Maslov.cpp:36-44)
+                put_edge(p.bits, n, V1, V3, true); put_edge(p.bits, n, V3, V1, true);
+                put_edge(p.bits, n, V2, V4, true); put_edge(p.bits, n, V4, V2, true);
+                p.eb[t.i] = V3;
+                p.ea[t.j] = V2;
+            } else {        // 1-4, 3-2 (Maslov.cpp:47-56)
+                put_edge(p.bits, n, V1, V4, true); put_edge(p.bits, n, V4, V1, true);
+                put_edge(p.bits, n, V2, V3, true); put_edge(p.bits, n, V3, V2, true);
+                p.eb[t.i] = V4;
+                p.eb[t.j] = V2;
+            }
+            mine++;
+        }
+        mine = __reduce_add_sync(0xffffffffu, (unsigned)mine);
+        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&p.st->committed, mine);
+        grid.sync();
+        // ---- release the claims and write records; advance the round counters
+        for (long long it = tid; it < (long long)total; it += nt) {
+            const MsItem t = items[it];
+            p.slot_owner[t.i] = p.slot_owner[t.j] = 0xffffffffu;
+            p.slot_wr[t.i] = p.slot_wr[t.j] = 0xffffffffu;
+            p.table[t.h[0]] = p.table[t.h[1]] = 0xffffffffu;
+            p.pair_wr[t.h[0]] = p.pair_wr[t.h[1]] = 0xffffffffu;
+            p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)] = 0xffffffffu;
+            p.pair_wr[pair_slot(t.v[2], t.v[3], n, p.hmask)] = 0xffffffffu;
+        }
+        if (tid == 0) {
+            p.st->n_pending = p.st->n_next;
+            p.st->oldest = p.st->next_oldest;
+            p.st->n_next = 0;
+            p.st->next_oldest = ~0ULL;
+            p.st->fresh_next = fresh + take;
+            p.st->rounds++;
+        }
+        grid.sync();
+        unsigned long long* tmp = pend;
+        pend = pnext;
+        pnext = tmp;
     }
 }
 
@@ -158,70 +285,107 @@ __global__ void k_ms_pairs(const int* __restrict__ ea, const int* __restrict__ e
 }
 }  // namespace
 
-extern "C" int64_t pg_maslov_round_size(int64_t M)
+int64_t ms_round_size(int64_t M)
 {
-    int64_t b = M / 16;
-    if (b < 1) b = 1;
-    if (b > 65536) b = 65536;
+    int64_t b = M / 32;
+    if (b < 64) b = 64;
+    if (b > (1LL << 20)) b = 1LL << 20;
     return b;
 }
+
+uint32_t ms_table_size(int64_t B)
+{
+    uint32_t h = 1024;
+    while ((int64_t)h < 64 * B) h <<= 1;
+    return h;
+}
+
+pg_status ms_prepare(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t attempts, MsArgs* a)
+{
+    const int n = g->n;
+    const long long M = g->nnz / 2;
+    const long long B = ms_round_size(M);
+    const uint32_t H = ms_table_size(B);
+    const uint64_t nbits = (uint64_t)n * (uint64_t)n;
+    const size_t words = (size_t)((nbits + 63) / 64);
+    memset(a, 0, sizeof *a);
+    a->n = n;
+    a->M = M;
+    a->B = B;
+    a->hmask = H - 1;
+    a->seed = seed;
+    PG_TRY(pg_wst(ctx, "ms.cnt", (size_t)n + 1, &a->cnt));
+    PG_TRY(pg_wst(ctx, "ms.off", (size_t)n + 2, &a->off));
+    PG_TRY(pg_wst(ctx, "ms.ea", (size_t)M + 1, &a->ea));
+    PG_TRY(pg_wst(ctx, "ms.eb", (size_t)M + 1, &a->eb));
+    PG_TRY(pg_wst(ctx, "ms.ew", (size_t)M + 1, &a->ew));
+    PG_TRY(pg_wst(ctx, "ms.bits", words + 1, &a->bits));
+    PG_TRY(pg_wst(ctx, "ms.slot_owner", (size_t)M + 1, &a->slot_owner));
+    PG_TRY(pg_wst(ctx, "ms.table", (size_t)H, &a->table));
+    PG_TRY(pg_wst(ctx, "ms.slot_wr", (size_t)M + 1, &a->slot_wr));
+    PG_TRY(pg_wst(ctx, "ms.pair_wr", (size_t)H, &a->pair_wr));
+    PG_TRY(pg_wst(ctx, "ms.items", (size_t)B, (MsItem**)&a->items));
+    PG_TRY(pg_wst(ctx, "ms.pend_a", (size_t)B, &a->pend_a));
+    PG_TRY(pg_wst(ctx, "ms.pend_b", (size_t)B, &a->pend_b));
+    PG_TRY(pg_wst(ctx, "ms.ctl", 1, &a->st));
+    PG_TRY(pg_wst(ctx, "ms.pairs", (size_t)M + 1, &a->pairs));
+    a->words = words;
+    a->attempts = (uint64_t)attempts;
+    int per_sm = 0;
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ms_rounds, MS_THREADS, 0));
+    if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "maslov: kernel does not fit an SM");
+    a->grid = ctx->sm_count * std::min(per_sm, 4);
+    return PG_OK;
+}
+
+// Enqueues the whole rewiring on the context stream: no host round trip, no
+// allocation (ms_prepare sized the workspace).
+pg_status ms_enqueue(pg_ctx* ctx, const pg_graph* g, MsArgs* a)
+{
+    const int grid = ctx->sm_count * 4;
+    PG_CUDA(ctx, cudaMemsetAsync(a->bits, 0, sizeof(unsigned long long) * a->words, ctx->stream));
+    k_ms_reset<<<grid, 256, 0, ctx->stream>>>(a->st, a->attempts, a->slot_owner, a->slot_wr, a->M, a->table,
+                                               a->pair_wr, a->hmask + 1);
+    PG_LAUNCHED(ctx);
+    k_ms_upper_count<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, a->n, a->cnt);
+    PG_LAUNCHED(ctx);
+    PG_TRY(pg_scan_counts(ctx, a->cnt, (int64_t*)a->off, a->n));
+    k_ms_init<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, g->V, a->n, a->off, a->ea, a->eb, a->ew, a->bits);
+    PG_LAUNCHED(ctx);
+    if (a->M >= 2 && a->attempts > 0) {
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeCooperative;
+        attr.val.cooperative = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(a->grid);
+        cfg.blockDim = dim3(MS_THREADS);
+        cfg.stream = ctx->stream;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_ms_rounds, *a));
+        PG_LAUNCHED(ctx);
+    }
+    k_ms_pairs<<<grid, 256, 0, ctx->stream>>>(a->ea, a->eb, a->M, a->pairs);
+    PG_LAUNCHED(ctx);
+    return PG_OK;
+}
+
+extern "C" int64_t pg_maslov_round_size(int64_t M) { return ms_round_size(M); }
 
 extern "C" pg_status pg_maslov(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t attempts, pg_graph** out,
                                int64_t* committed)
 {
     if (!ctx || !g || !out || attempts < 0) return pg_fail(ctx, PG_ERR_INVALID, "pg_maslov: bad arguments");
+    if (g->nnz / 2 > INT32_MAX) return pg_fail(ctx, PG_ERR_TOO_LARGE, "pg_maslov: too many edges");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    const int n = g->n;
-    const long long M = g->nnz / 2;
-    int32_t* cnt;
-    long long* off;
-    int *ea, *eb;
-    float* ew;
-    unsigned long long *bits, *ncommit;
-    unsigned int* owner;
-    Attempt* at;
-    const uint64_t nbits = (uint64_t)n * (uint64_t)n;
-    const size_t words = (size_t)((nbits + 63) / 64);
-    const long long B = pg_maslov_round_size(M);
-    PG_TRY(pg_wst(ctx, "ms.cnt", (size_t)n + 1, &cnt));
-    PG_TRY(pg_wst(ctx, "ms.off", (size_t)n + 2, &off));
-    PG_TRY(pg_wst(ctx, "ms.ea", (size_t)M + 1, &ea));
-    PG_TRY(pg_wst(ctx, "ms.eb", (size_t)M + 1, &eb));
-    PG_TRY(pg_wst(ctx, "ms.ew", (size_t)M + 1, &ew));
-    PG_TRY(pg_wst(ctx, "ms.bits", words + 1, &bits));
-    PG_TRY(pg_wst(ctx, "ms.owner", (size_t)n + 1, &owner));
-    PG_TRY(pg_wst(ctx, "ms.at", (size_t)B, &at));
-    PG_TRY(pg_wst(ctx, "ms.ncommit", 1, &ncommit));
-    PG_CUDA(ctx, cudaMemsetAsync(bits, 0, sizeof(unsigned long long) * words, ctx->stream));
-    PG_CUDA(ctx, cudaMemsetAsync(owner, 0xff, sizeof(unsigned int) * (n + 1), ctx->stream));
-    PG_CUDA(ctx, cudaMemsetAsync(ncommit, 0, sizeof(unsigned long long), ctx->stream));
-    const int grid = ctx->sm_count * 4;
-    k_ms_upper_count<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, n, cnt);
-    PG_LAUNCHED(ctx);
-    PG_TRY(pg_scan_counts(ctx, cnt, (int64_t*)off, n));
-    k_ms_init<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, g->V, n, off, ea, eb, ew, bits);
-    PG_LAUNCHED(ctx);
-    if (M >= 2) {
-        for (long long base = 0; base < attempts; base += B) {
-            int nb = (int)std::min<long long>(B, attempts - base);
-            int gr = std::max(1, std::min(grid, ceil_div(nb, 256)));
-            k_ms_propose<<<gr, 256, 0, ctx->stream>>>(ea, eb, M, n, bits, seed, base, nb, at, owner);
-            PG_LAUNCHED(ctx);
-            k_ms_commit<<<gr, 256, 0, ctx->stream>>>(at, nb, n, owner, ea, eb, bits, ncommit);
-            PG_LAUNCHED(ctx);
-            k_ms_release<<<gr, 256, 0, ctx->stream>>>(at, nb, owner);
-            PG_LAUNCHED(ctx);
-        }
-    }
-    int2* pairs;
-    PG_TRY(pg_wst(ctx, "ms.pairs", (size_t)M + 1, &pairs));
-    k_ms_pairs<<<grid, 256, 0, ctx->stream>>>(ea, eb, M, pairs);
-    PG_LAUNCHED(ctx);
-    PG_TRY(pg_csr_from_pairs(ctx, n, pairs, g->V ? ew : nullptr, M, out));
+    MsArgs a;
+    PG_TRY(ms_prepare(ctx, g, seed, attempts, &a));
+    PG_TRY(ms_enqueue(ctx, g, &a));
+    PG_TRY(pg_csr_from_pairs(ctx, g->n, a.pairs, g->V ? a.ew : nullptr, a.M, out));
     if (committed) {
-        unsigned long long c;
-        PG_TRY(pg_d2h(ctx, &c, ncommit, sizeof c));
-        *committed = (int64_t)c;
+        MsControl c;
+        PG_TRY(pg_d2h(ctx, &c, a.st, sizeof c));
+        *committed = (int64_t)c.committed;
     }
     return PG_OK;
 }

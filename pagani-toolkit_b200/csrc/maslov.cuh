@@ -1,0 +1,50 @@
+// maslov.cuh -- the Maslov rewiring pieces that the surrogate pipeline
+// (runner.cu) enqueues without host round trips.
+#pragma once
+#include "pg_internal.cuh"
+
+// Round counters of one rewiring, in device memory.
+struct MsControl {
+    unsigned long long fresh_next;   // next attempt index never evaluated
+    unsigned long long attempts;     // attempts to evaluate in total
+    unsigned long long n_pending;    // deferred attempts carried into this round
+    unsigned long long n_next;       // deferred attempts of this round
+    unsigned long long oldest;       // smallest index among the pending ones
+    unsigned long long next_oldest;
+    unsigned long long committed;
+    unsigned long long rounds;
+};
+
+struct MsArgs {
+    int n;
+    long long M;                     // undirected edges (slots)
+    long long B;                     // attempts per round
+    uint32_t hmask;                  // pair table size - 1
+    uint64_t seed;
+    uint64_t attempts;
+    size_t words;                    // edge bitmap words
+    int grid;                        // cooperative grid of k_ms_rounds
+    int32_t* cnt;
+    long long* off;
+    int *ea, *eb;                    // slot end points
+    float* ew;                       // slot weights
+    unsigned long long* bits;        // n x n edge bitmap
+    uint32_t* slot_owner;            // per slot: lowest claiming attempt (relative)
+    uint32_t* table;                 // per pair entry: lowest claiming attempt (relative)
+    uint32_t* slot_wr;               // per slot: the committed attempt writing it
+    uint32_t* pair_wr;               // per pair entry: lowest committed attempt writing it
+    void* items;                     // per round item: the evaluated attempt
+    unsigned long long *pend_a, *pend_b;
+    MsControl* st;
+    int2* pairs;                     // result: the M slots as pairs
+};
+
+// Round size and pair-table size for M slots (fixed functions of M, so the
+// surrogate of a seed does not depend on anything else).
+int64_t ms_round_size(int64_t M);
+uint32_t ms_table_size(int64_t B);
+// Sizes the workspace (may allocate) and fills the arguments.
+pg_status ms_prepare(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t attempts, MsArgs* a);
+// Enqueues the rewiring of g on the context stream: result slots in a->pairs
+// (and a->ew); no allocation, no host synchronisation.
+pg_status ms_enqueue(pg_ctx* ctx, const pg_graph* g, MsArgs* a);
