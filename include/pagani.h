@@ -294,11 +294,19 @@ pg_status pg_smallworld(double cp, const double* cp_rand, int32_t n_cp, double l
  * W/SmallWorldProperty/SmallWorldProperty.cpp:14); here each subject's graph stays on the device
  * while every requested metric runs.  Subjects may differ in N and T.
  * Output arrays are host buffers of N entries; NULL skips the metric.  With
- * bc set, eff and lp come from the Brandes sweep, else from pg_paths; cp uses
- * Onnela's formula when build.weighted is set.  n_random > 0 adds that many
- * Maslov surrogates per subject (swaps_per_edge x edges attempts, seed
- * pg_surrogate_seed(seed, subject, r)) and their clustering and hop path
- * length for gamma, lambda and sigma. */
+ * bc set, eff and lp come from the Brandes sweep, else from pg_paths.
+ * n_random > 0 adds that many Maslov surrogates per subject (swaps_per_edge x
+ * edges attempts, seed pg_surrogate_seed(seed, subject, r)) and their
+ * clustering and hop path length for gamma, lambda and sigma; the surrogate
+ * chain is captured into a CUDA graph once per subject and replayed
+ * (cuda_graphs = 0 enqueues it directly; the results are the same).
+ * With build.weighted set the weighted tools' rules apply where the
+ * reference has them: degree is strength (W Degree.cpp), clustering is
+ * Onnela's (real graph and surrogates, W Cp_2.cpp) and modules come from
+ * pg_newman_weighted (W Newman_Modularity_GPU); path length, efficiency and
+ * betweenness stay hop-based (BFS_MulCPU / CUBC semantics: the weighted
+ * tree's path-length tool, CUBFW_Lp, is pg_fw_paths, an N^3 computation
+ * called separately). */
 typedef struct {
     const float* bold;       /* T x N float32 (device pointer with build.input_on_device) */
     int32_t N, T;
@@ -311,6 +319,7 @@ typedef struct {
     double tau, cp_mean, lp, Q;
     int32_t n_modules;
     double gamma, lambda, sigma;
+    int32_t surrogate_graph_replays;   /* surrogates run as CUDA graph replays */
 } pg_subject;
 
 typedef struct {
@@ -318,10 +327,11 @@ typedef struct {
     int32_t n_random;
     int64_t swaps_per_edge;
     uint64_t seed;
+    int32_t cuda_graphs;     /* replay the surrogate chain from a CUDA graph (default 1) */
 } pg_run_opts;
 
 /* Defaults: pg_build_opts_default, no surrogates, 2 swap attempts per edge
- * (U/cuda_EC/cuda_EC/Maslov.cpp:19 tries 2M), seed 1. */
+ * (U/cuda_EC/cuda_EC/Maslov.cpp:19 tries 2M), seed 1, CUDA graphs on. */
 void      pg_run_opts_default(pg_run_opts* o);
 uint64_t  pg_surrogate_seed(uint64_t base, int32_t subject, int32_t r);
 pg_status pg_run_subjects(pg_ctx* ctx, pg_subject* subjects, int32_t n, const pg_run_opts* opts);

@@ -520,15 +520,20 @@ __global__ void k_row_bitmap_sort(const int32_t* __restrict__ R, int32_t n, cons
     }
 }
 
-static pg_status launch_row_sort(pg_ctx* ctx, const int32_t* R, int32_t n, const int32_t* Cin,
-                                 const float* Vin, int32_t* Cout, float* Vout)
+pg_status launch_row_sort(pg_ctx* ctx, const int32_t* R, int32_t n, const int32_t* Cin,
+                          const float* Vin, int32_t* Cout, float* Vout)
 {
+    // largest dynamic shared memory granted to the kernel so far, per device
+    // (set once outside any stream capture, then only launches)
+    static size_t granted[64];
     size_t smem = (size_t)((n + 31) / 32) * 4;
     if (smem > ctx->smem_optin - 8192)
         return pg_fail(ctx, PG_ERR_TOO_LARGE, "row sort: n=%d exceeds the shared-memory bitmap", n);
-    if (smem > 48 * 1024)
+    if (smem > 48 * 1024 && (ctx->device >= 64 || smem > granted[ctx->device])) {
         PG_CUDA(ctx, cudaFuncSetAttribute(k_row_bitmap_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
+        if (ctx->device < 64) granted[ctx->device] = smem;
+    }
     int grid = ctx->sm_count * 4;
     if (grid > n) grid = n > 0 ? n : 1;
     k_row_bitmap_sort<<<grid, 256, smem, ctx->stream>>>(R, n, Cin, Vin, Cout, Vout);

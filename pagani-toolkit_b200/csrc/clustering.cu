@@ -10,6 +10,7 @@
 // which halves the work (each triangle is then counted twice at each of its
 // three nodes).
 #include "pg_internal.cuh"
+#include "clustering.cuh"
 #include <cuda.h>
 #include <algorithm>
 #include <cmath>
@@ -227,9 +228,11 @@ __global__ void k_mean_segments(const float* __restrict__ x, const int* __restri
 }
 }  // namespace
 
-// Onnela for a table of graphs already on the device (used by pg_fw_batched too).
-pg_status pg_onnela_table(pg_ctx* ctx, const pg_graph* const* graphs, int ng, int first_n, float* cp_dev,
-                          double* mean_dev)
+// Onnela for a table of graphs already on the device (used by pg_fw_batched
+// too): the table is uploaded (and the stream synchronised) here, the
+// kernels are enqueued by onnela_enqueue.
+pg_status onnela_prepare(pg_ctx* ctx, const pg_graph* const* graphs, int ng, int first_n, float* cp_dev,
+                         double* mean_dev, OnnelaArgs* a)
 {
     std::vector<GraphRef> tab(ng);
     std::vector<int> node0(ng);
@@ -242,27 +245,75 @@ pg_status pg_onnela_table(pg_ctx* ctx, const pg_graph* const* graphs, int ng, in
         nmax = std::max(nmax, (int)graphs[i]->n);
     }
     GraphRef* dtab;
-    int *dnode0, *counter;
-    float* vmax;
     PG_TRY(pg_wst(ctx, "on.tab", (size_t)ng, &dtab));
-    PG_TRY(pg_wst(ctx, "on.node0", (size_t)ng, &dnode0));
-    PG_TRY(pg_wst(ctx, "on.ctr", 1, &counter));
-    PG_TRY(pg_wst(ctx, "on.vmax", (size_t)ng, &vmax));
+    PG_TRY(pg_wst(ctx, "on.node0", (size_t)ng, &a->node0));
+    PG_TRY(pg_wst(ctx, "on.ctr", 1, &a->counter));
+    PG_TRY(pg_wst(ctx, "on.vmax", (size_t)ng, &a->vmax));
     PG_CUDA(ctx, cudaMemcpyAsync(dtab, tab.data(), sizeof(GraphRef) * ng, cudaMemcpyHostToDevice, ctx->stream));
-    PG_CUDA(ctx, cudaMemcpyAsync(dnode0, node0.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, ctx->stream));
-    PG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
-    k_vmax<<<std::min(ng, 4096), 256, 0, ctx->stream>>>(dtab, ng, first_n, vmax);
-    PG_LAUNCHED(ctx);
-    size_t smem = (size_t)((nmax + 31) / 32) * 4;
-    if (smem > ctx->smem_optin - 4096) return pg_fail(ctx, PG_ERR_TOO_LARGE, "Onnela: n=%d too large", nmax);
-    if (smem > 48 * 1024)
-        PG_CUDA(ctx, cudaFuncSetAttribute(k_onnela, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_onnela<<<ctx->sm_count * 4, THREADS, smem, ctx->stream>>>(dtab, dnode0, ng, total, vmax, cp_dev, counter);
-    PG_LAUNCHED(ctx);
-    k_mean_segments<<<std::min(ng, 4096), 32, 0, ctx->stream>>>(cp_dev, dnode0, ng, total, mean_dev);
-    PG_LAUNCHED(ctx);
+    PG_CUDA(ctx, cudaMemcpyAsync(a->node0, node0.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, ctx->stream));
+    a->smem = (size_t)((nmax + 31) / 32) * 4;
+    if (a->smem > ctx->smem_optin - 4096) return pg_fail(ctx, PG_ERR_TOO_LARGE, "Onnela: n=%d too large", nmax);
+    if (a->smem > 48 * 1024)
+        PG_CUDA(ctx, cudaFuncSetAttribute(k_onnela, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a->smem));
+    a->tab = dtab;
+    a->ng = ng;
+    a->total = total;
+    a->first_n = first_n;
+    a->cp = cp_dev;
+    a->mean = mean_dev;
     // keep the host tables alive until the copies have been consumed
     PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PG_OK;
+}
+
+pg_status onnela_enqueue(pg_ctx* ctx, const OnnelaArgs* a)
+{
+    const GraphRef* tab = (const GraphRef*)a->tab;
+    PG_CUDA(ctx, cudaMemsetAsync(a->counter, 0, sizeof(int), ctx->stream));
+    k_vmax<<<std::min(a->ng, 4096), 256, 0, ctx->stream>>>(tab, a->ng, a->first_n, a->vmax);
+    PG_LAUNCHED(ctx);
+    k_onnela<<<ctx->sm_count * 4, THREADS, a->smem, ctx->stream>>>(tab, a->node0, a->ng, a->total, a->vmax, a->cp,
+                                                                   a->counter);
+    PG_LAUNCHED(ctx);
+    k_mean_segments<<<std::min(a->ng, 4096), 32, 0, ctx->stream>>>(a->cp, a->node0, a->ng, a->total, a->mean);
+    PG_LAUNCHED(ctx);
+    return PG_OK;
+}
+
+pg_status pg_onnela_table(pg_ctx* ctx, const pg_graph* const* graphs, int ng, int first_n, float* cp_dev,
+                          double* mean_dev)
+{
+    OnnelaArgs a;
+    PG_TRY(onnela_prepare(ctx, graphs, ng, first_n, cp_dev, mean_dev, &a));
+    return onnela_enqueue(ctx, &a);
+}
+
+// Binary clustering of one graph, enqueued only: per-node Cp (float), exact
+// triangles (optional) and the FP64 mean over all nodes, in device memory.
+pg_status binary_cp_prepare(pg_ctx* ctx, int n, BinaryCpArgs* a)
+{
+    PG_TRY(pg_wst(ctx, "cl.tri2", (size_t)n + 1, &a->tri2));
+    PG_TRY(pg_wst(ctx, "cl.ctr", 1, &a->counter));
+    a->smem = (size_t)((n + 31) / 32) * 4;
+    if (a->smem > ctx->smem_optin - 4096) return pg_fail(ctx, PG_ERR_TOO_LARGE, "clustering: n=%d too large", n);
+    if (a->smem > 48 * 1024)
+        PG_CUDA(ctx, cudaFuncSetAttribute(k_triangles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a->smem));
+    return PG_OK;
+}
+
+pg_status binary_cp_enqueue(pg_ctx* ctx, const BinaryCpArgs* a, const int32_t* R, const int32_t* C, int n, float* cp,
+                            long long* tri, double* mean)
+{
+    PG_CUDA(ctx, cudaMemsetAsync(a->tri2, 0, sizeof(unsigned long long) * (n + 1), ctx->stream));
+    PG_CUDA(ctx, cudaMemsetAsync(a->counter, 0, sizeof(int), ctx->stream));
+    if (n > 0) {
+        k_triangles<<<ctx->sm_count * 4, THREADS, a->smem, ctx->stream>>>(R, C, n, a->tri2, a->counter);
+        PG_LAUNCHED(ctx);
+        k_cp_binary<<<ctx->sm_count * 4, 256, 0, ctx->stream>>>(R, n, a->tri2, cp, tri);
+        PG_LAUNCHED(ctx);
+    }
+    k_mean_f32<<<1, 1024, 0, ctx->stream>>>(cp, n, mean);
+    PG_LAUNCHED(ctx);
     return PG_OK;
 }
 
@@ -277,26 +328,11 @@ extern "C" pg_status pg_clustering(pg_ctx* ctx, const pg_graph* g, int32_t kind,
     PG_TRY(pg_wst(ctx, "cl.cp", (size_t)n + 1, &dcp));
     PG_TRY(pg_wst(ctx, "cl.mean", 1, &dmean));
     if (kind == 0) {
-        unsigned long long* tri2;
         long long* tri = nullptr;
-        int* counter;
-        PG_TRY(pg_wst(ctx, "cl.tri2", (size_t)n + 1, &tri2));
-        PG_TRY(pg_wst(ctx, "cl.ctr", 1, &counter));
+        BinaryCpArgs a;
+        PG_TRY(binary_cp_prepare(ctx, n, &a));
         if (triangles) PG_TRY(pg_wst(ctx, "cl.tri", (size_t)n + 1, &tri));
-        PG_CUDA(ctx, cudaMemsetAsync(tri2, 0, sizeof(unsigned long long) * (n + 1), ctx->stream));
-        PG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
-        size_t smem = (size_t)((n + 31) / 32) * 4;
-        if (smem > ctx->smem_optin - 4096) return pg_fail(ctx, PG_ERR_TOO_LARGE, "clustering: n=%d too large", n);
-        if (smem > 48 * 1024)
-            PG_CUDA(ctx, cudaFuncSetAttribute(k_triangles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (n > 0) {
-            k_triangles<<<ctx->sm_count * 4, THREADS, smem, ctx->stream>>>(g->R, g->C, n, tri2, counter);
-            PG_LAUNCHED(ctx);
-            k_cp_binary<<<ctx->sm_count * 4, 256, 0, ctx->stream>>>(g->R, n, tri2, dcp, tri);
-            PG_LAUNCHED(ctx);
-        }
-        k_mean_f32<<<1, 1024, 0, ctx->stream>>>(dcp, n, dmean);
-        PG_LAUNCHED(ctx);
+        PG_TRY(binary_cp_enqueue(ctx, &a, g->R, g->C, n, dcp, tri, dmean));
         if (triangles) PG_TRY(pg_d2h(ctx, triangles, tri, sizeof(long long) * n));
     } else if (kind == 1) {
         const pg_graph* one[1] = {g};

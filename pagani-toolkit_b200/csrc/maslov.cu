@@ -161,7 +161,7 @@ k_ms_rounds(MsArgs p)
     const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
     const uint64_t n = (uint64_t)p.n;
-    const uint64_t key = stream_key(p.seed);
+    const uint64_t key = stream_key(p.seed_dev ? p.seed_dev[*p.round_dev] : p.seed);
     unsigned long long* pend = p.pend_a;
     unsigned long long* pnext = p.pend_b;
     MsItem* items = (MsItem*)p.items;
@@ -278,10 +278,27 @@ k_ms_rounds(MsArgs p)
     }
 }
 
-__global__ void k_ms_pairs(const int* __restrict__ ea, const int* __restrict__ eb, long long M, int2* __restrict__ p)
+// Rows of the rewired graph: R is unchanged (degrees are preserved), so each
+// slot's two directions are scattered behind per-row cursors and the rows are
+// then sorted (launch_row_sort), carrying the slot's weight.
+__global__ void k_ms_cursor(const int32_t* __restrict__ R, int32_t n, int32_t* __restrict__ cur)
 {
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < M; q += (long long)gridDim.x * blockDim.x)
-        p[q] = make_int2(ea[q], eb[q]);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) cur[v] = R[v];
+}
+
+__global__ void k_ms_scatter(const int* __restrict__ ea, const int* __restrict__ eb, const float* __restrict__ ew,
+                             long long M, int32_t* __restrict__ cur, int32_t* __restrict__ Ct, float* __restrict__ Vt)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < M; q += (long long)gridDim.x * blockDim.x) {
+        const int a = ea[q], b = eb[q];
+        const int32_t pa = atomicAdd(&cur[a], 1), pb = atomicAdd(&cur[b], 1);
+        Ct[pa] = b;
+        Ct[pb] = a;
+        if (Vt) {
+            Vt[pa] = ew[q];
+            Vt[pb] = ew[q];
+        }
+    }
 }
 }  // namespace
 
@@ -328,7 +345,9 @@ pg_status ms_prepare(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t atte
     PG_TRY(pg_wst(ctx, "ms.pend_a", (size_t)B, &a->pend_a));
     PG_TRY(pg_wst(ctx, "ms.pend_b", (size_t)B, &a->pend_b));
     PG_TRY(pg_wst(ctx, "ms.ctl", 1, &a->st));
-    PG_TRY(pg_wst(ctx, "ms.pairs", (size_t)M + 1, &a->pairs));
+    PG_TRY(pg_wst(ctx, "ms.cursor", (size_t)n + 1, &a->cursor));
+    PG_TRY(pg_wst(ctx, "ms.ct", (size_t)(2 * M) + 1, &a->ct));
+    if (g->V) PG_TRY(pg_wst(ctx, "ms.vt", (size_t)(2 * M) + 1, &a->vt));
     a->words = words;
     a->attempts = (uint64_t)attempts;
     int per_sm = 0;
@@ -365,9 +384,17 @@ pg_status ms_enqueue(pg_ctx* ctx, const pg_graph* g, MsArgs* a)
         PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_ms_rounds, *a));
         PG_LAUNCHED(ctx);
     }
-    k_ms_pairs<<<grid, 256, 0, ctx->stream>>>(a->ea, a->eb, a->M, a->pairs);
-    PG_LAUNCHED(ctx);
     return PG_OK;
+}
+
+pg_status ms_rows_enqueue(pg_ctx* ctx, const pg_graph* g, MsArgs* a, int32_t* C_out, float* V_out)
+{
+    const int grid = ctx->sm_count * 4;
+    k_ms_cursor<<<grid, 256, 0, ctx->stream>>>(g->R, a->n, a->cursor);
+    PG_LAUNCHED(ctx);
+    k_ms_scatter<<<grid, 256, 0, ctx->stream>>>(a->ea, a->eb, a->ew, a->M, a->cursor, a->ct, V_out ? a->vt : nullptr);
+    PG_LAUNCHED(ctx);
+    return launch_row_sort(ctx, g->R, a->n, a->ct, V_out ? a->vt : nullptr, C_out, V_out);
 }
 
 extern "C" int64_t pg_maslov_round_size(int64_t M) { return ms_round_size(M); }
@@ -381,7 +408,17 @@ extern "C" pg_status pg_maslov(pg_ctx* ctx, const pg_graph* g, uint64_t seed, in
     MsArgs a;
     PG_TRY(ms_prepare(ctx, g, seed, attempts, &a));
     PG_TRY(ms_enqueue(ctx, g, &a));
-    PG_TRY(pg_csr_from_pairs(ctx, g->n, a.pairs, g->V ? a.ew : nullptr, a.M, out));
+    pg_graph* r;
+    PG_TRY(pg_graph_alloc(ctx, g->n, g->nnz, g->V != nullptr, &r));
+    cudaError_t e = cudaMemcpyAsync(r->R, g->R, sizeof(int32_t) * ((size_t)g->n + 1), cudaMemcpyDeviceToDevice,
+                                    ctx->stream);
+    pg_status st = e == cudaSuccess ? ms_rows_enqueue(ctx, g, &a, r->C, r->V)
+                                    : pg_fail(ctx, PG_ERR_CUDA, "pg_maslov: %s", cudaGetErrorString(e));
+    if (st != PG_OK) {
+        pg_graph_free(r);
+        return st;
+    }
+    *out = r;
     if (committed) {
         MsControl c;
         PG_TRY(pg_d2h(ctx, &c, a.st, sizeof c));

@@ -36,7 +36,11 @@ struct MsArgs {
     void* items;                     // per round item: the evaluated attempt
     unsigned long long *pend_a, *pend_b;
     MsControl* st;
-    int2* pairs;                     // result: the M slots as pairs
+    const uint64_t* seed_dev;        // optional: seed = seed_dev[*round_dev] (one captured graph, many seeds)
+    const int* round_dev;
+    int32_t* cursor;                 // row cursors of the rebuild
+    int32_t* ct;                     // unsorted rows of the rebuild
+    float* vt;
 };
 
 // Round size and pair-table size for M slots (fixed functions of M, so the
@@ -45,6 +49,9 @@ int64_t ms_round_size(int64_t M);
 uint32_t ms_table_size(int64_t B);
 // Sizes the workspace (may allocate) and fills the arguments.
 pg_status ms_prepare(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t attempts, MsArgs* a);
-// Enqueues the rewiring of g on the context stream: result slots in a->pairs
-// (and a->ew); no allocation, no host synchronisation.
+// Enqueues the rewiring of g on the context stream: result slots in
+// a->ea / a->eb (and a->ew); no allocation, no host synchronisation.
 pg_status ms_enqueue(pg_ctx* ctx, const pg_graph* g, MsArgs* a);
+// Enqueues the rows of the rewired graph: R is g->R (unchanged), columns
+// ascending into C_out (nnz entries), weights into V_out (null: binary).
+pg_status ms_rows_enqueue(pg_ctx* ctx, const pg_graph* g, MsArgs* a, int32_t* C_out, float* V_out);

@@ -4,116 +4,253 @@
 // node.  A level is a pull sweep: node v ORs the frontier words of its
 // neighbours, keeps the bits it has not seen, and stops scanning once every
 // missing source bit is found.  Because the graph is undirected,
-// d(s, v) = d(v, s): node v accumulates sum_s 1/d(s, v) directly, so the
-// per-node efficiency needs no transposition or atomics.
+// d(s, v) = d(v, s), so node v counts the sources it reaches at each
+// distance itself: cnt[v][d] (exact integers, summed over all batches), and
+// at the end inv[v] = sum_d cnt[v][d] / d with d ascending -- the oracle's and
+// APSP_BFS's per-source order, so the result does not depend on how the
+// sources are batched and equals the oracle's bit for bit.  Distances beyond
+// MAX_D are added to inv[v] directly as they are found.
+//
+// One cooperative launch runs every batch and level (grid-wide barriers
+// between levels, the "any source still growing" flag in device memory), so
+// the computation needs no host round trip and can be captured in a CUDA
+// graph.  The sources per batch (NW) and the CTAs per SM are picked by the
+// autotuner; the result is the same for every choice.
 #include "pg_internal.cuh"
+#include "paths.cuh"
+#include "tune.cuh"
 #include <algorithm>
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 namespace {
-constexpr int NW = 4;               // 256 sources per batch
-constexpr int SRC_PER_BATCH = 64 * NW;
+constexpr int THREADS = 256;
 
-struct Words { unsigned long long w[NW]; };
+template <int NW>
+struct Words {
+    unsigned long long w[NW];
+};
 
-__global__ void k_msbfs_init(int32_t n, int s0, int ns, Words* __restrict__ front, Words* __restrict__ seen)
+template <int NW>
+__global__ void __launch_bounds__(THREADS)
+k_msbfs_all(PathArgs p)
 {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        Words f;
-#pragma unroll
-        for (int q = 0; q < NW; q++) f.w[q] = 0ULL;
-        int b = v - s0;
-        if (b >= 0 && b < ns) f.w[b >> 6] = 1ULL << (b & 63);
-        front[v] = f;
-        seen[v] = f;
-    }
-}
-
-// One level: warp per node.  Writes the next frontier, merges it into `seen`
-// after the sweep (double buffered: seen_in -> seen_out), accumulates
-// popcount/d into inv[v] and the hop histogram.
-__global__ void k_msbfs_level(const int32_t* __restrict__ R, const int32_t* __restrict__ C, int32_t n,
-                              const Words* __restrict__ front, Words* __restrict__ next,
-                              const Words* __restrict__ seen_in, Words* __restrict__ seen_out, int d,
-                              Words full, double* __restrict__ inv, unsigned long long* __restrict__ hist,
-                              int max_hop, int* __restrict__ active)
-{
+    cg::grid_group grid = cg::this_grid();
+    const int n = p.n;
     const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    unsigned long long found_total = 0;
-    for (int v = gw; v < n; v += nw) {
-        Words sv = seen_in[v];
-        Words need;
-        bool any_need = false;
-#pragma unroll
-        for (int q = 0; q < NW; q++) { need.w[q] = full.w[q] & ~sv.w[q]; any_need |= need.w[q] != 0ULL; }
-        Words acc;
-#pragma unroll
-        for (int q = 0; q < NW; q++) acc.w[q] = 0ULL;
-        if (any_need) {
-            const int32_t s = R[v], e = R[v + 1];
-            for (int32_t base = s; base < e; base += 32) {
-                int32_t f = base + lane;
-                if (f < e) {
-                    Words fu = front[C[f]];
-#pragma unroll
-                    for (int q = 0; q < NW; q++) acc.w[q] |= fu.w[q];
-                }
-                bool done = true;
-#pragma unroll
-                for (int q = 0; q < NW; q++) {
-                    unsigned long long x = acc.w[q];
-                    for (int o = 16; o; o >>= 1) x |= __shfl_xor_sync(0xffffffffu, x, o);
-                    acc.w[q] = x;
-                    done &= (x & need.w[q]) == need.w[q];
-                }
-                if (done) break;
-            }
-        }
-        Words nx;
-        int cnt = 0;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    const int gw = (int)(tid >> 5), nw = (int)(nt >> 5);
+    Words<NW>* front = (Words<NW>*)p.front;
+    Words<NW>* next = (Words<NW>*)p.next;
+    Words<NW>* seen_a = (Words<NW>*)p.seen_a;
+    Words<NW>* seen_b = (Words<NW>*)p.seen_b;
+    constexpr int SRC = 64 * NW;
+    int diam = 0;
+    for (int s0 = 0; s0 < n; s0 += SRC) {
+        const int ns = min(SRC, n - s0);
+        Words<NW> full;
 #pragma unroll
         for (int q = 0; q < NW; q++) {
-            nx.w[q] = acc.w[q] & need.w[q];
-            cnt += __popcll(nx.w[q]);
+            const int c = max(0, min(64, ns - q * 64));
+            full.w[q] = c == 64 ? ~0ULL : (c ? ((1ULL << c) - 1ULL) : 0ULL);
         }
-        if (lane == 0) {
-            next[v] = nx;
-            Words so;
+        for (int v = (int)tid; v < n; v += (int)nt) {
+            Words<NW> f;
 #pragma unroll
-            for (int q = 0; q < NW; q++) so.w[q] = sv.w[q] | nx.w[q];
-            seen_out[v] = so;
-            if (cnt) inv[v] += (double)cnt / (double)d;
+            for (int q = 0; q < NW; q++) f.w[q] = 0ULL;
+            const int b = v - s0;
+            if (b >= 0 && b < ns) f.w[b >> 6] = 1ULL << (b & 63);
+            front[v] = f;
+            seen_a[v] = f;
         }
-        found_total += cnt;
+        if (tid == 0) p.flags[0] = p.flags[1] = p.flags[2] = 0;
+        grid.sync();
+        Words<NW>*sin = seen_a, *sout = seen_b, *cur = front, *nxt = next;
+        for (int d = 1;; d++) {
+            unsigned long long found_total = 0;
+            for (int v = gw; v < n; v += nw) {
+                const Words<NW> sv = sin[v];
+                Words<NW> need, acc;
+                bool any_need = false;
+#pragma unroll
+                for (int q = 0; q < NW; q++) {
+                    need.w[q] = full.w[q] & ~sv.w[q];
+                    any_need |= need.w[q] != 0ULL;
+                    acc.w[q] = 0ULL;
+                }
+                if (any_need) {
+                    const int32_t s = p.R[v], e = p.R[v + 1];
+                    for (int32_t base = s; base < e; base += 32) {
+                        const int32_t f = base + lane;
+                        if (f < e) {
+                            const Words<NW> fu = cur[p.C[f]];
+#pragma unroll
+                            for (int q = 0; q < NW; q++) acc.w[q] |= fu.w[q];
+                        }
+                        bool done = true;
+#pragma unroll
+                        for (int q = 0; q < NW; q++) {
+                            unsigned long long x = acc.w[q];
+                            for (int o = 16; o; o >>= 1) x |= __shfl_xor_sync(0xffffffffu, x, o);
+                            acc.w[q] = x;
+                            done &= (x & need.w[q]) == need.w[q];
+                        }
+                        if (done) break;
+                    }
+                }
+                int cnt = 0;
+                Words<NW> nx, so;
+#pragma unroll
+                for (int q = 0; q < NW; q++) {
+                    nx.w[q] = acc.w[q] & need.w[q];
+                    so.w[q] = sv.w[q] | nx.w[q];
+                    cnt += __popcll(nx.w[q]);
+                }
+                if (lane == 0) {
+                    nxt[v] = nx;
+                    sout[v] = so;
+                    if (cnt) {
+                        if (d <= MAX_D) p.cnt[(long long)v * MAX_D + (d - 1)] += (unsigned)cnt;
+                        else p.inv_far[v] += (double)cnt / (double)d;
+                    }
+                }
+                found_total += (unsigned)cnt;
+            }
+            if (lane == 0 && found_total) {
+                p.flags[d % 3] = 1;
+                if (p.hist && d <= p.max_hop) atomicAdd(&p.hist[d], found_total);
+            }
+            grid.sync();
+            if (tid == 0) p.flags[(d + 2) % 3] = 0;   // last read before this barrier, next written after the next
+            if (!((volatile int*)p.flags)[d % 3]) break;
+            diam = max(diam, d);
+            Words<NW>* t = sin; sin = sout; sout = t;
+            t = cur; cur = nxt; nxt = t;
+        }
     }
-    if (lane == 0 && found_total) {
-        *active = 1;
-        if (d <= max_hop) atomicAdd(&hist[d], found_total);
-    }
+    if (tid == 0) *p.diameter = diam;
 }
 
-__global__ void k_eff(const double* __restrict__ inv, int32_t n, float* __restrict__ eff)
+// inv[v] = sum_d cnt[v][d] / d (d ascending), eff[v] = inv[v] / (n - 1)
+__global__ void k_inv_eff(PathArgs p)
 {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-        eff[v] = n > 1 ? (float)(inv[v] / (double)(n - 1)) : 0.0f;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < p.n; v += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        const unsigned* c = p.cnt + (long long)v * MAX_D;
+        for (int d = 1; d <= MAX_D; d++)
+            if (c[d - 1]) acc += (double)c[d - 1] / (double)d;
+        acc += p.inv_far[v];
+        p.inv[v] = acc;
+        if (p.eff) p.eff[v] = p.n > 1 ? (float)(acc / (double)(p.n - 1)) : 0.0f;
+    }
 }
 
-__global__ void k_sum_f64(const double* __restrict__ x, int32_t n, double* __restrict__ out)
+// total = sum_v inv[v] in a fixed order; lp = n(n-1)/total (0 without paths)
+__global__ void k_lp(PathArgs p)
 {
     __shared__ double sh[1024];
+    const int n = p.n;
     double a = 0.0;
-    int per = (n + blockDim.x - 1) / blockDim.x;
-    int lo = threadIdx.x * per, hi = min(n, lo + per);
-    for (int i = lo; i < hi; i++) a += x[i];
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int lo = threadIdx.x * per, hi = min(n, lo + per);
+    for (int i = lo; i < hi; i++) a += p.inv[i];
     sh[threadIdx.x] = a;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int i = 0; i < (int)blockDim.x; i++) t += sh[i];
-        *out = t;
+        p.out[0] = t;
+        p.out[1] = t > 0.0 ? (double)n * (double)(n - 1) / t : 0.0;
     }
 }
+
+template <int NW>
+pg_status launch_all(pg_ctx* ctx, PathArgs& a, int ctas_per_sm)
+{
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeCooperative;
+    attr.val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctx->sm_count * ctas_per_sm);
+    cfg.blockDim = dim3(THREADS);
+    cfg.stream = ctx->stream;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_msbfs_all<NW>, a));
+    PG_LAUNCHED(ctx);
+    return PG_OK;
+}
+
+int max_ctas(pg_ctx* ctx, int nw)
+{
+    int per_sm = 0;
+    cudaError_t e = nw == 8 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_msbfs_all<8>, THREADS, 0)
+                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_msbfs_all<4>, THREADS, 0);
+    (void)ctx;
+    return e == cudaSuccess ? per_sm : 0;
+}
 }  // namespace
+
+pg_status paths_prepare(pg_ctx* ctx, const pg_graph* g, int max_hop, PathArgs* a)
+{
+    const int n = g->n;
+    memset(a, 0, sizeof *a);
+    a->n = n;
+    a->R = g->R;
+    a->C = g->C;
+    a->max_hop = max_hop;
+    // both word widths share the buffers: sized for the wider one
+    PG_TRY(pg_ws(ctx, "bfs.front", ((size_t)n + 1) * 64, &a->front));
+    PG_TRY(pg_ws(ctx, "bfs.next", ((size_t)n + 1) * 64, &a->next));
+    PG_TRY(pg_ws(ctx, "bfs.seen_a", ((size_t)n + 1) * 64, &a->seen_a));
+    PG_TRY(pg_ws(ctx, "bfs.seen_b", ((size_t)n + 1) * 64, &a->seen_b));
+    PG_TRY(pg_wst(ctx, "bfs.cnt", ((size_t)n + 1) * MAX_D, &a->cnt));
+    PG_TRY(pg_wst(ctx, "bfs.inv_far", (size_t)n + 1, &a->inv_far));
+    PG_TRY(pg_wst(ctx, "bfs.inv", (size_t)n + 1, &a->inv));
+    PG_TRY(pg_wst(ctx, "bfs.eff", (size_t)n + 1, &a->eff));
+    PG_TRY(pg_wst(ctx, "bfs.hist", (size_t)max_hop + 2, &a->hist));
+    PG_TRY(pg_wst(ctx, "bfs.flags", 4, &a->flags));
+    PG_TRY(pg_wst(ctx, "bfs.diam", 1, &a->diameter));
+    PG_TRY(pg_wst(ctx, "bfs.out", 2, &a->out));
+    // launch shape: sources per batch x CTAs per SM, from the autotuner
+    const int cap4 = max_ctas(ctx, 4), cap8 = max_ctas(ctx, 8);
+    if (cap4 < 1 || cap8 < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "paths: kernel does not fit an SM");
+    std::vector<TuneChoice> cands;
+    for (int nw : {4, 8})
+        for (int c : {2, 4, 8})
+            if (c <= (nw == 8 ? cap8 : cap4)) cands.push_back({nw, c});
+    const std::string key = tune_key("msbfs", n, g->nnz);
+    TuneChoice best{4, std::min(4, cap4)};
+    PG_TRY(tune_pick(ctx, key, cands, &best, [&](const TuneChoice& c) -> pg_status {
+        a->nw = c.a;
+        a->ctas_per_sm = c.b;
+        return paths_enqueue(ctx, a);
+    }));
+    a->nw = best.a;
+    a->ctas_per_sm = best.b;
+    return PG_OK;
+}
+
+pg_status paths_enqueue(pg_ctx* ctx, PathArgs* a)
+{
+    const int n = a->n;
+    PG_CUDA(ctx, cudaMemsetAsync(a->cnt, 0, sizeof(unsigned) * ((size_t)n + 1) * MAX_D, ctx->stream));
+    PG_CUDA(ctx, cudaMemsetAsync(a->inv_far, 0, sizeof(double) * ((size_t)n + 1), ctx->stream));
+    PG_CUDA(ctx, cudaMemsetAsync(a->hist, 0, sizeof(unsigned long long) * ((size_t)a->max_hop + 2), ctx->stream));
+    PG_CUDA(ctx, cudaMemsetAsync(a->diameter, 0, sizeof(int), ctx->stream));
+    if (n > 0) {
+        if (a->nw == 8) PG_TRY(launch_all<8>(ctx, *a, a->ctas_per_sm));
+        else PG_TRY(launch_all<4>(ctx, *a, a->ctas_per_sm));
+    }
+    const int grid = std::max(1, std::min(ctx->sm_count * 8, ceil_div(n, 256)));
+    k_inv_eff<<<grid, 256, 0, ctx->stream>>>(*a);
+    PG_LAUNCHED(ctx);
+    k_lp<<<1, 1024, 0, ctx->stream>>>(*a);
+    PG_LAUNCHED(ctx);
+    return PG_OK;
+}
 
 extern "C" pg_status pg_paths(pg_ctx* ctx, const pg_graph* g, float* eff, double* inv_sum, double* lp,
                               int64_t* hop_hist, int32_t max_hop, int32_t* diameter)
@@ -121,65 +258,24 @@ extern "C" pg_status pg_paths(pg_ctx* ctx, const pg_graph* g, float* eff, double
     if (!ctx || !g) return pg_fail(ctx, PG_ERR_INVALID, "pg_paths: null argument");
     if (max_hop < 0) max_hop = 0;
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    PathArgs a;
+    PG_TRY(paths_prepare(ctx, g, max_hop, &a));
+    PG_TRY(paths_enqueue(ctx, &a));
     const int n = g->n;
-    Words *front, *next, *seen_a, *seen_b;
-    double *inv, *tot;
-    unsigned long long* hist;
-    int* active;
-    PG_TRY(pg_wst(ctx, "bfs.front", (size_t)n + 1, &front));
-    PG_TRY(pg_wst(ctx, "bfs.next", (size_t)n + 1, &next));
-    PG_TRY(pg_wst(ctx, "bfs.seen_a", (size_t)n + 1, &seen_a));
-    PG_TRY(pg_wst(ctx, "bfs.seen_b", (size_t)n + 1, &seen_b));
-    PG_TRY(pg_wst(ctx, "bfs.inv", (size_t)n + 1, &inv));
-    PG_TRY(pg_wst(ctx, "bfs.tot", 1, &tot));
-    PG_TRY(pg_wst(ctx, "bfs.hist", (size_t)max_hop + 2, &hist));
-    PG_TRY(pg_wst(ctx, "bfs.active", 64, &active));
-    PG_CUDA(ctx, cudaMemsetAsync(inv, 0, sizeof(double) * (n + 1), ctx->stream));
-    PG_CUDA(ctx, cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * (max_hop + 2), ctx->stream));
-    int* hact;
-    PG_TRY(pg_pinned(ctx, 4096, (void**)&hact));
-    int diam = 0;
-    const int grid_nodes = std::max(1, std::min(ctx->sm_count * 16, ceil_div(n, 256)));
-    const int grid_warps = std::max(1, std::min(ctx->sm_count * 16, ceil_div((long long)n * 32, 256)));
-    for (int s0 = 0; s0 < n; s0 += SRC_PER_BATCH) {
-        const int ns = std::min(SRC_PER_BATCH, n - s0);
-        Words full;
-        for (int q = 0; q < NW; q++) {
-            int lo = q * 64, c = std::max(0, std::min(64, ns - lo));
-            full.w[q] = c == 64 ? ~0ULL : (c ? ((1ULL << c) - 1ULL) : 0ULL);
-        }
-        k_msbfs_init<<<grid_nodes, 256, 0, ctx->stream>>>(n, s0, ns, front, seen_a);
-        PG_LAUNCHED(ctx);
-        Words *sin = seen_a, *sout = seen_b, *cur = front, *nxt = next;
-        for (int d = 1; d <= n; d++) {
-            PG_CUDA(ctx, cudaMemsetAsync(active, 0, sizeof(int), ctx->stream));
-            k_msbfs_level<<<grid_warps, 256, 0, ctx->stream>>>(g->R, g->C, n, cur, nxt, sin, sout, d, full, inv,
-                                                               hist, max_hop, active);
-            PG_LAUNCHED(ctx);
-            PG_CUDA(ctx, cudaMemcpyAsync(hact, active, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-            PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            if (!*hact) break;
-            diam = std::max(diam, d);
-            std::swap(sin, sout);
-            std::swap(cur, nxt);
-        }
-    }
-    float* deff;
-    PG_TRY(pg_wst(ctx, "bfs.eff", (size_t)n + 1, &deff));
-    k_eff<<<grid_nodes, 256, 0, ctx->stream>>>(inv, n, deff);
-    PG_LAUNCHED(ctx);
-    k_sum_f64<<<1, 1024, 0, ctx->stream>>>(inv, n, tot);
-    PG_LAUNCHED(ctx);
-    double total = 0.0;
-    PG_TRY(pg_d2h(ctx, &total, tot, sizeof(double)));
-    if (eff) PG_TRY(pg_d2h(ctx, eff, deff, sizeof(float) * n));
-    if (inv_sum) PG_TRY(pg_d2h(ctx, inv_sum, inv, sizeof(double) * n));
+    double out[2];
+    PG_TRY(pg_d2h(ctx, out, a.out, sizeof out));
+    if (eff) PG_TRY(pg_d2h(ctx, eff, a.eff, sizeof(float) * n));
+    if (inv_sum) PG_TRY(pg_d2h(ctx, inv_sum, a.inv, sizeof(double) * n));
     if (hop_hist) {
         std::vector<unsigned long long> h(max_hop + 1);
-        PG_TRY(pg_d2h(ctx, h.data(), hist, sizeof(unsigned long long) * (max_hop + 1)));
+        PG_TRY(pg_d2h(ctx, h.data(), a.hist, sizeof(unsigned long long) * (max_hop + 1)));
         for (int d = 0; d <= max_hop; d++) hop_hist[d] = (int64_t)h[d];
     }
-    if (lp) *lp = total > 0.0 ? (double)n * (double)(n - 1) / total : 0.0;
-    if (diameter) *diameter = diam;
+    if (lp) *lp = out[1];
+    if (diameter) {
+        int dm = 0;
+        PG_TRY(pg_d2h(ctx, &dm, a.diameter, sizeof dm));
+        *diameter = dm;
+    }
     return PG_OK;
 }

@@ -107,6 +107,11 @@ pg_status pg_csr_from_pairs(pg_ctx* ctx, int32_t n, const int2* pairs, const flo
                             int64_t npairs, pg_graph** out);
 // Sorts the columns of every row ascending (carrying V when present).
 pg_status pg_csr_sort_rows(pg_ctx* ctx, pg_graph* g);
+// Row sort of a CSR whose rows are filled but unordered: Cin/Vin -> Cout/Vout
+// (Vin may be null).  Only launches kernels (capture-safe once the kernel's
+// shared-memory attribute has been set by a first call).
+pg_status launch_row_sort(pg_ctx* ctx, const int32_t* R, int32_t n, const int32_t* Cin, const float* Vin,
+                          int32_t* Cout, float* Vout);
 
 // Exclusive scan of int32 counts into int64 offsets (n+1 entries).
 pg_status pg_scan_counts(pg_ctx* ctx, const int32_t* cnt, int64_t* off, int32_t n);

@@ -68,12 +68,12 @@ class Subject(ct.Structure):
                 ("cp", ct.c_void_p), ("eff", ct.c_void_p), ("bc", ct.c_void_p), ("modules", ct.c_void_p),
                 ("edges", ct.c_int64), ("tau", ct.c_double), ("cp_mean", ct.c_double), ("lp", ct.c_double),
                 ("Q", ct.c_double), ("n_modules", ct.c_int32), ("gamma", ct.c_double), ("lambda_", ct.c_double),
-                ("sigma", ct.c_double)]
+                ("sigma", ct.c_double), ("surrogate_graph_replays", ct.c_int32)]
 
 
 class RunOpts(ct.Structure):
     _fields_ = [("build", BuildOpts), ("n_random", ct.c_int32), ("swaps_per_edge", ct.c_int64),
-                ("seed", ct.c_uint64)]
+                ("seed", ct.c_uint64), ("cuda_graphs", ct.c_int32)]
 
 
 LOG_FN = ct.CFUNCTYPE(None, ct.c_char_p, ct.c_void_p)
@@ -334,31 +334,44 @@ class Context:
         return Cohort(self, N, fisher, weighted)
 
     def run_subjects(self, bolds, mode="s", value=1.0, sign="abs", n_random=0, swaps_per_edge=2, seed=1,
-                     metrics=("degree", "cp", "eff", "bc", "modules")):
+                     metrics=("degree", "cp", "eff", "bc", "modules"), weighted=False, precision="bf16x3",
+                     cuda_graphs=True, device_ptrs=None):
         """pg_run_subjects over (T, N) float32 series: one dict per subject with
-        the requested per-node arrays and the scalar results."""
+        the requested per-node arrays and the scalar results.  device_ptrs:
+        optional list of (pointer, (T, N)) of series already on the device."""
         o = RunOpts()
         lib().pg_run_opts_default(ct.byref(o))
         o.build.mode = PG_THRESH_SPARSITY if mode in ("s", "sparsity") else PG_THRESH_R
         o.build.value = value
         o.build.sign = PG_ABS if sign == "abs" else PG_SIGNED
+        o.build.weighted = int(weighted)
+        o.build.precision = PG_FP32 if precision == "fp32" else PG_SPLIT_BF16
+        o.build.input_on_device = int(device_ptrs is not None)
         o.n_random, o.swaps_per_edge, o.seed = n_random, swaps_per_edge, seed
-        keep, subs = [], (Subject * max(1, len(bolds)))()
+        o.cuda_graphs = int(cuda_graphs)
+        count = len(device_ptrs) if device_ptrs is not None else len(bolds)
+        keep, subs = [], (Subject * max(1, count))()
         outs = []
-        for k, b in enumerate(bolds):
-            b = np.ascontiguousarray(b, np.float32)
-            T, N = b.shape
+        for k in range(count):
+            if device_ptrs is not None:
+                ptr, (T, N) = device_ptrs[k]
+            else:
+                b = np.ascontiguousarray(bolds[k], np.float32)
+                T, N = b.shape
+                keep.append(b)
+                ptr = b.ctypes.data
             arrs = {m: np.zeros(N, np.int32 if m == "modules" else np.float32) for m in metrics}
-            keep += [b] + list(arrs.values())
-            subs[k].bold, subs[k].N, subs[k].T = b.ctypes.data, N, T
+            keep += list(arrs.values())
+            subs[k].bold, subs[k].N, subs[k].T = ptr, N, T
             for m, a in arrs.items():
                 setattr(subs[k], m, a.ctypes.data)
             outs.append(arrs)
-        self._check(lib().pg_run_subjects(self.h, subs, len(bolds), ct.byref(o)))
+        self._check(lib().pg_run_subjects(self.h, subs, count, ct.byref(o)))
         res = []
         for k, arrs in enumerate(outs):
             d = dict(arrs)
-            for f in ("edges", "tau", "cp_mean", "lp", "Q", "n_modules", "gamma", "lambda_", "sigma"):
+            for f in ("edges", "tau", "cp_mean", "lp", "Q", "n_modules", "gamma", "lambda_", "sigma",
+                      "surrogate_graph_replays"):
                 d[f.rstrip("_")] = getattr(subs[k], f)
             res.append(d)
         return res
