@@ -257,6 +257,188 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+
+# ------------------------------------------------- precision report (config 3)
+FIXTURE_58K = os.path.join(ROOT, "tests", "golden", "subject58k.npz")
+FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # FP32 lanes x FMA x max clock
+
+
+def _sha(*arrays):
+    import hashlib
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def precision_report(ctx, bold_dev, last):
+    """The 58k subject against the FP64 oracle's results committed in
+    tests/golden/subject58k.npz: edge sets at 0.5 / 1 / 2 % for both Gram
+    precisions (SHA-256 of the CSR, tau, k), the tile error |r_tile - r| over
+    the FP64 recheck band, and the relative errors of the timed step's
+    betweenness, Q and Lp."""
+    if N_VOX != 58000 or not os.path.exists(FIXTURE_58K):
+        return None
+    fx = np.load(FIXTURE_58K)
+    rep = {"oracle": "FP64 restatement (tests/golden/subject58k.npz)", "edge_sets": {}}
+    for prec in ("bf16x3", "fp32"):
+        rows = []
+        for q, s in enumerate(fx["sparsities"]):
+            g, info = ctx.build_graph(None, mode="s", value=float(s), sign="abs", precision=prec,
+                                      device_ptr=(bold_dev.data_ptr(), (T_LEN, N_VOX)))
+            R, C, _ = g.to_csr()
+            g.free()
+            rows.append({"sparsity_percent": float(s), "k": int(fx["k"][q]), "edges": info["edges"],
+                         "tau_equal": info["tau"] == float(fx["tau"][q]),
+                         "edge_set_identical": _sha(R, C) == str(fx["csr_sha256"][q]),
+                         "band_pairs": info["band_pairs"], "band_err_max": info["band_err_max"],
+                         "band_err_mean": info["band_err_mean"]})
+        rep["edge_sets"][prec] = rows
+    bc_ref = fx["bc"]
+    rep["bc_rel_err_max"] = float(np.max(np.abs(last["bc64"] - bc_ref) / np.maximum(np.abs(bc_ref), 1.0)))
+    rep["Q_rel_err"] = abs(last["Q"] - float(fx["Q"])) / abs(float(fx["Q"]))
+    rep["newman_labels_identical"] = bool(np.array_equal(last["labels"], fx["labels"]))
+    rep["lp_rel_err"] = abs(last["lp"] - float(fx["lp"])) / float(fx["lp"])
+    rep["timed_step_edges_and_tau_equal"] = (last["nnz"] // 2 == int(fx["k"][1]) and
+                                             last["build"]["tau"] == float(fx["tau"][1]))
+    return rep
+
+
+def build_stage(ctx, bold_dev, stream, hbm_peak, bf16_peak, reps=5):
+    """Network construction alone for each Gram precision (CUDA events around
+    pg_build_graph with the series on the device, after one warm-up), and the
+    emit pass's arithmetic rate: 2*M1*T useful flop per product (3 products
+    in split-BF16) against the measured bf16 tensor peak, or against the
+    nominal FP32 SIMT peak for the FP32 path."""
+    import torch
+    M1 = N_VOX * (N_VOX - 1) // 2
+    out = {}
+    for prec in ("bf16x3", "fp32"):
+        kw = dict(mode="s", value=SPARSITY, sign="abs", precision=prec, device_ptr=(bold_dev.data_ptr(), (T_LEN, N_VOX)))
+        g, info = ctx.build_graph(None, **kw)
+        g.free()
+        ms, emit, hist = [], [], []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g, info = ctx.build_graph(None, **kw)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            g.free()
+            ms.append(e0.elapsed_time(e1))
+            emit.append(info["ms_emit"])
+            hist.append(info["ms_hist"])
+        emit_ms = float(np.median(emit))
+        products = 3 if prec == "bf16x3" else 1
+        tflops = products * 2.0 * M1 * T_LEN / (emit_ms / 1000.0) / 1e12
+        peak = bf16_peak if prec == "bf16x3" else FP32_SIMT_NOMINAL_TFLOPS
+        out[prec] = {"ms_build": float(np.median(ms)), "ms_gram_hist_passes": float(np.median(hist)),
+                     "ms_gram_emit_pass": emit_ms, "kernel": "k_gram_tc" if prec == "bf16x3" else "k_gram_simt",
+                     "emit_tflops": tflops, "peak_tflops": peak,
+                     "peak_source": "measured bf16 (MEASURED_PEAKS.json)" if prec == "bf16x3"
+                     else "nominal FP32 SIMT (148 SMs x 128 lanes x 2 x 1.965 GHz)",
+                     "frac": tflops / peak}
+    out["split_bf16_speedup_vs_fp32"] = out["fp32"]["ms_build"] / out["bf16x3"]["ms_build"]
+    return out
+
+
+# ----------------------------------------------------------- cohort (config 5)
+COHORT_N, COHORT_T, COHORT_SPARSITY, COHORT_RANDOM, COHORT_SWAPS = (40000, 70000), (150, 240), 0.5, 20, 10
+
+
+def cohort_subjects(count, rank=0):
+    """Subjects of the 64-subject cohort configuration, drawn in order from one
+    seeded stream: N ~ U{40k..70k}, T ~ U{150..240}, 20 latent signals."""
+    from pagani import synth
+    rng = np.random.Generator(np.random.PCG64(synth.subject_seed(5, 500 + rank)))
+    out = []
+    for k in range(count):
+        n = int(rng.integers(COHORT_N[0], COHORT_N[1] + 1))
+        t = int(rng.integers(COHORT_T[0], COHORT_T[1] + 1))
+        out.append((n, t, synth.subject_seed(5, 64 * rank + k)))
+    return out
+
+
+def cohort_leg(ctx, count, rank=0):
+    """pg_run_subjects on `count` subjects of the cohort configuration, series
+    in pinned host memory (the copy to the device is inside the time): build
+    at 0.5 %, degree, Cp, hop Lp / efficiency, 20 Maslov surrogates with
+    10 x |E| attempts each (clustering and Lp of every surrogate, CUDA-graph
+    replays) and sigma.  Wall time per subject around the call (it returns
+    after its results are on the host)."""
+    import torch
+    from pagani import synth
+    subs = cohort_subjects(count, rank)
+    series = [torch.from_numpy(synth.bold_series(n, t, N_SIG, sd)).pin_memory() for n, t, sd in subs]
+    res = {}
+    for prec in ("bf16x3", "fp32"):
+        kw = dict(mode="s", value=COHORT_SPARSITY, sign="abs", n_random=COHORT_RANDOM, swaps_per_edge=COHORT_SWAPS,
+                  seed=5, metrics=("degree", "cp", "eff"), precision=prec)
+        ctx.run_subjects([series[0].numpy()], **kw)          # warm-up (autotuner, workspace)
+        secs, sig = [], []
+        for b in series:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = ctx.run_subjects([b.numpy()], **kw)[0]
+            secs.append(time.perf_counter() - t0)
+            sig.append({"sigma": r["sigma"], "gamma": r["gamma"], "lambda": r["lambda"], "edges": r["edges"],
+                        "replays": r["surrogate_graph_replays"]})
+        res[prec] = {"subjects_per_min": 60.0 * len(secs) / sum(secs), "s_per_subject": secs, "results": sig}
+    res["subjects"] = [{"N": n, "T": t} for n, t, _ in subs]
+    res["workload"] = (f"cohort sample: {count} of the 64 subjects (N ~ U{{40k..70k}}, T ~ U{{150..240}}), top 0.5% "
+                       f"|r|, degree, Cp, Lp/efficiency, {COHORT_RANDOM} Maslov surrogates x {COHORT_SWAPS}|E| "
+                       "attempts with Cp and Lp each, gamma/lambda/sigma; series from pinned host memory")
+    return res
+
+
+# ------------------------------------------------- weighted ROI batch (config 4)
+ROI_GRAPHS, ROI_N, ROI_T, ROI_R = 512, (90, 1024), 1200, 0.2
+
+
+def roi_batch_leg(ctx, stream, reps=3):
+    """512 ROI-level graphs, n ~ U{90..1024}, T = 1200, weight r for r > 0.2
+    (the weighted tool's rule), distance 1/w: blocked Floyd-Warshall APSP
+    (FP32 min-plus) and Onnela clustering of all graphs in one cooperative
+    launch (pg_fw_batched), CUDA events around the call after a warm-up
+    (graphs built beforehand).  FP32 roofline: 2 operations (add, min) per
+    (i, j, k) update, useful updates sum n^3, against the nominal FP32 rate."""
+    import torch
+    from pagani import synth
+    series = synth.roi_batch(ROI_GRAPHS, ROI_N[0], ROI_N[1], ROI_T, N_SIG, synth.subject_seed(4))
+    t0 = time.perf_counter()
+    graphs = [ctx.build_graph(b, mode="r", value=ROI_R, sign="signed", weighted=True)[0] for b in series]
+    build_s = time.perf_counter() - t0
+    ctx.fw_batched(graphs)                       # warm-up (autotuner, workspace)
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = ctx.fw_batched(graphs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    ctx.profile(True)
+    ctx.profile_reset()
+    ctx.fw_batched(graphs)
+    k_launches, k_ms = ctx.kernel_time("k_fw_batch")
+    ctx.profile(False)
+    sizes = np.array([b.shape[1] for b in series], np.float64)
+    padded = np.ceil(sizes / 64.0) * 64.0
+    updates = float(np.sum(sizes ** 3))
+    t = float(np.median(ms))
+    for g in graphs:
+        g.free()
+    return {"graphs": ROI_GRAPHS, "n_range": list(ROI_N), "T": ROI_T, "ms_fw_onnela_call": t,
+            "ms_kernel": k_ms / max(1, k_launches), "kernel": "k_fw_batch",
+            "graphs_per_s": ROI_GRAPHS / (t / 1000.0), "useful_updates": updates,
+            "padded_updates": float(np.sum(padded ** 3)),
+            "fp32_ops_per_s_tera": 2.0 * updates / (k_ms / max(1, k_launches) / 1000.0) / 1e12,
+            "frac_of_nominal_fp32": 2.0 * updates / (k_ms / max(1, k_launches) / 1000.0) / 1e12
+            / FP32_SIMT_NOMINAL_TFLOPS,
+            "s_graph_builds": build_s, "lp_mean": float(np.mean([o[1] for o in out])),
+            "cp_mean": float(np.mean([o[3] for o in out]))}
+
+
 # ------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -268,6 +450,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-leg", action="store_true")
     ap.add_argument("--no-cohort", action="store_true", help="skip the subject-average figure")
+    ap.add_argument("--cohort-subjects", type=int, default=3,
+                    help="subjects of the cohort configuration timed beside the step (0: skip)")
+    ap.add_argument("--no-precision-report", action="store_true")
+    ap.add_argument("--no-roi-batch", action="store_true", help="skip the 512-graph weighted batch figure")
     ap.add_argument("--voxels", type=int, default=N_VOX,
                     help="profiling aid: a smaller subject for ncu captures (the metric is quoted at 58000)")
     args = ap.parse_args()
@@ -323,7 +509,8 @@ def run(args):
         if timings is not None:
             torch.cuda.synchronize()
             timings.append({"bc_ms": ev[0].elapsed_time(ev[1]), "newman_ms": ev[1].elapsed_time(ev[2]),
-                            "build": info, "nnz": g.info[1], "lp": lp, "Q": Q, "modules": nmod})
+                            "build": info, "nnz": g.info[1], "lp": lp, "Q": Q, "modules": nmod,
+                            "bc64": bc64, "labels": labels})
         g.free()
 
     def timed(precision, on_device, steps, warmup, timings=None, prof=None):
@@ -421,6 +608,10 @@ def run(args):
     value = world * 60000.0 / ms_dev
     e2e = world * 60000.0 / ms_e2e
     tm = timings[-1]
+    prec_rep = None if args.no_precision_report else precision_report(ctx, bold_dev, tm)
+    build = build_stage(ctx, bold_dev, stream, hbm_peak, bf16_peak)
+    cohort5 = cohort_leg(ctx, args.cohort_subjects, rank) if args.cohort_subjects > 0 else None
+    roi = None if args.no_roi_batch else roi_batch_leg(ctx, stream)
     nnz = tm["nnz"]
     # roofline of the dominant kernel, k_brandes (the gather sweeps of every
     # 128-source batch: level 1, the levels after the tensor-core ones and the
@@ -476,6 +667,10 @@ def run(args):
         "step_ms_all": all_ms,
         "eigen_centrality": eigen,
         "subject_average": cohort,
+        "precision_report": prec_rep,
+        "build_stage": build,
+        "cohort": cohort5,
+        "roi_batch": roi,
         "clocks": clk,
     }
     if fp32:

@@ -66,6 +66,13 @@ int64_t     pg_launch_count(const pg_ctx* ctx);
 pg_status   pg_profile_enable(pg_ctx* ctx, int32_t on);
 pg_status   pg_profile_reset(pg_ctx* ctx);
 pg_status   pg_profile_get(pg_ctx* ctx, const char* kernel, int64_t* launches, double* ms);
+/* Failure-path test hook (no counterpart in the reference): the next
+ * split-BF16 tensor-core Gram launch of this context makes its TMA producer
+ * wait wait_ns on a barrier that nothing arrives on, before it issues any
+ * copy; the wait runs out, every warp of the kernel gives up, TMEM is freed
+ * and the call (pg_build_graph) returns PG_ERR_TIMEOUT.  The context stays
+ * usable.  Applies to one launch; 0 clears it. */
+pg_status   pg_debug_stall_next_gram(pg_ctx* ctx, uint64_t wait_ns);
 
 /* ------------------------------------------------------------- graphs */
 /* Replaces the .csr reads of every metric tool (e.g. U/Cp/Cp/Cp_main.cpp:107-116,

@@ -185,6 +185,13 @@ extern "C" pg_status pg_profile_get(pg_ctx* ctx, const char* kernel, int64_t* la
 }
 extern "C" int64_t pg_launch_count(const pg_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+extern "C" pg_status pg_debug_stall_next_gram(pg_ctx* ctx, uint64_t wait_ns)
+{
+    if (!ctx) return PG_ERR_INVALID;
+    ctx->debug_gram_stall_ns = wait_ns;
+    return PG_OK;
+}
+
 // --------------------------------------------------------------- workspace
 pg_status pg_ws(pg_ctx* ctx, const char* key, size_t bytes, void** out)
 {

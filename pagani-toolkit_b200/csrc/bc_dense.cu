@@ -71,10 +71,7 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, u64 a, u64 b, uint32_t 
         ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC_I8), "r"(acc));
 }
 
-__device__ __forceinline__ void mbar_arrive(u64* b)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
+
 
 struct DArgs {
     int n, d;

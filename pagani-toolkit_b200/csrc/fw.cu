@@ -1,22 +1,47 @@
 // fw.cu -- weighted path length by blocked Floyd-Warshall in FP32 min-plus
 // (CUBFW_Lp, W/Lp/CUBFW_Lp/CUBFW_Lp/CUBFW_Lp.cpp:13-162; phases of cuAPSP,
-// CUBFW.cpp:19-168 and BFW_C, BFW.cpp:40-109) for one graph or a batch of
-// graphs in grouped launches.
+// CUBFW.cpp:19-168, CUBFW_ph1/2/3.cu, and BFW_C, BFW.cpp:40-109) and Onnela
+// weighted clustering (Cp_2, W/Cp/Cp/Cp_2.cpp:23-130) for one graph or a
+// batch of graphs in ONE persistent cooperative launch.
 //
-// Every graph's dense distance matrix stays in HBM for the whole sweep
-// (the reference streamed 3072^2 blocks over PCIe per phase).  Matrices are
-// padded to a multiple of the 32x32 block; block k of every graph is
-// processed by the same three launches (diagonal block, its row and column
-// panels, the rest), so a batch of 512 graphs needs 3 launches per k step.
+// Every graph's dense distance matrix (padded to a multiple of 64) stays in
+// HBM for the whole sweep (the reference streams 3072^2 blocks over PCIe per
+// phase and pads every graph to 3072).  The launch runs, with grid-wide
+// barriers between them:
+//   A  matrices set to +inf (0 on the diagonal); the weight maximum of every
+//      graph (the Onnela normalisation);
+//   B  edge distances 1/w; Onnela clustering of every node of every graph
+//      (one CTA per node, dynamic scheduler, neighbour bitmap in shared
+//      memory);
+//   then for every 64-wide k-block round kb, over all graphs with more than
+//   kb blocks at once (graphs are sorted by block count, so the active ones
+//   are a prefix of the order):
+//   1  closure of the diagonal block in shared memory, 64 steps, one barrier
+//      per step (row and column k are fixed during step k: d_kk = 0);
+//   2  the row and column panels against the closed diagonal block, in
+//      place, likewise;
+//   3  every other block: d_ij = min(d_ij, d_i,kb (x) d_kb,j) as a register-
+//      tiled min-plus product -- 4 x 4 outputs per thread, the kb column
+//      block transposed into shared memory so both operands are 16-byte
+//      vector loads, no barrier inside the k loop (the reference's phase 3
+//      keeps 6 x 6 per thread with scalar shared loads, CUBFW_ph3.cu:32-222);
+//   C  per-row sums of 1/d (CUBFW_Lp.cpp:77-104), then per graph Lp and the
+//      mean clustering.
+// The k-block width is fixed (64), so the distances do not depend on any
+// tuning; the autotuner only picks the CTAs per SM.
 #include "pg_internal.cuh"
-#include <cmath>
+#include "tune.cuh"
 #include <algorithm>
+#include <cmath>
+#include <cooperative_groups.h>
+#include <numeric>
 
-pg_status pg_onnela_table(pg_ctx* ctx, const pg_graph* const* graphs, int ng, int first_n, float* cp_dev,
-                          double* mean_dev);
+namespace cg = cooperative_groups;
 
 namespace {
-constexpr int B = 32;
+constexpr int B = 64;           // k-block width
+constexpr int FW_THREADS = 256; // 16 x 16 threads, 4 x 4 outputs each
+constexpr int BMAX_BITS = 16384;// largest graph of a batch for the Onnela bitmap (n bits)
 
 struct FWGraph {
     const int32_t* R;
@@ -27,137 +52,319 @@ struct FWGraph {
     int32_t node0;      // offset of its nodes in concatenated outputs
 };
 
-__global__ void k_fw_fill(const FWGraph* __restrict__ gs, int ng, float* __restrict__ D)
-{
-    const FWGraph g = gs[blockIdx.y];
-    const long long tot = (long long)g.np * g.np;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-        long long i = q / g.np, j = q % g.np;
-        D[g.off + q] = (i == j) ? 0.0f : INFINITY;
-    }
-}
-
-// Edge distances 1/w (init_block, FormBlock.cpp:64); diagonal stays 0.
-__global__ void k_fw_edges(const FWGraph* __restrict__ gs, int ng, float* __restrict__ D)
-{
-    const FWGraph g = gs[blockIdx.y];
-    for (int i = blockIdx.x; i < g.n; i += gridDim.x)
-        for (int32_t q = g.R[i] + threadIdx.x; q < g.R[i + 1]; q += blockDim.x) {
-            int j = g.C[q];
-            if (j == i) continue;
-            float d = g.V ? __fdiv_rn(1.0f, g.V[q]) : 1.0f;
-            D[g.off + (long long)i * g.np + j] = d;
-        }
-}
+struct FwBatch {
+    const FWGraph* gs;          // in processing order (blocks per side descending)
+    int ng;
+    int total_nodes;
+    int max_nb;
+    const int* active;          // [kb]: graphs with more than kb blocks (a prefix of gs)
+    const long long* p2;        // prefix over gs of 2 (nb - 1): panel tasks
+    const long long* p3;        // prefix over gs of (nb - 1)^2: phase-3 tasks
+    const int* node_graph;      // concatenated node -> index in gs
+    float* D;
+    float* vmax;
+    int* onnela_next;           // dynamic node scheduler
+    int onnela;                 // compute the clustering
+    double* rowsum;             // per node
+    float* eff;                 // per node
+    double* lp;                 // per graph (in gs order)
+    float* cp;                  // per node
+    double* cp_mean;            // per graph (in gs order)
+};
 
 __device__ __forceinline__ float* blk(float* D, const FWGraph& g, int bi, int bj)
 {
     return D + g.off + (long long)bi * B * g.np + (long long)bj * B;
 }
 
-// Phase 1: closure of the diagonal block kb.
-__global__ void k_fw_ph1(const FWGraph* __restrict__ gs, float* __restrict__ D, int kb)
+// graph of task t in a prefix array of `count` graphs
+__device__ __forceinline__ int task_graph(const long long* pre, int count, long long t)
 {
-    const FWGraph g = gs[blockIdx.y];
-    if (kb >= g.nb) return;
-    __shared__ float s[B][B + 1];
-    const int ty = threadIdx.y, tx = threadIdx.x;
-    float* p = blk(D, g, kb, kb);
-    s[ty][tx] = p[(long long)ty * g.np + tx];
-    __syncthreads();
-    for (int k = 0; k < B; k++) {
-        float c = s[ty][k] + s[k][tx];
-        __syncthreads();
-        if (c < s[ty][tx]) s[ty][tx] = c;
-        __syncthreads();
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= t) lo = mid; else hi = mid - 1;
     }
-    p[(long long)ty * g.np + tx] = s[ty][tx];
+    return lo;
 }
 
-// Phase 2: row panel (kb, j) and column panel (i, kb) against the closed
-// diagonal block, in place inside the panel block as BFW_one_block_C does.
-__global__ void k_fw_ph2(const FWGraph* __restrict__ gs, float* __restrict__ D, int kb)
+// Onnela for node x of the batch (W/Cp/Cp/Cp_2.cpp:23-130, GPU weight maximum
+// over all edges): sum over connected neighbour pairs j < h of
+// (w_jh w_uj w_uh)^(1/3), w = V / vmax (float division); the weight of (u, h)
+// by binary search in u's sorted row.
+__device__ void onnela_node(const FwBatch& p, int x, unsigned* bm, double* red)
 {
-    const FWGraph g = gs[blockIdx.y];
-    if (kb >= g.nb) return;
-    int idx = blockIdx.x;
-    if (idx >= 2 * (g.nb - 1)) return;
-    const bool row = idx < g.nb - 1;
-    int other = row ? idx : idx - (g.nb - 1);
-    if (other >= kb) other++;
-    __shared__ float dg[B][B + 1];
-    __shared__ float s[B][B + 1];
-    const int ty = threadIdx.y, tx = threadIdx.x;
-    float* pd = blk(D, g, kb, kb);
-    float* p = row ? blk(D, g, kb, other) : blk(D, g, other, kb);
-    dg[ty][tx] = pd[(long long)ty * g.np + tx];
-    s[ty][tx] = p[(long long)ty * g.np + tx];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = FW_THREADS / 32;
+    const int gi = p.node_graph[x];
+    const FWGraph g = p.gs[gi];
+    const int u = x - g.node0;
+    const int32_t s = g.R[u], e = g.R[u + 1];
+    const int k = e - s;
+    const float vm = p.vmax[gi];
+    const int W = (g.n + 31) >> 5;
+    for (int w = threadIdx.x; w < W; w += FW_THREADS) bm[w] = 0u;
     __syncthreads();
-    for (int k = 0; k < B; k++) {
-        float c = row ? dg[ty][k] + s[k][tx] : s[ty][k] + dg[k][tx];
+    double acc = 0.0;
+    if (k >= 2) {
+        for (int32_t q = s + threadIdx.x; q < e; q += FW_THREADS) atomicOr(&bm[g.C[q] >> 5], 1u << (g.C[q] & 31));
         __syncthreads();
-        if (c < s[ty][tx]) s[ty][tx] = c;
-        __syncthreads();
-    }
-    p[(long long)ty * g.np + tx] = s[ty][tx];
-}
-
-// Phase 3: every other block (i, j) = min(d_ij, d_i,kb (x) d_kb,j).
-__global__ void k_fw_ph3(const FWGraph* __restrict__ gs, float* __restrict__ D, int kb)
-{
-    const FWGraph g = gs[blockIdx.y];
-    if (kb >= g.nb) return;
-    const int m = g.nb - 1;
-    int idx = blockIdx.x;
-    if (idx >= m * m) return;
-    int bi = idx / m, bj = idx % m;
-    if (bi >= kb) bi++;
-    if (bj >= kb) bj++;
-    __shared__ float a[B][B + 1];
-    __shared__ float b[B][B + 1];
-    const int ty = threadIdx.y, tx = threadIdx.x;
-    a[ty][tx] = blk(D, g, bi, kb)[(long long)ty * g.np + tx];
-    b[ty][tx] = blk(D, g, kb, bj)[(long long)ty * g.np + tx];
-    __syncthreads();
-    float* p = blk(D, g, bi, bj) + (long long)ty * g.np + tx;
-    float cur = *p;
-#pragma unroll
-    for (int k = 0; k < B; k++) cur = fminf(cur, a[ty][k] + b[k][tx]);
-    *p = cur;
-}
-
-// Row sums of 1/d over finite, non-tiny distances (CUBFW_Lp.cpp:77-83,99-104).
-__global__ void k_fw_rows(const FWGraph* __restrict__ gs, int ng, const float* __restrict__ D,
-                          double* __restrict__ rowsum, float* __restrict__ eff)
-{
-    const FWGraph g = gs[blockIdx.y];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int u = blockIdx.x * nw + w; u < g.n; u += gridDim.x * nw) {
-        const float* row = D + g.off + (long long)u * g.np;
-        double acc = 0.0;
-        for (int v = lane; v < g.n; v += 32) {
-            float x = row[v];
-            if (v == u || !(x >= 0.1f)) continue;
-            acc += 1.0 / (double)x;
-        }
-        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) {
-            rowsum[g.node0 + u] = acc;
-            float e = g.n > 1 ? (float)(acc / (double)(g.n - 1)) : 0.0f;
-            if (e < 1.0f / (float)g.n) e = 0.0f;
-            eff[g.node0 + u] = e;
+        for (int32_t q = s + warp; q < e; q += nwarp) {
+            const int j = g.C[q];
+            const double wuj = (double)__fdiv_rn(g.V[q], vm);
+            for (int32_t f = g.R[j] + lane; f < g.R[j + 1]; f += 32) {
+                const int h = g.C[f];
+                if (h <= j || !((bm[h >> 5] >> (h & 31)) & 1u)) continue;
+                const float wjh = __fdiv_rn(g.V[f], vm);
+                if (wjh == 0.0f) continue;
+                int32_t lo = s, hi = e - 1;
+                while (lo < hi) {
+                    const int32_t mid = (lo + hi) >> 1;
+                    if (g.C[mid] < h) lo = mid + 1; else hi = mid;
+                }
+                const double wuh = (double)__fdiv_rn(g.V[lo], vm);
+                acc += pow((double)wjh * wuj * wuh, 1.0 / 3.0);
+            }
         }
     }
-}
-
-__global__ void k_fw_lp(const FWGraph* __restrict__ gs, int ng, const double* __restrict__ rowsum,
-                        double* __restrict__ lp)
-{
-    for (int gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ng; gi += gridDim.x * blockDim.x) {
-        const FWGraph g = gs[gi];
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int u = 0; u < g.n; u++) t += rowsum[g.node0 + u];
-        lp[gi] = t > 0.0 ? 1.0 / (t / g.n / (g.n - 1)) : INFINITY;
+        for (int w = 0; w < nwarp; w++) t += red[w];
+        p.cp[x] = k >= 2 ? (float)(2.0 * t / k / (k - 1)) : 0.0f;
+    }
+    __syncthreads();
+}
+
+// Closure of a 64 x 64 block in shared memory against the diagonal block dg
+// (which may be the block itself): mode 0 diagonal, 1 row panel
+// (s = min(s, dg (x) s)), 2 column panel (s = min(s, s (x) dg)).
+__device__ __forceinline__ void panel_steps(float (*s)[B + 1], float (*dg)[B + 1], int mode)
+{
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+    for (int k = 0; k < B; k++) {
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const int i = ty * 4 + a;
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const int j = tx * 4 + b;
+                const float c = mode == 1 ? dg[i][k] + s[k][j] : (mode == 2 ? s[i][k] + dg[k][j] : s[i][k] + s[k][j]);
+                s[i][j] = fminf(s[i][j], c);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void load_block(float (*s)[B + 1], const float* src, int ld)
+{
+    for (int q = threadIdx.x; q < B * B / 4; q += FW_THREADS) {
+        const int i = q / (B / 4), j4 = (q % (B / 4)) * 4;
+        const float4 v = *(const float4*)(src + (long long)i * ld + j4);
+        s[i][j4] = v.x; s[i][j4 + 1] = v.y; s[i][j4 + 2] = v.z; s[i][j4 + 3] = v.w;
+    }
+}
+
+__device__ __forceinline__ void store_block(float* dst, int ld, float (*s)[B + 1])
+{
+    for (int q = threadIdx.x; q < B * B / 4; q += FW_THREADS) {
+        const int i = q / (B / 4), j4 = (q % (B / 4)) * 4;
+        *(float4*)(dst + (long long)i * ld + j4) = make_float4(s[i][j4], s[i][j4 + 1], s[i][j4 + 2], s[i][j4 + 3]);
+    }
+}
+
+struct __align__(16) FwSmem {
+    union {
+        struct {
+            float s[B][B + 1];
+            float dg[B][B + 1];
+        } panel;
+        struct {
+            float at[B][B + 4];     // the (bi, kb) block transposed: at[k][i]
+            float bk[B][B + 4];     // the (kb, bj) block: bk[k][j]
+        } prod;
+        unsigned bitmap[BMAX_BITS / 32];
+    };
+    double red[FW_THREADS / 32];
+};
+
+__global__ void __launch_bounds__(FW_THREADS, 2)
+k_fw_batch(FwBatch p)
+{
+    cg::grid_group grid = cg::this_grid();
+    __shared__ FwSmem sm;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    // ---- A: +inf matrices with a zero diagonal; weight maxima
+    for (int gi = 0; gi < p.ng; gi++) {
+        const FWGraph g = p.gs[gi];
+        const long long tot4 = (long long)g.np * g.np / 4;
+        float4* d = (float4*)(p.D + g.off);
+        for (long long q = tid; q < tot4; q += nt) {
+            const long long e = q * 4, i = e / g.np, j = e % g.np;
+            float4 v = make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+            if (i >= j && i < j + 4) ((float*)&v)[i - j] = 0.0f;
+            d[q] = v;
+        }
+    }
+    if (p.onnela) {
+        for (int gi = blockIdx.x; gi < p.ng; gi += gridDim.x) {
+            const FWGraph g = p.gs[gi];
+            const int32_t nnz = g.R[g.n];
+            float m = -INFINITY;
+            for (int32_t q = threadIdx.x; q < nnz; q += FW_THREADS) m = fmaxf(m, g.V[q]);
+            for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            __shared__ float mx[FW_THREADS / 32];
+            if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = m;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                float t = -INFINITY;
+                for (int w = 0; w < FW_THREADS / 32; w++) t = fmaxf(t, mx[w]);
+                p.vmax[gi] = t;
+            }
+            __syncthreads();
+        }
+    }
+    grid.sync();
+    // ---- B: edge distances 1/w (init_block, FormBlock.cpp:64); Onnela
+    for (int gi = 0; gi < p.ng; gi++) {
+        const FWGraph g = p.gs[gi];
+        const long long warps = nt >> 5;
+        for (long long i = tid >> 5; i < g.n; i += warps)
+            for (int32_t q = g.R[i] + (threadIdx.x & 31); q < g.R[i + 1]; q += 32) {
+                const int j = g.C[q];
+                if (j == i) continue;
+                p.D[g.off + i * g.np + j] = g.V ? __fdiv_rn(1.0f, g.V[q]) : 1.0f;
+            }
+    }
+    if (p.onnela) {
+        __shared__ int s_x;
+        for (;;) {
+            if (threadIdx.x == 0) s_x = atomicAdd(p.onnela_next, 1);
+            __syncthreads();
+            const int x = s_x;
+            __syncthreads();
+            if (x >= p.total_nodes) break;
+            onnela_node(p, x, sm.bitmap, sm.red);
+        }
+    }
+    grid.sync();
+    // ---- FW rounds over all graphs with more than kb blocks
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+    for (int kb = 0; kb < p.max_nb; kb++) {
+        const int act = p.active[kb];
+        // 1: diagonal blocks
+        for (int gi = blockIdx.x; gi < act; gi += gridDim.x) {
+            const FWGraph g = p.gs[gi];
+            float* d = blk(p.D, g, kb, kb);
+            load_block(sm.panel.s, d, g.np);
+            __syncthreads();
+            panel_steps(sm.panel.s, sm.panel.s, 0);
+            store_block(d, g.np, sm.panel.s);
+            __syncthreads();
+        }
+        grid.sync();
+        // 2: row and column panels
+        const long long n2 = p.p2[act];
+        for (long long t = blockIdx.x; t < n2; t += gridDim.x) {
+            const int gi = task_graph(p.p2, act, t);
+            const FWGraph g = p.gs[gi];
+            const int local = (int)(t - p.p2[gi]);
+            const bool row = local < g.nb - 1;
+            int other = row ? local : local - (g.nb - 1);
+            if (other >= kb) other++;
+            float* d = row ? blk(p.D, g, kb, other) : blk(p.D, g, other, kb);
+            load_block(sm.panel.dg, blk(p.D, g, kb, kb), g.np);
+            load_block(sm.panel.s, d, g.np);
+            __syncthreads();
+            panel_steps(sm.panel.s, sm.panel.dg, row ? 1 : 2);
+            store_block(d, g.np, sm.panel.s);
+            __syncthreads();
+        }
+        grid.sync();
+        // 3: the other blocks, register-tiled min-plus
+        const long long n3 = p.p3[act];
+        for (long long t = blockIdx.x; t < n3; t += gridDim.x) {
+            const int gi = task_graph(p.p3, act, t);
+            const FWGraph g = p.gs[gi];
+            const int m = g.nb - 1;
+            const int local = (int)(t - p.p3[gi]);
+            int bi = local / m, bj = local % m;
+            if (bi >= kb) bi++;
+            if (bj >= kb) bj++;
+            const float* a = blk(p.D, g, bi, kb);
+            const float* b = blk(p.D, g, kb, bj);
+            for (int q = threadIdx.x; q < B * B / 4; q += FW_THREADS) {
+                const int i = q / (B / 4), j4 = (q % (B / 4)) * 4;
+                const float4 va = *(const float4*)(a + (long long)i * g.np + j4);
+                sm.prod.at[j4][i] = va.x; sm.prod.at[j4 + 1][i] = va.y;
+                sm.prod.at[j4 + 2][i] = va.z; sm.prod.at[j4 + 3][i] = va.w;
+                *(float4*)&sm.prod.bk[i][j4] = *(const float4*)(b + (long long)i * g.np + j4);
+            }
+            float* c = blk(p.D, g, bi, bj);
+            float acc[4][4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const float4 v = *(const float4*)(c + (long long)(ty * 4 + r) * g.np + tx * 4);
+                acc[r][0] = v.x; acc[r][1] = v.y; acc[r][2] = v.z; acc[r][3] = v.w;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int k = 0; k < B; k++) {
+                const float4 ai = *(const float4*)&sm.prod.at[k][ty * 4];
+                const float4 bj4 = *(const float4*)&sm.prod.bk[k][tx * 4];
+                const float av[4] = {ai.x, ai.y, ai.z, ai.w};
+                const float bv[4] = {bj4.x, bj4.y, bj4.z, bj4.w};
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[r][q] = fminf(acc[r][q], av[r] + bv[q]);
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                *(float4*)(c + (long long)(ty * 4 + r) * g.np + tx * 4) =
+                    make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+            __syncthreads();
+        }
+        grid.sync();
+    }
+    // ---- C: row sums of 1/d over finite, non-tiny distances (CUBFW_Lp.cpp:77-83,99-104)
+    {
+        const int lane = threadIdx.x & 31;
+        const long long warps = nt >> 5;
+        for (long long x = tid >> 5; x < p.total_nodes; x += warps) {
+            const int gi = p.node_graph[x];
+            const FWGraph g = p.gs[gi];
+            const int u = (int)x - g.node0;
+            const float* row = p.D + g.off + (long long)u * g.np;
+            double acc = 0.0;
+            for (int v = lane; v < g.n; v += 32) {
+                const float d = row[v];
+                if (v == u || !(d >= 0.1f)) continue;
+                acc += 1.0 / (double)d;
+            }
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) {
+                p.rowsum[x] = acc;
+                float e = g.n > 1 ? (float)(acc / (double)(g.n - 1)) : 0.0f;
+                if (e < 1.0f / (float)g.n) e = 0.0f;
+                p.eff[x] = e;
+            }
+        }
+    }
+    grid.sync();
+    for (long long gi = tid; gi < p.ng; gi += nt) {
+        const FWGraph g = p.gs[gi];
+        double t = 0.0;
+        for (int u = 0; u < g.n; u++) t += p.rowsum[g.node0 + u];
+        p.lp[gi] = t > 0.0 ? 1.0 / (t / g.n / (g.n - 1)) : INFINITY;
+        if (p.onnela) {
+            double c = 0.0;
+            for (int u = 0; u < g.n; u++) c += (double)p.cp[g.node0 + u];
+            p.cp_mean[gi] = g.n > 0 ? c / g.n : 0.0;
+        }
     }
 }
 
@@ -168,53 +375,162 @@ __global__ void k_fw_copy_out(const FWGraph* __restrict__ gs, const float* __res
          q += (long long)gridDim.x * blockDim.x)
         out[q] = D[g.off + (q / g.n) * g.np + q % g.n];
 }
-}  // namespace
 
-static pg_status fw_run(pg_ctx* ctx, const pg_graph* const* graphs, int ng, float* eff_dev, double* lp_dev,
-                        float** dist_dev_out, FWGraph** tab_out)
+// outputs in processing order -> caller's order
+__global__ void k_fw_unpermute(const int* __restrict__ perm, const FWGraph* __restrict__ gs, int ng,
+                               const int* __restrict__ node0_out, const float* __restrict__ eff,
+                               const double* __restrict__ lp, const float* __restrict__ cp,
+                               const double* __restrict__ cpm, float* __restrict__ eff_o, double* __restrict__ lp_o,
+                               float* __restrict__ cp_o, double* __restrict__ cpm_o, int onnela)
 {
-    std::vector<FWGraph> tab(ng);
-    long long off = 0;
-    int node0 = 0, nbmax = 0;
-    for (int i = 0; i < ng; i++) {
-        const pg_graph* g = graphs[i];
-        int np = std::max(B, (g->n + B - 1) / B * B);
-        tab[i] = {g->R, g->C, g->V, g->n, np, np / B, off, node0};
-        off += (long long)np * np;
-        node0 += g->n;
-        nbmax = std::max(nbmax, np / B);
-    }
-    float* D;
-    FWGraph* dtab;
-    double* rowsum;
-    PG_TRY(pg_wst(ctx, "fw.D", (size_t)off, &D));
-    PG_TRY(pg_wst(ctx, "fw.tab", (size_t)ng, &dtab));
-    PG_TRY(pg_wst(ctx, "fw.rows", (size_t)node0 + 1, &rowsum));
-    PG_CUDA(ctx, cudaMemcpyAsync(dtab, tab.data(), sizeof(FWGraph) * ng, cudaMemcpyHostToDevice, ctx->stream));
-    // grid.y carries the graph index (at most 65535 graphs per launch)
-    if (ng > 65535) return pg_fail(ctx, PG_ERR_INVALID, "at most 65535 graphs per batch");
-    k_fw_fill<<<dim3(64, ng), 256, 0, ctx->stream>>>(dtab, ng, D);
-    PG_LAUNCHED(ctx);
-    k_fw_edges<<<dim3(256, ng), 128, 0, ctx->stream>>>(dtab, ng, D);
-    PG_LAUNCHED(ctx);
-    for (int kb = 0; kb < nbmax; kb++) {
-        k_fw_ph1<<<dim3(1, ng), dim3(B, B), 0, ctx->stream>>>(dtab, D, kb);
-        PG_LAUNCHED(ctx);
-        if (nbmax > 1) {
-            k_fw_ph2<<<dim3(2 * (nbmax - 1), ng), dim3(B, B), 0, ctx->stream>>>(dtab, D, kb);
-            PG_LAUNCHED(ctx);
-            k_fw_ph3<<<dim3((nbmax - 1) * (nbmax - 1), ng), dim3(B, B), 0, ctx->stream>>>(dtab, D, kb);
-            PG_LAUNCHED(ctx);
+    for (int gi = blockIdx.x; gi < ng; gi += gridDim.x) {
+        const FWGraph g = gs[gi];
+        const int dst = perm[gi];
+        const int o = node0_out[dst];
+        for (int u = threadIdx.x; u < g.n; u += blockDim.x) {
+            eff_o[o + u] = eff[g.node0 + u];
+            if (onnela) cp_o[o + u] = cp[g.node0 + u];
+        }
+        if (threadIdx.x == 0) {
+            lp_o[dst] = lp[gi];
+            if (onnela) cpm_o[dst] = cpm[gi];
         }
     }
-    k_fw_rows<<<dim3(std::max(1, std::min(1024, ceil_div(tab.empty() ? 1 : 1024, 8))), ng), 256, 0, ctx->stream>>>(
-        dtab, ng, D, rowsum, eff_dev);
+}
+}  // namespace
+
+// Graph table in processing order and the device batch description.
+struct FwPlan {
+    FwBatch b;
+    FWGraph* dtab;
+    int* perm;          // processing index -> caller's index
+    int* node0_out;     // caller's node offsets
+    long long total;
+    int grid;
+};
+
+static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, bool onnela, FwPlan* P)
+{
+    std::vector<int> order(ng);
+    std::iota(order.begin(), order.end(), 0);
+    auto nb_of = [&](int i) { return std::max(1, (graphs[i]->n + B - 1) / B); };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nb_of(x) > nb_of(y); });
+    std::vector<FWGraph> tab(ng);
+    std::vector<long long> p2(ng + 1, 0), p3(ng + 1, 0);
+    std::vector<int> perm(ng), node0_out(ng), node_graph;
+    long long off = 0;
+    int node0 = 0, nmax = 1, max_nb = 0;
+    int o = 0;
+    for (int i = 0; i < ng; i++) {
+        node0_out[i] = o;
+        o += graphs[i]->n;
+    }
+    for (int q = 0; q < ng; q++) {
+        const pg_graph* g = graphs[order[q]];
+        if (onnela && !g->V) return pg_fail(ctx, PG_ERR_INVALID, "Onnela clustering needs a weighted graph");
+        const int nb = nb_of(order[q]);
+        tab[q] = {g->R, g->C, g->V, g->n, nb * B, nb, off, node0};
+        perm[q] = order[q];
+        off += (long long)nb * B * nb * B;
+        for (int u = 0; u < g->n; u++) node_graph.push_back(q);
+        node0 += g->n;
+        nmax = std::max(nmax, (int)g->n);
+        max_nb = std::max(max_nb, nb);
+        p2[q + 1] = p2[q] + 2LL * (nb - 1);
+        p3[q + 1] = p3[q] + (long long)(nb - 1) * (nb - 1);
+    }
+    if (onnela && nmax > BMAX_BITS)
+        return pg_fail(ctx, PG_ERR_TOO_LARGE, "Onnela in the batched launch: n=%d above %d", nmax, BMAX_BITS);
+    std::vector<int> active(max_nb);
+    for (int kb = 0; kb < max_nb; kb++) {
+        int a = 0;
+        while (a < ng && tab[a].nb > kb) a++;
+        active[kb] = a;
+    }
+    FwBatch& b = P->b;
+    memset(&b, 0, sizeof b);
+    int *dact, *dng, *dperm, *dn0;
+    long long *dp2, *dp3;
+    PG_TRY(pg_wst(ctx, "fw.D", (size_t)off, &b.D));
+    PG_TRY(pg_wst(ctx, "fw.tab", (size_t)ng, &P->dtab));
+    PG_TRY(pg_wst(ctx, "fw.active", (size_t)max_nb, &dact));
+    PG_TRY(pg_wst(ctx, "fw.p2", (size_t)ng + 1, &dp2));
+    PG_TRY(pg_wst(ctx, "fw.p3", (size_t)ng + 1, &dp3));
+    PG_TRY(pg_wst(ctx, "fw.ngraph", (size_t)node0 + 1, &dng));
+    PG_TRY(pg_wst(ctx, "fw.perm", (size_t)ng, &dperm));
+    PG_TRY(pg_wst(ctx, "fw.node0o", (size_t)ng, &dn0));
+    PG_TRY(pg_wst(ctx, "fw.vmax", (size_t)ng, &b.vmax));
+    PG_TRY(pg_wst(ctx, "fw.next", 1, &b.onnela_next));
+    PG_TRY(pg_wst(ctx, "fw.rows", (size_t)node0 + 1, &b.rowsum));
+    PG_TRY(pg_wst(ctx, "fw.eff", (size_t)node0 + 1, &b.eff));
+    PG_TRY(pg_wst(ctx, "fw.lp", (size_t)ng, &b.lp));
+    PG_TRY(pg_wst(ctx, "fw.cp", (size_t)node0 + 1, &b.cp));
+    PG_TRY(pg_wst(ctx, "fw.cpm", (size_t)ng, &b.cp_mean));
+    PG_CUDA(ctx, cudaMemcpyAsync(P->dtab, tab.data(), sizeof(FWGraph) * ng, cudaMemcpyHostToDevice, ctx->stream));
+    PG_CUDA(ctx, cudaMemcpyAsync(dact, active.data(), sizeof(int) * max_nb, cudaMemcpyHostToDevice, ctx->stream));
+    PG_CUDA(ctx, cudaMemcpyAsync(dp2, p2.data(), sizeof(long long) * (ng + 1), cudaMemcpyHostToDevice, ctx->stream));
+    PG_CUDA(ctx, cudaMemcpyAsync(dp3, p3.data(), sizeof(long long) * (ng + 1), cudaMemcpyHostToDevice, ctx->stream));
+    if (node0 > 0)
+        PG_CUDA(ctx, cudaMemcpyAsync(dng, node_graph.data(), sizeof(int) * node0, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    PG_CUDA(ctx, cudaMemcpyAsync(dperm, perm.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, ctx->stream));
+    PG_CUDA(ctx, cudaMemcpyAsync(dn0, node0_out.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, ctx->stream));
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // host tables' lifetime
+    b.gs = P->dtab;
+    b.ng = ng;
+    b.total_nodes = node0;
+    b.max_nb = max_nb;
+    b.active = dact;
+    b.p2 = dp2;
+    b.p3 = dp3;
+    b.node_graph = dng;
+    b.onnela = onnela;
+    P->perm = dperm;
+    P->node0_out = dn0;
+    P->total = node0;
+    int per_sm = 0;
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fw_batch, FW_THREADS, 0));
+    if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "FW: kernel does not fit an SM");
+    std::vector<TuneChoice> cands;
+    for (int c = 1; c <= std::min(per_sm, 4); c++) cands.push_back({c, 0});
+    TuneChoice best{std::min(per_sm, 2), 0};
+    const std::string key = tune_key("fw_batch", off > 0 ? (long long)std::sqrt((double)off / ng) : 0, ng);
+    PG_TRY(tune_pick(ctx, key, cands, &best, [&](const TuneChoice& c) -> pg_status {
+        P->grid = ctx->sm_count * c.a;
+        PG_CUDA(ctx, cudaMemsetAsync(b.onnela_next, 0, sizeof(int), ctx->stream));
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeCooperative;
+        attr.val.cooperative = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(P->grid);
+        cfg.blockDim = dim3(FW_THREADS);
+        cfg.stream = ctx->stream;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_fw_batch, b));
+        PG_LAUNCHED(ctx);
+        return PG_OK;
+    }));
+    P->grid = ctx->sm_count * best.a;
+    return PG_OK;
+}
+
+static pg_status fw_launch(pg_ctx* ctx, FwPlan* P)
+{
+    PG_CUDA(ctx, cudaMemsetAsync(P->b.onnela_next, 0, sizeof(int), ctx->stream));
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeCooperative;
+    attr.val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P->grid);
+    cfg.blockDim = dim3(FW_THREADS);
+    cfg.stream = ctx->stream;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    const int h = pg_prof_begin(ctx, "k_fw_batch");
+    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_fw_batch, P->b));
     PG_LAUNCHED(ctx);
-    k_fw_lp<<<ceil_div(ng, 128), 128, 0, ctx->stream>>>(dtab, ng, rowsum, lp_dev);
-    PG_LAUNCHED(ctx);
-    if (dist_dev_out) *dist_dev_out = D;
-    if (tab_out) *tab_out = dtab;
-    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // host table lifetime
+    pg_prof_end(ctx, h);
     return PG_OK;
 }
 
@@ -223,23 +539,19 @@ extern "C" pg_status pg_fw_paths(pg_ctx* ctx, const pg_graph* g, float* dist, fl
     if (!ctx || !g) return pg_fail(ctx, PG_ERR_INVALID, "pg_fw_paths: null argument");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
     const int n = g->n;
-    float* deff;
-    double* dlp;
-    PG_TRY(pg_wst(ctx, "fw.eff", (size_t)n + 1, &deff));
-    PG_TRY(pg_wst(ctx, "fw.lp", 1, &dlp));
     const pg_graph* one[1] = {g};
-    float* D;
-    FWGraph* tab;
-    PG_TRY(fw_run(ctx, one, 1, deff, dlp, &D, &tab));
+    FwPlan P;
+    PG_TRY(fw_plan(ctx, one, 1, false, &P));
+    PG_TRY(fw_launch(ctx, &P));
     if (dist) {
         float* tmp;
         PG_TRY(pg_wst(ctx, "fw.out", (size_t)n * n + 1, &tmp));
-        k_fw_copy_out<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(tab, D, tmp);
+        k_fw_copy_out<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(P.dtab, P.b.D, tmp);
         PG_LAUNCHED(ctx);
         PG_TRY(pg_d2h(ctx, dist, tmp, sizeof(float) * (size_t)n * n));
     }
-    if (eff) PG_TRY(pg_d2h(ctx, eff, deff, sizeof(float) * n));
-    if (lp) PG_TRY(pg_d2h(ctx, lp, dlp, sizeof(double)));
+    if (eff) PG_TRY(pg_d2h(ctx, eff, P.b.eff, sizeof(float) * n));
+    if (lp) PG_TRY(pg_d2h(ctx, lp, P.b.lp, sizeof(double)));
     return PG_OK;
 }
 
@@ -248,24 +560,25 @@ extern "C" pg_status pg_fw_batched(pg_ctx* ctx, const pg_graph* const* graphs, i
 {
     if (!ctx || !graphs || count < 1) return pg_fail(ctx, PG_ERR_INVALID, "pg_fw_batched: bad arguments");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    long long total = 0;
-    for (int i = 0; i < count; i++) {
+    for (int i = 0; i < count; i++)
         if (!graphs[i]) return pg_fail(ctx, PG_ERR_INVALID, "graph %d is null", i);
-        total += graphs[i]->n;
-    }
+    const bool onnela = cp || cp_mean;
+    FwPlan P;
+    PG_TRY(fw_plan(ctx, graphs, count, onnela, &P));
+    PG_TRY(fw_launch(ctx, &P));
     float *deff, *dcp;
     double *dlp, *dcpm;
-    PG_TRY(pg_wst(ctx, "fwb.eff", (size_t)total + 1, &deff));
+    PG_TRY(pg_wst(ctx, "fwb.eff", (size_t)P.total + 1, &deff));
+    PG_TRY(pg_wst(ctx, "fwb.cp", (size_t)P.total + 1, &dcp));
     PG_TRY(pg_wst(ctx, "fwb.lp", (size_t)count, &dlp));
-    PG_TRY(fw_run(ctx, graphs, count, deff, dlp, nullptr, nullptr));
-    if (cp || cp_mean) {
-        PG_TRY(pg_wst(ctx, "fwb.cp", (size_t)total + 1, &dcp));
-        PG_TRY(pg_wst(ctx, "fwb.cpm", (size_t)count, &dcpm));
-        PG_TRY(pg_onnela_table(ctx, graphs, count, 0, dcp, dcpm));
-        if (cp) PG_TRY(pg_d2h(ctx, cp, dcp, sizeof(float) * total));
-        if (cp_mean) PG_TRY(pg_d2h(ctx, cp_mean, dcpm, sizeof(double) * count));
-    }
-    if (eff) PG_TRY(pg_d2h(ctx, eff, deff, sizeof(float) * total));
+    PG_TRY(pg_wst(ctx, "fwb.cpm", (size_t)count, &dcpm));
+    k_fw_unpermute<<<std::min(count, 4096), 256, 0, ctx->stream>>>(P.perm, P.dtab, count, P.node0_out, P.b.eff, P.b.lp,
+                                                                   P.b.cp, P.b.cp_mean, deff, dlp, dcp, dcpm,
+                                                                   onnela);
+    PG_LAUNCHED(ctx);
+    if (eff) PG_TRY(pg_d2h(ctx, eff, deff, sizeof(float) * P.total));
     if (lp) PG_TRY(pg_d2h(ctx, lp, dlp, sizeof(double) * count));
+    if (cp) PG_TRY(pg_d2h(ctx, cp, dcp, sizeof(float) * P.total));
+    if (cp_mean) PG_TRY(pg_d2h(ctx, cp_mean, dcpm, sizeof(double) * count));
     return PG_OK;
 }

@@ -10,20 +10,22 @@
 // of D against the exact dot product of the rounded z-scores stays below
 // 1e-4, far inside the 2e-3 guard band that the FP64 recheck covers.
 //
-// Structure (one persistent CTA of 4 warps per SM, upper-triangle tiles in
-// row-major order):
-//   - thread 0 streams K in 64-element chunks (128 B rows, 128B swizzle)
-//     with TMA into a 3-stage shared-memory ring (A_hi, A_lo, B_hi, B_lo per
-//     stage) guarded by mbarriers, and issues 12 UMMA instructions
-//     (M=128, N=128, K=16, bf16 x bf16 -> fp32) per chunk; tcgen05.commit
-//     releases each stage and finally signals the accumulator;
-//   - the next tile's first chunks are loaded while all 4 warps run the
-//     epilogue: warp w reads TMEM lanes 32w..32w+31 (rows) with
-//     tcgen05.ld 32x32b.x32, 32 columns at a time, and classifies every
-//     pair (histogram, decided edge, FP64 band) in registers.
-// Every mbarrier wait is bounded by the global timer; on expiry the kernel
-// records an error, drains its own TMA copies (bounded), frees TMEM and
-// returns.
+// Structure: one persistent CTA of 6 warps per SM over the upper-triangle
+// tiles in row-major order, warp-specialised:
+//   - warp 0 (one lane) streams K in 64-element chunks (128 B rows, 128B
+//     swizzle) with TMA into a 3-stage shared-memory ring (A_hi, A_lo, B_hi,
+//     B_lo per stage) guarded by full/empty mbarriers;
+//   - warp 1 (one lane) issues 12 UMMA (M=128, N=128, K=16, bf16 x bf16 ->
+//     fp32) per chunk into one of TWO TMEM accumulators (256 columns), a
+//     tcgen05.commit releasing every stage and, per tile, the accumulator;
+//   - warps 2-5 run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+//     (rows) with tcgen05.ld 32x32b.x32, 32 columns at a time, classifies
+//     every pair (histogram, decided edge, FP64 band) in registers and hands
+//     the accumulator back (4 arrivals), so the next tile's MMAs run while
+//     this tile's epilogue does.
+// Every mbarrier wait is bounded by the global timer and gives up at once
+// when another warp has given up; the kernel then records an error, waits
+// (bounded) for its own MMAs and TMA copies, frees TMEM and returns.
 #include "build_graph.cuh"
 #include "tma.cuh"
 #include <cuda.h>
@@ -32,16 +34,21 @@ namespace {
 using namespace pg_tma;
 constexpr int BM = 128, BN = 128, KC = 64;
 constexpr int STAGES = 3;
-constexpr int THREADS = 128;
+constexpr int WARPS = 6;
+constexpr int THREADS = WARPS * 32;
 constexpr uint32_t TILE_BYTES = BM * KC * 2;       // 16 KB per operand tile
 constexpr uint32_t STAGE_BYTES = 4 * TILE_BYTES;   // A_hi, A_lo, B_hi, B_lo
-constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t ACC_COLS = BN;                  // one FP32 accumulator
+constexpr uint32_t TMEM_COLS = 2 * ACC_COLS;       // double-buffered
 
 struct Ctl {
     unsigned long long full[STAGES];
     unsigned long long empty[STAGES];
-    unsigned long long accbar;
+    unsigned long long tfull[2];
+    unsigned long long tempty[2];
     unsigned long long drainbar;
+    unsigned long long stallbar;   // test hook: nothing ever arrives on it
+    long long issued, consumed;
     uint32_t tmem_base;
     int abort;
 };
@@ -64,12 +71,13 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, unsigned long long a, unsi
 template <int MODE>
 __global__ void __launch_bounds__(THREADS, 1)
 k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo, int nb, int nk,
-          EpiParams p, int* __restrict__ err)
+          EpiParams p, unsigned long long stall_ns, int* __restrict__ err)
 {
     extern __shared__ unsigned char smem_raw[];
     __shared__ unsigned int sh_hist[MODE == EPI_HIST ? HIST_BINS : 1];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     Ctl* ctl = (Ctl*)(smem + STAGES * STAGE_BYTES);
+    volatile int* abort_flag = &ctl->abort;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
 
     if (MODE == EPI_HIST)
@@ -79,8 +87,14 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             mbar_init(&ctl->full[s], 1);
             mbar_init(&ctl->empty[s], 1);
         }
-        mbar_init(&ctl->accbar, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&ctl->tfull[b], 1);
+            mbar_init(&ctl->tempty[b], 4);
+        }
         mbar_init(&ctl->drainbar, 1);
+        mbar_init(&ctl->stallbar, 1);
+        ctl->issued = 0;
+        ctl->consumed = 0;
         ctl->abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -95,80 +109,98 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     const uint32_t tmem = ctl->tmem_base;
 
     const long long nt = (long long)nb * (nb + 1) / 2;
+    const long long first = (long long)blockIdx.x * (MODE == EPI_HIST ? p.tile_stride : 1);
     const long long stride = (MODE == EPI_HIST ? (long long)p.tile_stride : 1LL) * gridDim.x;
     unsigned int below = 0u, neg = 0u;
-    // chunk counters drive the stage ring: issued (loads) and consumed (MMAs)
-    long long issued = 0, consumed = 0;
-    int tiles_done = 0;
 
-    // loads chunk c of tile (bi, bj) into the next ring slot (thread 0 only)
-    auto issue = [&](int bi, int bj, int c) -> bool {
-        const int s = (int)(issued % STAGES);
-        const uint32_t par = (uint32_t)((issued / STAGES) & 1) ^ 1u;
-        if (!mbar_wait(&ctl->empty[s], par)) return false;
-        unsigned char* st = smem + (size_t)s * STAGE_BYTES;
-        mbar_expect_tx(&ctl->full[s], STAGE_BYTES);
-        tma_load(st, &map_hi, c * KC, bi * BM, &ctl->full[s]);
-        tma_load(st + TILE_BYTES, &map_lo, c * KC, bi * BM, &ctl->full[s]);
-        tma_load(st + 2 * TILE_BYTES, &map_hi, c * KC, bj * BN, &ctl->full[s]);
-        tma_load(st + 3 * TILE_BYTES, &map_lo, c * KC, bj * BN, &ctl->full[s]);
-        issued++;
-        return true;
-    };
-
-    long long L = (long long)blockIdx.x * (MODE == EPI_HIST ? p.tile_stride : 1);
-    int bi = 0, bj = 0;
-    if (L < nt) tri_tile(L, nb, bi, bj);
-    // prologue: first chunks of the first tile
-    if (t == 0 && L < nt)
-        for (int c = 0; c < min(nk, STAGES); c++)
-            if (!issue(bi, bj, c)) { ctl->abort = 1; break; }
-    __syncthreads();
-
-    while (L < nt && !ctl->abort) {
-        // ---- MMA (thread 0): all chunks of this tile
-        if (t == 0) {
-            for (int c = 0; c < nk; c++) {
-                const int s = (int)(consumed % STAGES);
-                const uint32_t par = (uint32_t)((consumed / STAGES) & 1);
-                if (!mbar_wait(&ctl->full[s], par)) { ctl->abort = 1; break; }
-                tc_fence_after();
-                unsigned char* st = smem + (size_t)s * STAGE_BYTES;
-                const unsigned long long ahi = sdesc(st), alo = sdesc(st + TILE_BYTES);
-                const unsigned long long bhi = sdesc(st + 2 * TILE_BYTES), blo = sdesc(st + 3 * TILE_BYTES);
-#pragma unroll
-                for (int kk = 0; kk < KC / 16; kk++) {
-                    const unsigned long long o = (unsigned long long)(kk * 32) >> 4;  // 32 B per K=16 step
-                    umma(tmem, ahi + o, bhi + o, (c | kk) != 0);
-                    umma(tmem, ahi + o, blo + o, 1u);
-                    umma(tmem, alo + o, bhi + o, 1u);
+    if (warp == 0) {
+        // ---- TMA producer
+        if (lane == 0) {
+            // failure-path test hook: wait on a barrier nothing arrives on,
+            // before anything is issued
+            if (stall_ns && !mbar_wait_abort(&ctl->stallbar, 0, abort_flag, stall_ns)) *abort_flag = 1;
+            long long q = 0;
+            for (long long L = first; L < nt && !*abort_flag; L += stride) {
+                int bi, bj;
+                tri_tile(L, nb, bi, bj);
+                for (int c = 0; c < nk; c++) {
+                    const int s = (int)(q % STAGES);
+                    if (!mbar_wait_abort(&ctl->empty[s], (uint32_t)((q / STAGES) & 1) ^ 1u, abort_flag)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    unsigned char* st = smem + (size_t)s * STAGE_BYTES;
+                    mbar_expect_tx(&ctl->full[s], STAGE_BYTES);
+                    tma_load(st, &map_hi, c * KC, bi * BM, &ctl->full[s]);
+                    tma_load(st + TILE_BYTES, &map_lo, c * KC, bi * BM, &ctl->full[s]);
+                    tma_load(st + 2 * TILE_BYTES, &map_hi, c * KC, bj * BN, &ctl->full[s]);
+                    tma_load(st + 3 * TILE_BYTES, &map_lo, c * KC, bj * BN, &ctl->full[s]);
+                    q++;
+                    ctl->issued = q;
                 }
-                umma_commit(&ctl->empty[s]);
-                consumed++;
-                if (c + STAGES < nk)
-                    if (!issue(bi, bj, c + STAGES)) { ctl->abort = 1; break; }
             }
-            if (!ctl->abort) umma_commit(&ctl->accbar);
         }
-        __syncthreads();
-        if (ctl->abort) break;
-        // ---- wait for the accumulator, then prefetch the next tile's first chunks
-        const bool ok = mbar_wait(&ctl->accbar, (uint32_t)(tiles_done & 1));
-        if (!ok) ctl->abort = 1;
-        tc_fence_after();
-        const long long Ln = L + stride;
-        int nbi = 0, nbj = 0;
-        if (Ln < nt) tri_tile(Ln, nb, nbi, nbj);
-        if (t == 0 && ok && Ln < nt)
-            for (int c = 0; c < min(nk, STAGES); c++)
-                if (!issue(nbi, nbj, c)) { ctl->abort = 1; break; }
-        // ---- epilogue: rows 32*warp + lane of the tile, 32 columns at a time
-        if (ok) {
-            const int i = bi * BM + warp * 32 + lane;
+    } else if (warp == 1) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            long long q = 0;
+            int tl = 0;
+            for (long long L = first; L < nt && !*abort_flag; L += stride, tl++) {
+                const int buf = tl & 1;
+                if (!mbar_wait_abort(&ctl->tempty[buf], (uint32_t)((tl >> 1) & 1) ^ 1u, abort_flag)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t dst = tmem + (uint32_t)(buf * ACC_COLS);
+                bool ok = true;
+                for (int c = 0; c < nk; c++) {
+                    const int s = (int)(q % STAGES);
+                    if (!mbar_wait_abort(&ctl->full[s], (uint32_t)((q / STAGES) & 1), abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    unsigned char* st = smem + (size_t)s * STAGE_BYTES;
+                    const unsigned long long ahi = sdesc(st), alo = sdesc(st + TILE_BYTES);
+                    const unsigned long long bhi = sdesc(st + 2 * TILE_BYTES), blo = sdesc(st + 3 * TILE_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < KC / 16; kk++) {
+                        const unsigned long long o = (unsigned long long)(kk * 32) >> 4;  // 32 B per K=16 step
+                        umma(dst, ahi + o, bhi + o, (c | kk) != 0);
+                        umma(dst, ahi + o, blo + o, 1u);
+                        umma(dst, alo + o, bhi + o, 1u);
+                    }
+                    umma_commit(&ctl->empty[s]);
+                    q++;
+                    ctl->consumed = q;
+                }
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+                umma_commit(&ctl->tfull[buf]);
+            }
+        }
+    } else {
+        // ---- epilogue: row 32 (warp % 4) + lane of the tile, 32 columns at a time
+        const int quarter = warp & 3;
+        int tl = 0;
+        for (long long L = first; L < nt; L += stride, tl++) {
+            int bi, bj;
+            tri_tile(L, nb, bi, bj);
+            const int buf = tl & 1;
+            if (!mbar_wait_abort(&ctl->tfull[buf], (uint32_t)((tl >> 1) & 1), abort_flag)) {
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            const int i = bi * BM + quarter * 32 + lane;
+            const uint32_t src = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * ACC_COLS);
 #pragma unroll 1
             for (int cb = 0; cb < BN / 32; cb++) {
                 uint32_t r[32];
-                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 32), r);
+                tmem_ld32(src + (uint32_t)(cb * 32), r);
                 const int j0 = bj * BN + cb * 32;
                 if (MODE == EPI_HIST) {
 #pragma unroll
@@ -192,24 +224,24 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
                     });
                 }
             }
+            // the accumulator may be overwritten once every epilogue warp has read it
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->tempty[buf]);
         }
-        tc_fence_before();
-        __syncthreads();   // TMEM is free for the next tile's MMAs
-        tiles_done++;
-        L = Ln;
-        bi = nbi;
-        bj = nbj;
     }
-    if (ctl->abort && t == 0) {
-        atomicExch(err, 1);
-        // wait (bounded) for our own MMAs, then for our own copies still in flight
+    // the MMA thread waits (bounded) until its own MMAs have completed: TMEM
+    // is freed below, whichever way the roles ended
+    if (warp == 1 && lane == 0) {
         umma_commit(&ctl->drainbar);
         mbar_wait(&ctl->drainbar, 0);
-        while (consumed < issued) {
-            const int s = (int)(consumed % STAGES);
-            if (!mbar_wait(&ctl->full[s], (uint32_t)((consumed / STAGES) & 1))) break;
-            consumed++;
-        }
+    }
+    __syncthreads();
+    if (*abort_flag && t == 0) {
+        atomicExch(err, 1);
+        // the producer waits (bounded) for its copies still in flight
+        for (long long q = ctl->consumed; q < ctl->issued; q++)
+            if (!mbar_wait(&ctl->full[(int)(q % STAGES)], (uint32_t)((q / STAGES) & 1))) break;
     }
     if (MODE == EPI_HIST) {
         epi_hist_flush(below, neg, p);
@@ -254,14 +286,17 @@ pg_status launch_gram_tc(pg_ctx* ctx, const ZOperands& z, int mode, const EpiPar
     int* err;
     PG_TRY(pg_wst(ctx, "tc.err", 1, &err));
     PG_CUDA(ctx, cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+    // a pending failure-path test stall applies to this launch only
+    const unsigned long long stall = ctx->debug_gram_stall_ns;
+    ctx->debug_gram_stall_ns = 0;
     if (mode == EPI_HIST) {
         PG_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc<EPI_HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)SMEM_BYTES));
-        k_gram_tc<EPI_HIST><<<(int)grid, THREADS, SMEM_BYTES, ctx->stream>>>(mhi, mlo, nb, nk, p, err);
+        k_gram_tc<EPI_HIST><<<(int)grid, THREADS, SMEM_BYTES, ctx->stream>>>(mhi, mlo, nb, nk, p, stall, err);
     } else {
         PG_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc<EPI_EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)SMEM_BYTES));
-        k_gram_tc<EPI_EMIT><<<(int)grid, THREADS, SMEM_BYTES, ctx->stream>>>(mhi, mlo, nb, nk, p, err);
+        k_gram_tc<EPI_EMIT><<<(int)grid, THREADS, SMEM_BYTES, ctx->stream>>>(mhi, mlo, nb, nk, p, stall, err);
     }
     PG_LAUNCHED(ctx);
     int herr = 0;

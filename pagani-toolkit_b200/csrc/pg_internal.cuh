@@ -33,6 +33,9 @@ struct pg_ctx {
     std::vector<ProfSpan> prof_open;
     std::map<std::string, std::pair<int64_t, double>> prof_sum;
     std::vector<cudaEvent_t> prof_free;
+    // failure-path test hook (pg_debug_stall_next_gram): the next tcgen05 Gram
+    // launch waits this long on a barrier nothing arrives on, then gives up
+    unsigned long long debug_gram_stall_ns = 0;
 };
 
 struct pg_graph {

@@ -54,6 +54,23 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, uint32_t parity
     return true;
 }
 
+// Bounded wait that also gives up as soon as *abort is set (by another warp
+// of the CTA that gave up first).
+__device__ __forceinline__ bool mbar_wait_abort(unsigned long long* b, uint32_t parity, volatile int* abort,
+                                                unsigned long long ns = WAIT_NS)
+{
+    if (mbar_try(b, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (!mbar_try(b, parity))
+        if (*abort || gtimer() - t0 > ns) return false;
+    return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
 // 2-D tiled TMA load of the box at (x, y) into shared memory, completing
 // on `bar` (expect_tx must have been posted for its bytes).
 __device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar)

@@ -32,7 +32,7 @@ EXPORTS = [
     "pg_clustering_noalloc", "pg_clustering_noalloc_max_nodes",
     "pg_cohort_create", "pg_cohort_add", "pg_cohort_graph", "pg_cohort_packed", "pg_cohort_info",
     "pg_cohort_free", "pg_profile_enable", "pg_profile_reset", "pg_profile_get",
-    "pg_run_opts_default", "pg_surrogate_seed", "pg_run_subjects",
+    "pg_run_opts_default", "pg_surrogate_seed", "pg_run_subjects", "pg_debug_stall_next_gram",
 ]
 
 
@@ -142,6 +142,7 @@ def lib():
         L.pg_surrogate_seed.argtypes = [ct.c_uint64, i32, i32]
         L.pg_surrogate_seed.restype = ct.c_uint64
         L.pg_run_subjects.argtypes = [vp, P(Subject), i32, P(RunOpts)]
+        L.pg_debug_stall_next_gram.argtypes = [vp, ct.c_uint64]
         _lib = L
     return _lib
 

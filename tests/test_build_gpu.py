@@ -104,3 +104,51 @@ def test_tiny_and_ragged_sizes(ctx, N):
         R, C, _ = g.to_csr()
         Ro, Co, _, _ = _oracle_graph(bold, "s", 10.0)
         assert np.array_equal(R, Ro) and np.array_equal(C, Co)
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "fp32"])
+def test_nan_series_give_isolated_voxels(ctx, precision):
+    """A voxel with a NaN sample (or NaN everywhere) has a NaN variance: the
+    reference's r is NaN there and post_block stores it as 0
+    (U/CorMat/CUCorMat/CUCORMAT/CorMat.cpp:821), so the voxel has no edge;
+    the rest of the graph equals the oracle's."""
+    N, T = 500, 120
+    bold = synth.bold_series(N, T, 8, 9090)
+    bold[:, 17] = np.nan
+    bold[40, 123] = np.nan
+    bold[:, 300] = np.inf
+    z, nz = O.zscore(bold)
+    assert nz == 3
+    r = O.corr_packed(z)
+    for mode, value in (("r", 0.3), ("s", 2.0)):
+        g, info = ctx.build_graph(bold, mode=mode, value=value, sign="signed", precision=precision)
+        R, C, _ = g.to_csr()
+        if mode == "r":
+            Ro, Co, _ = O.graph_r(r, N, value)
+        else:
+            Ro, Co, _, tau = O.graph_k(r, N, O.sparsity_k(N, value))
+            assert info["tau"] == tau
+        assert info["zero_variance"] == 3
+        assert np.array_equal(R, Ro) and np.array_equal(C, Co)
+        for v in (17, 123, 300):
+            assert R[v + 1] == R[v] or mode == "s"
+
+
+def test_gram_wait_that_runs_out_returns_timeout_and_context_stays_usable(ctx):
+    """Failure path of the tensor-core Gram kernel, with no GPU fault: a test
+    hook makes its TMA producer wait 1 ms on an mbarrier that nothing arrives
+    on, before any copy or MMA is issued.  Every warp gives up (the waits are
+    bounded and abort-aware), TMEM is freed, pg_build_graph returns
+    PG_ERR_TIMEOUT, and the same context then builds the graph correctly."""
+    import pagani
+    N, T = 700, 96
+    bold = synth.bold_series(N, T, 6, 4711)
+    pagani.lib().pg_debug_stall_next_gram(ctx.h, 1_000_000)
+    with pytest.raises(pagani.PaganiError) as e:
+        ctx.build_graph(bold, mode="s", value=2.0, sign="signed", precision="bf16x3")
+    assert e.value.status == 6                      # PG_ERR_TIMEOUT
+    g, info = ctx.build_graph(bold, mode="s", value=2.0, sign="signed", precision="bf16x3")
+    R, C, _ = g.to_csr()
+    z, _ = O.zscore(bold)
+    Ro, Co, _, tau = O.graph_k(O.corr_packed(z), N, O.sparsity_k(N, 2.0))
+    assert info["tau"] == tau and np.array_equal(R, Ro) and np.array_equal(C, Co)

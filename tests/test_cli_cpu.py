@@ -115,3 +115,62 @@ def test_convertnii_robust_masks(tmp_path):
             assert struct.unpack_from("<ff", raw, 112) == (0.0, 0.0)
         got = np.frombuffer(raw[352:], np.dtype(np.float32).newbyteorder(endian))
         np.testing.assert_array_equal(got, want)
+
+
+# ------------------------------------------------------- corrupt input files
+def _csr_bytes(R, C, V=None):
+    parts = [np.array([len(R)], np.int32), np.asarray(R, np.int32), np.array([len(C)], np.int32),
+             np.asarray(C, np.int32)]
+    if V is not None:
+        parts += [np.array([len(V)], np.int32), np.asarray(V, np.float32)]
+    return b"".join(p.tobytes() for p in parts)
+
+
+_R = [0, 2, 3, 4]
+_C = [1, 2, 0, 0]
+
+CORRUPT_CSR = {
+    "empty": (b"", "bad row header"),
+    "truncated_rows": (_csr_bytes(_R, _C)[:10], "truncated row array"),
+    "missing_columns": (_csr_bytes(_R, _C)[:20], "bad column header"),
+    "truncated_columns": (_csr_bytes(_R, _C)[:-4], "truncated column array"),
+    "negative_rows": (np.array([-3], np.int32).tobytes(), "bad row header"),
+    "rowptr_mismatch": (_csr_bytes([0, 2, 3, 5], _C), "does not match the column count"),
+    "decreasing_rows": (_csr_bytes([0, 3, 2, 4], _C), "row offsets decrease"),
+    "column_out_of_range": (_csr_bytes(_R, [1, 7, 0, 0]), "column index out of range"),
+    "value_length": (_csr_bytes(_R, _C) + np.array([3], np.int32).tobytes() + np.zeros(3, np.float32).tobytes(),
+                     "value length differs"),
+    "truncated_values": (_csr_bytes(_R, _C, [1, 1, 1, 1])[:-4], "truncated value array"),
+}
+
+
+@pytest.mark.parametrize("case", list(CORRUPT_CSR))
+def test_corrupt_csr_is_rejected_before_any_gpu_work(tmp_path, case):
+    """The .csr reader (the format of CorMat.cpp:285-294 / manual p10) checks
+    every header, length and index; the Maslov tool reads its graph before it
+    opens a GPU context, so a corrupt file ends with exit status 1 and the
+    reason, on any machine."""
+    data, msg = CORRUPT_CSR[case]
+    path = tmp_path / f"{case}.csr"
+    path.write_bytes(data)
+    p = subprocess.run([os.path.join(BIN, "Maslov"), str(path)], capture_output=True, text=True, timeout=60)
+    assert p.returncode == 1
+    assert msg in p.stderr, p.stderr
+    assert not (tmp_path / f"{case}_Maslov.csr").exists()
+
+
+def test_corrupt_mask_nifti_is_rejected(tmp_path):
+    """CUCorMat reads the mask before opening a GPU context: a truncated
+    header, truncated data or an unsupported data type stop it with status 1."""
+    from tests.nifti import write_nifti
+    write_nifti(tmp_path / "mask.nii", np.ones((4, 4, 2), np.uint8), 2)
+    full = (tmp_path / "mask.nii").read_bytes()
+    cases = {"truncated NIfTI header": full[:200], "truncated data": full[:352 + 5]}
+    bad_type = bytearray(full)
+    bad_type[70:72] = np.array([128], np.int16).tobytes()        # RGB: not a supported type
+    cases["data type is not"] = bytes(bad_type)
+    for msg, data in cases.items():
+        (tmp_path / "mask.nii").write_bytes(data)
+        p = subprocess.run([os.path.join(BIN, "CUCorMat"), str(tmp_path), "0.5", "n", "n", "r", "0.3"],
+                           capture_output=True, text=True, timeout=60)
+        assert p.returncode == 1 and msg in p.stderr, (msg, p.stderr)

@@ -252,3 +252,24 @@ def test_cucormat_subject_average(tmp_path, tool, avg, mode, thr):
         assert np.array_equal(V, Vo)
     per_subject = glob.glob(str(d / "s*_500_spa*.csr"))
     assert len(per_subject) == (2 if avg[0] == "b" else 0)
+
+
+def test_cucormat_volume_size_mismatch(tmp_path):
+    """A subject whose volume differs from the mask is skipped with a message
+    in per-subject mode (the others are processed) and stops an averaging run
+    (the average would silently lose a subject)."""
+    N, T, shape = 300, 80, (10, 10, 3)
+    flat = np.zeros(np.prod(shape), np.uint8)
+    flat[:N] = 1
+    write_nifti(tmp_path / "mask.nii", flat.reshape(shape[2], shape[1], shape[0]).transpose(2, 1, 0), 2)
+    good = synth.bold_series(N, T, 6, 901)
+    write_nifti(tmp_path / "a_good.nii", volume_from_series(good, shape), 16)
+    write_nifti(tmp_path / "b_bad.nii", volume_from_series(synth.bold_series(N, T, 6, 902), (10, 10, 4)), 16)
+    p = subprocess.run([os.path.join(BIN, "CUCorMat"), str(tmp_path), "0.5", "n", "n", "r", "0.3"],
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0
+    assert "volume size differs from the mask" in p.stderr
+    assert glob.glob(str(tmp_path / "a_good_*.csr")) and not glob.glob(str(tmp_path / "b_bad_*.csr"))
+    p = subprocess.run([os.path.join(BIN, "CUCorMat"), str(tmp_path), "0.5", "yn", "n", "r", "0.3"],
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 1 and "volume size differs from the mask" in p.stderr

@@ -347,3 +347,25 @@ def test_dense_levels_with_split_tail_tiles(ctx):
         d_or, s_or = O.bfs_source(R, C, int(s))
         assert np.array_equal(dist[q], d_or)
         assert np.array_equal(sigma[q], s_or)
+
+
+def test_fw_batched_many_graphs_one_launch(ctx):
+    """A batch of 160 weighted ROI graphs of uneven size (from the synthetic
+    generator, |r| > 0.2, distances 1/w) in the one-launch FW + Onnela kernel:
+    every graph's efficiency, Lp and clustering against the oracle, including
+    graphs of one 64-wide block and graphs spanning several k-blocks."""
+    rng = np.random.default_rng(404)
+    sizes = list(rng.integers(20, 200, size=158)) + [64, 257]
+    gs, refs = [], []
+    for q, n in enumerate(sizes):
+        R, C, V = G.from_bold(int(n), 300, 0.2, 2000 + q, weighted=True)
+        gs.append(ctx.graph(R, C, V))
+        refs.append((R, C, V))
+    out = ctx.fw_batched(gs)
+    for (eff, lp, cp, cpm), (R, C, V) in zip(out, refs):
+        eff_or, lp_or = O.weighted_paths(R, C, V)
+        np.testing.assert_allclose(eff, eff_or, rtol=1e-5)
+        assert lp == pytest.approx(lp_or, rel=1e-6)
+        cp_or, m_or = O.onnela(R, C, V)
+        np.testing.assert_allclose(cp, cp_or, rtol=1e-5, atol=1e-7)
+        assert cpm == pytest.approx(m_or, rel=1e-5, abs=1e-9)
