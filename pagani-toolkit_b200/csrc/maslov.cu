@@ -56,15 +56,22 @@ __device__ __host__ __forceinline__ uint64_t mix64(uint64_t z)
     return z ^ (z >> 31);
 }
 
+// Edge bitmap over the unordered pairs {a, b}, a != b: bit lo (2n - lo - 1) / 2
+// + (hi - lo - 1), n(n - 1)/2 bits.
+__device__ __forceinline__ uint64_t pair_bit(uint64_t n, int a, int b)
+{
+    const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+    return lo * (2 * n - lo - 1) / 2 + (hi - lo - 1);
+}
 __device__ __forceinline__ bool has_edge(const unsigned long long* bits, uint64_t n, int a, int b)
 {
-    uint64_t q = (uint64_t)a * n + (uint64_t)b;
+    const uint64_t q = pair_bit(n, a, b);
     return (bits[q >> 6] >> (q & 63)) & 1ULL;
 }
 __device__ __forceinline__ void put_edge(unsigned long long* bits, uint64_t n, int a, int b, bool on)
 {
-    uint64_t q = (uint64_t)a * n + (uint64_t)b;
-    unsigned long long m = 1ULL << (q & 63);
+    const uint64_t q = pair_bit(n, a, b);
+    const unsigned long long m = 1ULL << (q & 63);
     if (on) atomicOr(&bits[q >> 6], m); else atomicAnd(&bits[q >> 6], ~m);
 }
 
@@ -91,8 +98,8 @@ __global__ void k_ms_init(const int32_t* __restrict__ R, const int32_t* __restri
             int c = 0;
             if (q < R[i + 1]) {
                 c = C[q];
-                put_edge(bits, (uint64_t)n, i, c, true);
                 up = c > i;
+                if (up) put_edge(bits, (uint64_t)n, i, c, true);
             }
             unsigned m = __ballot_sync(0xffffffffu, up);
             if (up) {
@@ -119,21 +126,17 @@ __global__ void k_ms_upper_count(const int32_t* __restrict__ R, const int32_t* _
     }
 }
 
-__global__ void k_ms_reset(MsControl* __restrict__ st, uint64_t attempts, uint32_t* __restrict__ slot_owner,
-                           uint32_t* __restrict__ slot_wr, long long M, uint32_t* __restrict__ table,
-                           uint32_t* __restrict__ pair_wr, uint32_t hsize)
+__global__ void k_ms_reset(MsControl* __restrict__ st, uint64_t attempts, unsigned long long* __restrict__ slot_owner,
+                           unsigned long long* __restrict__ slot_wr, long long M, unsigned long long* __restrict__ table,
+                           unsigned long long* __restrict__ pair_wr, uint32_t hsize)
 {
     const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
-    for (long long q = tid; q < M; q += nt) slot_owner[q] = slot_wr[q] = 0xffffffffu;
-    for (long long q = tid; q < hsize; q += nt) table[q] = pair_wr[q] = 0xffffffffu;
+    for (long long q = tid; q < M; q += nt) slot_owner[q] = slot_wr[q] = ~0ULL;
+    for (long long q = tid; q < hsize; q += nt) table[q] = pair_wr[q] = ~0ULL;
     if (tid == 0) {
-        st->fresh_next = 0;
-        st->attempts = attempts;
-        st->n_pending = 0;
-        st->n_next = 0;
-        st->oldest = 0;
-        st->next_oldest = ~0ULL;
+        st->n_pending[0] = st->n_pending[1] = 0;
+        st->oldest[0] = st->oldest[1] = ~0ULL;
         st->committed = 0;
         st->rounds = 0;
     }
@@ -165,15 +168,24 @@ k_ms_rounds(MsArgs p)
     unsigned long long* pend = p.pend_a;
     unsigned long long* pnext = p.pend_b;
     MsItem* items = (MsItem*)p.items;
-    for (;;) {
-        const volatile MsControl* vst = p.st;
-        const unsigned long long np = vst->n_pending;
-        const unsigned long long fresh = vst->fresh_next;
-        const unsigned long long left = vst->attempts - fresh;
-        const unsigned long long take = min(left, (unsigned long long)p.B - np);
+    volatile MsControl* vst = p.st;
+    // Claims and write records are 64-bit (round tag << 32 | attempt index
+    // relative to the round's oldest); the tag decreases with the round, so
+    // this round's entries are below every older one and nothing needs to be
+    // cleared between rounds.
+    unsigned long long fresh = 0;
+    for (uint32_t round = 0;; round++) {
+        const int cur = round & 1;
+        const unsigned long long np = vst->n_pending[cur];
+        const unsigned long long take = min(p.attempts - fresh, (unsigned long long)p.B - np);
         const unsigned long long total = np + take;
         if (total == 0) break;                                   // uniform over the grid
-        const unsigned long long base = np ? vst->oldest : fresh;    // oldest attempt of the round
+        const unsigned long long base = np ? vst->oldest[cur] : fresh;   // oldest attempt of the round
+        const unsigned long long tag = (unsigned long long)(0xffffffffu - round) << 32;
+        if (tid == 0) {           // the next round's counters (last read one round ago)
+            p.st->n_pending[cur ^ 1] = 0;
+            p.st->oldest[cur ^ 1] = ~0ULL;
+        }
         // ---- evaluate on the round's state; valid attempts claim
         for (long long it = tid; it < (long long)total; it += nt) {
             MsItem t;
@@ -191,60 +203,45 @@ k_ms_rounds(MsArgs p)
             else if (has_edge(p.bits, n, x1, x2) || has_edge(p.bits, n, y1, y2)) t.state = 1;
             else t.state = 2;
             if (t.state == 2) {
-                const uint32_t pr = (uint32_t)(t.a - base);
-                atomicMin(&p.slot_owner[t.i], pr);
-                atomicMin(&p.slot_owner[t.j], pr);
-                atomicMin(&p.table[t.h[0]], pr);
-                atomicMin(&p.table[t.h[1]], pr);
+                const unsigned long long me = tag | (uint32_t)(t.a - base);
+                atomicMin(&p.slot_owner[t.i], me);
+                atomicMin(&p.slot_owner[t.j], me);
+                atomicMin(&p.table[t.h[0]], me);
+                atomicMin(&p.table[t.h[1]], me);
             }
             items[it] = t;
         }
         grid.sync();
-        // ---- valid attempts owning all four claims commit: record their writes
-        for (long long it = tid; it < (long long)total; it += nt) {
-            MsItem& t = items[it];
-            if (t.state != 2) continue;
-            const uint32_t pr = (uint32_t)(t.a - base);
-            if (!(p.slot_owner[t.i] == pr && p.slot_owner[t.j] == pr && p.table[t.h[0]] == pr &&
-                  p.table[t.h[1]] == pr))
-                continue;
-            t.state = 3;
-            p.slot_wr[t.i] = pr;          // committed slots are disjoint
-            p.slot_wr[t.j] = pr;
-            atomicMin(&p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)], pr);
-            atomicMin(&p.pair_wr[pair_slot(t.v[2], t.v[3], n, p.hmask)], pr);
-            atomicMin(&p.pair_wr[t.h[0]], pr);
-            atomicMin(&p.pair_wr[t.h[1]], pr);
-        }
-        grid.sync();
-        // ---- apply the commits; defer valid attempts that lost and rejected
-        // attempts whose reads a lower-index commit wrote
+        // ---- valid attempts owning all four claims commit (their writes are
+        // recorded, then applied); valid attempts that lost are deferred
         unsigned long long mine = 0;
         for (long long it = tid; it < (long long)total; it += nt) {
             const MsItem t = items[it];
-            const uint32_t pr = (uint32_t)(t.a - base);
-            bool defer = t.state == 2;
-            if (t.state < 2) {
-                defer = p.slot_wr[t.i] < pr || p.slot_wr[t.j] < pr;
-                if (t.state == 1) defer |= p.pair_wr[t.h[0]] < pr || p.pair_wr[t.h[1]] < pr;
-            }
-            if (defer) {
-                pnext[atomicAdd(&p.st->n_next, 1ULL)] = t.a;
-                atomicMin(&p.st->next_oldest, t.a);
+            if (t.state != 2) continue;
+            const unsigned long long me = tag | (uint32_t)(t.a - base);
+            if (!(p.slot_owner[t.i] == me && p.slot_owner[t.j] == me && p.table[t.h[0]] == me &&
+                  p.table[t.h[1]] == me)) {
+                pnext[atomicAdd(&p.st->n_pending[cur ^ 1], 1ULL)] = t.a;
+                atomicMin(&p.st->oldest[cur ^ 1], t.a);
                 continue;
             }
-            if (t.state != 3) continue;
+            p.slot_wr[t.i] = me;          // committed slots are disjoint
+            p.slot_wr[t.j] = me;
+            atomicMin(&p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)], me);
+            atomicMin(&p.pair_wr[pair_slot(t.v[2], t.v[3], n, p.hmask)], me);
+            atomicMin(&p.pair_wr[t.h[0]], me);
+            atomicMin(&p.pair_wr[t.h[1]], me);
             const int V1 = t.v[0], V2 = t.v[1], V3 = t.v[2], V4 = t.v[3];
-            put_edge(p.bits, n, V1, V2, false); put_edge(p.bits, n, V2, V1, false);
-            put_edge(p.bits, n, V3, V4, false); put_edge(p.bits, n, V4, V3, false);
+            put_edge(p.bits, n, V1, V2, false);
+            put_edge(p.bits, n, V3, V4, false);
             if (t.coin) {   // 1-3, 2-4 (Maslov.cpp:36-44)
-                put_edge(p.bits, n, V1, V3, true); put_edge(p.bits, n, V3, V1, true);
-                put_edge(p.bits, n, V2, V4, true); put_edge(p.bits, n, V4, V2, true);
+                put_edge(p.bits, n, V1, V3, true);
+                put_edge(p.bits, n, V2, V4, true);
                 p.eb[t.i] = V3;
                 p.ea[t.j] = V2;
             } else {        // 1-4, 3-2 (Maslov.cpp:47-56)
-                put_edge(p.bits, n, V1, V4, true); put_edge(p.bits, n, V4, V1, true);
-                put_edge(p.bits, n, V2, V3, true); put_edge(p.bits, n, V3, V2, true);
+                put_edge(p.bits, n, V1, V4, true);
+                put_edge(p.bits, n, V2, V3, true);
                 p.eb[t.i] = V4;
                 p.eb[t.j] = V2;
             }
@@ -253,24 +250,20 @@ k_ms_rounds(MsArgs p)
         mine = __reduce_add_sync(0xffffffffu, (unsigned)mine);
         if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&p.st->committed, mine);
         grid.sync();
-        // ---- release the claims and write records; advance the round counters
+        // ---- rejected attempts whose reads a lower-index commit wrote are deferred
         for (long long it = tid; it < (long long)total; it += nt) {
             const MsItem t = items[it];
-            p.slot_owner[t.i] = p.slot_owner[t.j] = 0xffffffffu;
-            p.slot_wr[t.i] = p.slot_wr[t.j] = 0xffffffffu;
-            p.table[t.h[0]] = p.table[t.h[1]] = 0xffffffffu;
-            p.pair_wr[t.h[0]] = p.pair_wr[t.h[1]] = 0xffffffffu;
-            p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)] = 0xffffffffu;
-            p.pair_wr[pair_slot(t.v[2], t.v[3], n, p.hmask)] = 0xffffffffu;
+            if (t.state >= 2) continue;
+            const unsigned long long me = tag | (uint32_t)(t.a - base);
+            bool defer = p.slot_wr[t.i] < me || p.slot_wr[t.j] < me;
+            if (t.state == 1) defer |= p.pair_wr[t.h[0]] < me || p.pair_wr[t.h[1]] < me;
+            if (defer) {
+                pnext[atomicAdd(&p.st->n_pending[cur ^ 1], 1ULL)] = t.a;
+                atomicMin(&p.st->oldest[cur ^ 1], t.a);
+            }
         }
-        if (tid == 0) {
-            p.st->n_pending = p.st->n_next;
-            p.st->oldest = p.st->next_oldest;
-            p.st->n_next = 0;
-            p.st->next_oldest = ~0ULL;
-            p.st->fresh_next = fresh + take;
-            p.st->rounds++;
-        }
+        fresh += take;
+        if (tid == 0) p.st->rounds = round + 1;
         grid.sync();
         unsigned long long* tmp = pend;
         pend = pnext;
@@ -323,7 +316,7 @@ pg_status ms_prepare(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t atte
     const long long M = g->nnz / 2;
     const long long B = ms_round_size(M);
     const uint32_t H = ms_table_size(B);
-    const uint64_t nbits = (uint64_t)n * (uint64_t)n;
+    const uint64_t nbits = (uint64_t)n * (uint64_t)(n > 0 ? n - 1 : 0) / 2;   // unordered pairs
     const size_t words = (size_t)((nbits + 63) / 64);
     memset(a, 0, sizeof *a);
     a->n = n;

@@ -5,12 +5,8 @@
 
 // Round counters of one rewiring, in device memory.
 struct MsControl {
-    unsigned long long fresh_next;   // next attempt index never evaluated
-    unsigned long long attempts;     // attempts to evaluate in total
-    unsigned long long n_pending;    // deferred attempts carried into this round
-    unsigned long long n_next;       // deferred attempts of this round
-    unsigned long long oldest;       // smallest index among the pending ones
-    unsigned long long next_oldest;
+    unsigned long long n_pending[2];  // deferred attempts carried into a round (by round parity)
+    unsigned long long oldest[2];     // smallest index among them
     unsigned long long committed;
     unsigned long long rounds;
 };
@@ -28,11 +24,13 @@ struct MsArgs {
     long long* off;
     int *ea, *eb;                    // slot end points
     float* ew;                       // slot weights
-    unsigned long long* bits;        // n x n edge bitmap
-    uint32_t* slot_owner;            // per slot: lowest claiming attempt (relative)
-    uint32_t* table;                 // per pair entry: lowest claiming attempt (relative)
-    uint32_t* slot_wr;               // per slot: the committed attempt writing it
-    uint32_t* pair_wr;               // per pair entry: lowest committed attempt writing it
+    unsigned long long* bits;        // edge bitmap over the n(n-1)/2 unordered pairs
+    // claims and write records: round tag << 32 | attempt index relative to
+    // the round's oldest (lowest wins)
+    unsigned long long* slot_owner;  // per slot: lowest claiming attempt
+    unsigned long long* table;       // per pair entry: lowest claiming attempt
+    unsigned long long* slot_wr;     // per slot: the committed attempt writing it
+    unsigned long long* pair_wr;     // per pair entry: lowest committed attempt writing it
     void* items;                     // per round item: the evaluated attempt
     unsigned long long *pend_a, *pend_b;
     MsControl* st;

@@ -56,19 +56,52 @@ k_msbfs_all(PathArgs p)
             const int c = max(0, min(64, ns - q * 64));
             full.w[q] = c == 64 ? ~0ULL : (c ? ((1ULL << c) - 1ULL) : 0ULL);
         }
+        // level 1 by push: the batch's sources OR their bit into their
+        // neighbours' frontier words (a pull sweep would read every edge)
         for (int v = (int)tid; v < n; v += (int)nt) {
-            Words<NW> f;
+            Words<NW> f, z;
 #pragma unroll
-            for (int q = 0; q < NW; q++) f.w[q] = 0ULL;
+            for (int q = 0; q < NW; q++) f.w[q] = z.w[q] = 0ULL;
             const int b = v - s0;
             if (b >= 0 && b < ns) f.w[b >> 6] = 1ULL << (b & 63);
-            front[v] = f;
+            front[v] = z;
             seen_a[v] = f;
         }
         if (tid == 0) p.flags[0] = p.flags[1] = p.flags[2] = 0;
         grid.sync();
-        Words<NW>*sin = seen_a, *sout = seen_b, *cur = front, *nxt = next;
-        for (int d = 1;; d++) {
+        for (int b = gw; b < ns; b += nw) {
+            const int src = s0 + b;
+            const unsigned long long bit = 1ULL << (b & 63);
+            for (int32_t q = p.R[src] + lane; q < p.R[src + 1]; q += 32) atomicOr(&front[p.C[q]].w[b >> 6], bit);
+        }
+        grid.sync();
+        {
+            unsigned long long found_total = 0;
+            for (int v = (int)tid; v < n; v += (int)nt) {
+                const Words<NW> f = front[v], sv = seen_a[v];
+                Words<NW> so;
+                int cnt = 0;
+#pragma unroll
+                for (int q = 0; q < NW; q++) {
+                    so.w[q] = sv.w[q] | f.w[q];
+                    cnt += __popcll(f.w[q]);
+                }
+                seen_b[v] = so;
+                if (cnt) p.cnt[(long long)v * MAX_D] += (unsigned)cnt;
+                found_total += (unsigned)cnt;
+            }
+            for (int o = 16; o; o >>= 1) found_total += __shfl_xor_sync(0xffffffffu, found_total, o);
+            if (lane == 0 && found_total) {
+                p.flags[1] = 1;
+                if (p.hist && 1 <= p.max_hop) atomicAdd(&p.hist[1], found_total);
+            }
+        }
+        grid.sync();
+        if (tid == 0) p.flags[0] = 0;
+        if (!((volatile int*)p.flags)[1]) continue;   // no source has a neighbour
+        diam = max(diam, 1);
+        Words<NW>*sin = seen_b, *sout = seen_a, *cur = front, *nxt = next;
+        for (int d = 2;; d++) {
             unsigned long long found_total = 0;
             for (int v = gw; v < n; v += nw) {
                 const Words<NW> sv = sin[v];
