@@ -374,7 +374,11 @@ def cohort_leg(ctx, count, rank=0):
     for prec in ("bf16x3", "fp32"):
         kw = dict(mode="s", value=COHORT_SPARSITY, sign="abs", n_random=COHORT_RANDOM, swaps_per_edge=COHORT_SWAPS,
                   seed=5, metrics=("degree", "cp", "eff"), precision=prec)
-        ctx.run_subjects([series[0].numpy()], **kw)          # warm-up (autotuner, workspace)
+        # warm-up: one surrogate per subject, so that every shape bucket is
+        # tuned (autotuner cache) and the workspace sized before timing
+        warm = dict(kw, n_random=1)
+        for b in series:
+            ctx.run_subjects([b.numpy()], **warm)
         secs, sig = [], []
         for b in series:
             torch.cuda.synchronize()

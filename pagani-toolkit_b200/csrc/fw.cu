@@ -10,9 +10,9 @@
 // barriers between them:
 //   A  matrices set to +inf (0 on the diagonal); the weight maximum of every
 //      graph (the Onnela normalisation);
-//   B  edge distances 1/w; Onnela clustering of every node of every graph
-//      (one CTA per node, dynamic scheduler, neighbour bitmap in shared
-//      memory);
+//   B  edge distances 1/w and the cube roots of the normalised weights;
+//      then Onnela clustering of every node of every graph (one CTA per
+//      node, dynamic scheduler, the node's row dense in shared memory);
 //   then for every 64-wide k-block round kb, over all graphs with more than
 //   kb blocks at once (graphs are sorted by block count, so the active ones
 //   are a prefix of the order):
@@ -41,7 +41,7 @@ namespace cg = cooperative_groups;
 namespace {
 constexpr int B = 64;           // k-block width
 constexpr int FW_THREADS = 256; // 16 x 16 threads, 4 x 4 outputs each
-constexpr int BMAX_BITS = 16384;// largest graph of a batch for the Onnela bitmap (n bits)
+constexpr int ONNELA_MAX_N = 4096; // largest graph of a batch for the Onnela row (n doubles in shared memory)
 
 struct FWGraph {
     const int32_t* R;
@@ -60,9 +60,11 @@ struct FwBatch {
     const int* active;          // [kb]: graphs with more than kb blocks (a prefix of gs)
     const long long* p2;        // prefix over gs of 2 (nb - 1): panel tasks
     const long long* p3;        // prefix over gs of (nb - 1)^2: phase-3 tasks
+    const long long* edge0;     // offset of each graph's edges in cw
     const int* node_graph;      // concatenated node -> index in gs
     float* D;
     float* vmax;
+    double* cw;                 // per edge of every graph: (V / vmax)^(1/3)
     int* onnela_next;           // dynamic node scheduler
     int onnela;                 // compute the clustering
     double* rowsum;             // per node
@@ -90,41 +92,36 @@ __device__ __forceinline__ int task_graph(const long long* pre, int count, long 
 
 // Onnela for node x of the batch (W/Cp/Cp/Cp_2.cpp:23-130, GPU weight maximum
 // over all edges): sum over connected neighbour pairs j < h of
-// (w_jh w_uj w_uh)^(1/3), w = V / vmax (float division); the weight of (u, h)
-// by binary search in u's sorted row.
-__device__ void onnela_node(const FwBatch& p, int x, unsigned* bm, double* red)
+// (w_jh w_uj w_uh)^(1/3), w = V / vmax (float division), computed as
+// cw_jh cw_uj cw_uh with the per-edge cube roots cw = w^(1/3) (FP64; the
+// same value up to rounding).  u's row is spread into a dense shared-memory
+// array (zero where h is not a neighbour), so the weight of (u, h) is one
+// shared load.
+__device__ void onnela_node(const FwBatch& p, int x, double* row, double* red)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = FW_THREADS / 32;
     const int gi = p.node_graph[x];
     const FWGraph g = p.gs[gi];
+    const long long e0 = p.edge0[gi];
     const int u = x - g.node0;
     const int32_t s = g.R[u], e = g.R[u + 1];
     const int k = e - s;
-    const float vm = p.vmax[gi];
-    const int W = (g.n + 31) >> 5;
-    for (int w = threadIdx.x; w < W; w += FW_THREADS) bm[w] = 0u;
-    __syncthreads();
     double acc = 0.0;
     if (k >= 2) {
-        for (int32_t q = s + threadIdx.x; q < e; q += FW_THREADS) atomicOr(&bm[g.C[q] >> 5], 1u << (g.C[q] & 31));
+        for (int32_t q = s + threadIdx.x; q < e; q += FW_THREADS) row[g.C[q]] = p.cw[e0 + q];
         __syncthreads();
         for (int32_t q = s + warp; q < e; q += nwarp) {
             const int j = g.C[q];
-            const double wuj = (double)__fdiv_rn(g.V[q], vm);
+            const double cuj = p.cw[e0 + q];
+            double part = 0.0;
             for (int32_t f = g.R[j] + lane; f < g.R[j + 1]; f += 32) {
                 const int h = g.C[f];
-                if (h <= j || !((bm[h >> 5] >> (h & 31)) & 1u)) continue;
-                const float wjh = __fdiv_rn(g.V[f], vm);
-                if (wjh == 0.0f) continue;
-                int32_t lo = s, hi = e - 1;
-                while (lo < hi) {
-                    const int32_t mid = (lo + hi) >> 1;
-                    if (g.C[mid] < h) lo = mid + 1; else hi = mid;
-                }
-                const double wuh = (double)__fdiv_rn(g.V[lo], vm);
-                acc += pow((double)wjh * wuj * wuh, 1.0 / 3.0);
+                if (h > j) part += p.cw[e0 + f] * row[h];
             }
+            acc += cuj * part;
         }
+        __syncthreads();
+        for (int32_t q = s + threadIdx.x; q < e; q += FW_THREADS) row[g.C[q]] = 0.0;
     }
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) red[warp] = acc;
@@ -185,7 +182,7 @@ struct __align__(16) FwSmem {
             float at[B][B + 4];     // the (bi, kb) block transposed: at[k][i]
             float bk[B][B + 4];     // the (kb, bj) block: bk[k][j]
         } prod;
-        unsigned bitmap[BMAX_BITS / 32];
+        double row[ONNELA_MAX_N];  // Onnela: the node's row, dense
     };
     double red[FW_THREADS / 32];
 };
@@ -228,26 +225,32 @@ k_fw_batch(FwBatch p)
         }
     }
     grid.sync();
-    // ---- B: edge distances 1/w (init_block, FormBlock.cpp:64); Onnela
+    // ---- B: edge distances 1/w (init_block, FormBlock.cpp:64); per-edge cube
+    // roots of the normalised weights for Onnela
     for (int gi = 0; gi < p.ng; gi++) {
         const FWGraph g = p.gs[gi];
         const long long warps = nt >> 5;
+        const float vm = p.onnela ? p.vmax[gi] : 1.0f;
+        const long long e0 = p.onnela ? p.edge0[gi] : 0;
         for (long long i = tid >> 5; i < g.n; i += warps)
             for (int32_t q = g.R[i] + (threadIdx.x & 31); q < g.R[i + 1]; q += 32) {
                 const int j = g.C[q];
+                if (p.onnela) p.cw[e0 + q] = cbrt((double)__fdiv_rn(g.V[q], vm));
                 if (j == i) continue;
                 p.D[g.off + i * g.np + j] = g.V ? __fdiv_rn(1.0f, g.V[q]) : 1.0f;
             }
     }
     if (p.onnela) {
+        grid.sync();
+        for (int q = threadIdx.x; q < ONNELA_MAX_N; q += FW_THREADS) sm.row[q] = 0.0;
         __shared__ int s_x;
         for (;;) {
+            __syncthreads();
             if (threadIdx.x == 0) s_x = atomicAdd(p.onnela_next, 1);
             __syncthreads();
             const int x = s_x;
-            __syncthreads();
             if (x >= p.total_nodes) break;
-            onnela_node(p, x, sm.bitmap, sm.red);
+            onnela_node(p, x, sm.row, sm.red);
         }
     }
     grid.sync();
@@ -416,7 +419,8 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
     auto nb_of = [&](int i) { return std::max(1, (graphs[i]->n + B - 1) / B); };
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nb_of(x) > nb_of(y); });
     std::vector<FWGraph> tab(ng);
-    std::vector<long long> p2(ng + 1, 0), p3(ng + 1, 0);
+    std::vector<long long> p2(ng + 1, 0), p3(ng + 1, 0), edge0(ng, 0);
+    long long edges = 0;
     std::vector<int> perm(ng), node0_out(ng), node_graph;
     long long off = 0;
     int node0 = 0, nmax = 1, max_nb = 0;
@@ -436,11 +440,13 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
         node0 += g->n;
         nmax = std::max(nmax, (int)g->n);
         max_nb = std::max(max_nb, nb);
+        edge0[q] = edges;
+        edges += g->nnz;
         p2[q + 1] = p2[q] + 2LL * (nb - 1);
         p3[q + 1] = p3[q] + (long long)(nb - 1) * (nb - 1);
     }
-    if (onnela && nmax > BMAX_BITS)
-        return pg_fail(ctx, PG_ERR_TOO_LARGE, "Onnela in the batched launch: n=%d above %d", nmax, BMAX_BITS);
+    if (onnela && nmax > ONNELA_MAX_N)
+        return pg_fail(ctx, PG_ERR_TOO_LARGE, "Onnela in the batched launch: n=%d above %d", nmax, ONNELA_MAX_N);
     std::vector<int> active(max_nb);
     for (int kb = 0; kb < max_nb; kb++) {
         int a = 0;
@@ -450,12 +456,14 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
     FwBatch& b = P->b;
     memset(&b, 0, sizeof b);
     int *dact, *dng, *dperm, *dn0;
-    long long *dp2, *dp3;
+    long long *dp2, *dp3, *de0;
     PG_TRY(pg_wst(ctx, "fw.D", (size_t)off, &b.D));
     PG_TRY(pg_wst(ctx, "fw.tab", (size_t)ng, &P->dtab));
     PG_TRY(pg_wst(ctx, "fw.active", (size_t)max_nb, &dact));
     PG_TRY(pg_wst(ctx, "fw.p2", (size_t)ng + 1, &dp2));
     PG_TRY(pg_wst(ctx, "fw.p3", (size_t)ng + 1, &dp3));
+    PG_TRY(pg_wst(ctx, "fw.edge0", (size_t)ng, &de0));
+    PG_TRY(pg_wst(ctx, "fw.cw", (size_t)(onnela ? edges : 0) + 1, &b.cw));
     PG_TRY(pg_wst(ctx, "fw.ngraph", (size_t)node0 + 1, &dng));
     PG_TRY(pg_wst(ctx, "fw.perm", (size_t)ng, &dperm));
     PG_TRY(pg_wst(ctx, "fw.node0o", (size_t)ng, &dn0));
@@ -470,6 +478,7 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
     PG_CUDA(ctx, cudaMemcpyAsync(dact, active.data(), sizeof(int) * max_nb, cudaMemcpyHostToDevice, ctx->stream));
     PG_CUDA(ctx, cudaMemcpyAsync(dp2, p2.data(), sizeof(long long) * (ng + 1), cudaMemcpyHostToDevice, ctx->stream));
     PG_CUDA(ctx, cudaMemcpyAsync(dp3, p3.data(), sizeof(long long) * (ng + 1), cudaMemcpyHostToDevice, ctx->stream));
+    PG_CUDA(ctx, cudaMemcpyAsync(de0, edge0.data(), sizeof(long long) * ng, cudaMemcpyHostToDevice, ctx->stream));
     if (node0 > 0)
         PG_CUDA(ctx, cudaMemcpyAsync(dng, node_graph.data(), sizeof(int) * node0, cudaMemcpyHostToDevice,
                                      ctx->stream));
@@ -483,6 +492,7 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
     b.active = dact;
     b.p2 = dp2;
     b.p3 = dp3;
+    b.edge0 = de0;
     b.node_graph = dng;
     b.onnela = onnela;
     P->perm = dperm;
