@@ -125,6 +125,27 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def l2_copy_gbs(device, mb=16, reps=200):
+    """Bandwidth of a device copy whose source and destination (2 x mb MB)
+    stay resident in the 126 MB L2: read + write bytes over the CUDA-event
+    time of `reps` back-to-back copies (best of three)."""
+    import torch
+    a = torch.ones(mb << 18, dtype=torch.float32, device=device)
+    b = torch.empty_like(a)
+    for _ in range(20):
+        b.copy_(a)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * a.numel() * 4 * reps / (e0.elapsed_time(e1) / 1000.0) / 1e9)
+    return best
+
+
 def reduce_max_ms(t_ms, device):
     """Step time of a multi-rank run: the maximum over ranks (replicas)."""
     import torch
@@ -443,6 +464,51 @@ def roi_batch_leg(ctx, stream, reps=3):
             "cp_mean": float(np.mean([o[3] for o in out]))}
 
 
+# ------------------------------------------------------- profiling cases
+def kernel_case(args):
+    """One small workload of one kernel family, for ncu captures (the metric
+    is not quoted on these): builds the subject of --voxels voxels (T = 240,
+    20 signals) and runs the case's call once after a warm-up call.
+      paths    -- hop paths of a Maslov surrogate at 0.5 % (k_msbfs_all)
+      maslov   -- one rewiring of 10 x |E| attempts at 0.5 % (k_ms_rounds)
+      fw_batch -- FW + Onnela of --graphs ROI graphs, n ~ U{90..1024} (k_fw_batch)
+      gram     -- one split-BF16 build at 1 % (k_gram_tc)
+      brandes  -- betweenness at 1 % (k_brandes, k_bc_dense)
+    Prints one JSON line with the call's device time."""
+    import torch
+    import pagani
+    from pagani import synth
+    ctx = pagani.Context(0)
+    stream = torch.cuda.ExternalStream(pagani.lib().pg_stream(ctx.h))
+    if args.case == "fw_batch":
+        series = synth.roi_batch(args.graphs, ROI_N[0], ROI_N[1], ROI_T, N_SIG, synth.subject_seed(4))
+        graphs = [ctx.build_graph(b, mode="r", value=ROI_R, sign="signed", weighted=True)[0] for b in series]
+        call = lambda: ctx.fw_batched(graphs)  # noqa: E731
+    else:
+        bold = synth.bold_series(N_VOX, T_LEN, N_SIG, synth.subject_seed(2, 0))
+        sp = 1.0 if args.case in ("gram", "brandes") else COHORT_SPARSITY
+        g, _ = ctx.build_graph(bold, mode="s", value=sp, sign="abs")
+        m = g.info[1] // 2
+        if args.case == "paths":
+            rg, _ = ctx.maslov(g, 7, COHORT_SWAPS * m)
+            call = lambda: ctx.paths(rg)  # noqa: E731
+        elif args.case == "maslov":
+            call = lambda: ctx.maslov(g, 7, COHORT_SWAPS * m)[0].free()  # noqa: E731
+        elif args.case == "gram":
+            call = lambda: ctx.build_graph(bold, mode="s", value=1.0, sign="abs")[0].free()  # noqa: E731
+        else:
+            call = lambda: ctx.betweenness(g)  # noqa: E731
+    call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "voxels": N_VOX, "ms": e0.elapsed_time(e1)}), flush=True)
+    ctx.close()
+
+
 # ------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -458,6 +524,9 @@ def main():
                     help="subjects of the cohort configuration timed beside the step (0: skip)")
     ap.add_argument("--no-precision-report", action="store_true")
     ap.add_argument("--no-roi-batch", action="store_true", help="skip the 512-graph weighted batch figure")
+    ap.add_argument("--case", default="step", choices=["step", "paths", "maslov", "fw_batch", "gram", "brandes"],
+                    help="profiling aid: one small workload of one kernel family instead of the benchmark")
+    ap.add_argument("--graphs", type=int, default=64, help="--case fw_batch: graphs in the batch")
     ap.add_argument("--voxels", type=int, default=N_VOX,
                     help="profiling aid: a smaller subject for ncu captures (the metric is quoted at 58000)")
     args = ap.parse_args()
@@ -469,6 +538,9 @@ def main():
 
 def run(args):
     set_voxels(args.voxels)
+    if args.case != "step":
+        kernel_case(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -611,6 +683,7 @@ def run(args):
 
     value = world * 60000.0 / ms_dev
     e2e = world * 60000.0 / ms_e2e
+    l2_peak = l2_copy_gbs(f"cuda:{local}")
     tm = timings[-1]
     prec_rep = None if args.no_precision_report else precision_report(ctx, bold_dev, tm)
     build = build_stage(ctx, bold_dev, stream, hbm_peak, bf16_peak)
@@ -659,6 +732,13 @@ def run(args):
         "roofline": {"bound": "hbm", "kernel": "k_brandes", "achieved": achieved, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved / hbm_peak if achieved else None,
                      "traffic": BRANDES_DRAM_BYTES_PER_BATCH_58K if N_VOX == 58000 else None,
+                     "traffic_source": "ncu one-pass dram__bytes_read.sum + dram__bytes_write.sum of the k_brandes "
+                                       "launches of one batch at 58k (profiles/k_brandes_subject58k.md)",
+                     "l2": {"peak_gbs_measured": l2_peak,
+                            "frac_of_l2": achieved / l2_peak if achieved and l2_peak else None,
+                            "note": "the DRAM traffic is 0.065 of the algorithmic bytes: the per-node source "
+                                    "rows and the CSR are served by L2, so L2 bandwidth and issue bound the "
+                                    "sweep, not HBM"},
                      "algorithmic_bytes_per_launch": bytes_batch,
                      "per_launch": "one 128-source batch (its k_brandes launches); algorithmic bytes of the "
                                    "backward sweep only",
