@@ -205,30 +205,17 @@ def cpu_baseline(n_sample=4000, threads=None):
         return _cpu_baseline(n_sample, threads)
 
 
-def _cpu_baseline(n_sample=4000, threads=None):
-    """The reference's own CPU pipeline (oracle/_ref) on a down-scaled subject.
-
-    The reference CPU code cannot run the 58k subject in bounded time
-    (single-thread Brandes alone is hours; CorMat_cpu_MT overflows its int
-    pair index beyond ~18.5k voxels).  The sample is a complete subject with
-    the same generator, T and density at n_sample voxels; each stage's time
-    is scaled to N = 58,000 by its work: N^2 for the correlation, selection
-    and CSR build, N^3 (fixed density, so N * nnz) for clustering, BFS path
-    length, betweenness and modularity.
-    """
-    from oracle import oracle as O
-    from pagani import synth
-    threads = threads or os.cpu_count() or 1
-    os.environ["PAGANI_REF_THREADS"] = str(threads)
-    ref = O.Ref()
-    bold = synth.bold_series(n_sample, T_LEN, N_SIG, synth.subject_seed(2, 99))
+def _cpu_stage_times(ref, O, synth, n, threads):
+    """Seconds per stage of the reference's CPU pipeline on a complete
+    n-voxel subject (same generator, T and density as the benchmark)."""
+    bold = synth.bold_series(n, T_LEN, N_SIG, synth.subject_seed(2, 99))
     st = {}
     t = time.perf_counter()
     cm = ref.cormat_cpu_mt(bold, threads)
     st["correlation"] = time.perf_counter() - t
-    k = O.sparsity_k(n_sample, SPARSITY)
+    k = O.sparsity_k(n, SPARSITY)
     t = time.perf_counter()
-    R, C, _ = ref.graph_s(np.abs(cm), n_sample, k)
+    R, C, _ = ref.graph_s(np.abs(cm), n, k)
     st["threshold_csr"] = time.perf_counter() - t
     t = time.perf_counter()
     ref.cp(R, C)
@@ -242,10 +229,34 @@ def _cpu_baseline(n_sample=4000, threads=None):
     t = time.perf_counter()
     ref.partition(R, C)
     st["newman"] = time.perf_counter() - t
-    scale2 = (N_VOX / n_sample) ** 2
-    scale3 = (N_VOX / n_sample) ** 3
-    sec = (st["correlation"] + st["threshold_csr"]) * scale2 + \
-        (st["cp"] + st["paths"] + st["betweenness"] + st["newman"]) * scale3
+    return st
+
+
+def _cpu_baseline(n_sample=4000, threads=None):
+    """The reference's own CPU pipeline (oracle/_ref) on a down-scaled subject.
+
+    The reference CPU code cannot run the 58k subject in bounded time
+    (single-thread Brandes alone is hours; CorMat_cpu_MT overflows its int
+    pair index beyond ~18.5k voxels).  The sample is a complete subject with
+    the same generator, T and density at n_sample voxels; each stage's time
+    is scaled to N = 58,000 by its work: N^2 for the correlation, selection
+    and CSR build, N^3 (fixed density, so N * nnz) for clustering, BFS path
+    length, betweenness and modularity.  A second complete subject of half
+    the size checks those exponents: the measured exponent of every stage
+    (log of the time ratio over log 2) is reported beside the assumed one.
+    """
+    from oracle import oracle as O
+    from pagani import synth
+    threads = threads or os.cpu_count() or 1
+    os.environ["PAGANI_REF_THREADS"] = str(threads)
+    ref = O.Ref()
+    half = _cpu_stage_times(ref, O, synth, n_sample // 2, threads)
+    st = _cpu_stage_times(ref, O, synth, n_sample, threads)
+    quad = ("correlation", "threshold_csr")
+    exps = {k2: (2 if k2 in quad else 3) for k2 in st}
+    measured = {k2: (float(np.log(st[k2] / half[k2]) / np.log(2.0)) if half[k2] > 0 and st[k2] > 0 else None)
+                for k2 in st}
+    sec = sum(st[k2] * (N_VOX / n_sample) ** exps[k2] for k2 in st)
     return {
         "value": 60.0 / sec, "unit": "subjects/min", "cores": threads, "kind": "reference",
         "sample": f"reference CPU pipeline (CorMat_cpu_MT, FormFullGraph_s on |r|, FormCSRGraph, Cp, APSP_BFS, "
@@ -253,6 +264,13 @@ def _cpu_baseline(n_sample=4000, threads=None):
                   f"times scaled to N={N_VOX} by N^2 (correlation/threshold) and N^3 (graph metrics); "
                   f"measured sample seconds " + json.dumps({k2: round(v, 3) for k2, v in st.items()}),
         "extrapolated_seconds_per_subject": sec,
+        "exponent_check": {"half_sample_voxels": n_sample // 2,
+                           "half_sample_seconds": {k2: round(v, 3) for k2, v in half.items()},
+                           "assumed": exps,
+                           "measured": {k2: (round(v, 2) if v is not None else None) for k2, v in measured.items()},
+                           "extrapolated_seconds_with_measured_exponents": float(sum(
+                               st[k2] * (N_VOX / n_sample) ** (measured[k2] if measured[k2] is not None else exps[k2])
+                               for k2 in st))},
     }
 
 

@@ -134,49 +134,82 @@ __device__ void onnela_node(const FwBatch& p, int x, double* row, double* red)
     __syncthreads();
 }
 
-// Closure of a 64 x 64 block in shared memory against the diagonal block dg
-// (which may be the block itself): mode 0 diagonal, 1 row panel
-// (s = min(s, dg (x) s)), 2 column panel (s = min(s, s (x) dg)).
-__device__ __forceinline__ void panel_steps(float (*s)[B + 1], float (*dg)[B + 1], int mode)
+// Closure of a 64 x 64 block held in registers (4 x 4 per thread, rows
+// 4 ty.., columns 4 tx..) against the diagonal block: mode 0 the diagonal
+// block itself, 1 a row panel (s = min(s, dg (x) s)), 2 a column panel
+// (s = min(s, s (x) dg)).  Row k and column k do not change in step k
+// (d_kk = 0), so at every step their owners publish them to shared rows
+// (double-buffered: one barrier per step) and every thread updates its tile
+// from 16-byte loads; the closed diagonal block is read from dgT (its
+// columns stored as rows) or dg.
+__device__ __forceinline__ void closure(float (&acc)[4][4], const float (*dg)[B + 4], const float (*dgT)[B + 4],
+                                        float (*rowbuf)[B], float (*colbuf)[B], int mode)
 {
     const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
-    for (int k = 0; k < B; k++) {
+#pragma unroll 1
+    for (int k0 = 0; k0 < B; k0 += 4) {
 #pragma unroll
-        for (int a = 0; a < 4; a++) {
-            const int i = ty * 4 + a;
+        for (int kk = 0; kk < 4; kk++) {
+            const int k = k0 + kk, buf = k & 1;
+            if (mode != 2 && ty == (k >> 2))   // row k of s: its owners are the threads of row block k/4
+                *(float4*)&rowbuf[buf][tx * 4] = make_float4(acc[kk][0], acc[kk][1], acc[kk][2], acc[kk][3]);
+            if (mode != 1 && tx == (k >> 2))   // column k of s
+                *(float4*)&colbuf[buf][ty * 4] = make_float4(acc[0][kk], acc[1][kk], acc[2][kk], acc[3][kk]);
+            __syncthreads();
+            const float4 a = mode == 1 ? *(const float4*)&dgT[k][ty * 4] : *(const float4*)&colbuf[buf][ty * 4];
+            const float4 b = mode == 2 ? *(const float4*)&dg[k][tx * 4] : *(const float4*)&rowbuf[buf][tx * 4];
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
-            for (int b = 0; b < 4; b++) {
-                const int j = tx * 4 + b;
-                const float c = mode == 1 ? dg[i][k] + s[k][j] : (mode == 2 ? s[i][k] + dg[k][j] : s[i][k] + s[k][j]);
-                s[i][j] = fminf(s[i][j], c);
-            }
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[r][c] = fminf(acc[r][c], av[r] + bv[c]);
         }
-        __syncthreads();
     }
 }
 
-__device__ __forceinline__ void load_block(float (*s)[B + 1], const float* src, int ld)
+__device__ __forceinline__ void tile_load(float (&acc)[4][4], const float* src, int ld)
 {
-    for (int q = threadIdx.x; q < B * B / 4; q += FW_THREADS) {
-        const int i = q / (B / 4), j4 = (q % (B / 4)) * 4;
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const float4 v = *(const float4*)(src + (long long)(ty * 4 + r) * ld + tx * 4);
+        acc[r][0] = v.x; acc[r][1] = v.y; acc[r][2] = v.z; acc[r][3] = v.w;
+    }
+}
+
+__device__ __forceinline__ void tile_store(float* dst, int ld, const float (&acc)[4][4])
+{
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        *(float4*)(dst + (long long)(ty * 4 + r) * ld + tx * 4) = make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+}
+
+// A 64 x 64 block into shared memory, row-major (rm) and/or transposed (tr).
+// Thread q reads the 4 floats at row q % 64, columns 4 (q / 64) + 16 it..:
+// a warp covers 32 consecutive rows of one column group, so the transposed
+// stores of a warp hit 32 consecutive words (no bank conflict).
+__device__ __forceinline__ void block_to_smem(const float* src, int ld, float (*rm)[B + 4], float (*tr)[B + 4])
+{
+#pragma unroll
+    for (int it = 0; it < B * B / 4 / FW_THREADS; it++) {
+        const int q = threadIdx.x + it * FW_THREADS;
+        const int i = q & (B - 1), j4 = (q >> 6) << 2;
         const float4 v = *(const float4*)(src + (long long)i * ld + j4);
-        s[i][j4] = v.x; s[i][j4 + 1] = v.y; s[i][j4 + 2] = v.z; s[i][j4 + 3] = v.w;
-    }
-}
-
-__device__ __forceinline__ void store_block(float* dst, int ld, float (*s)[B + 1])
-{
-    for (int q = threadIdx.x; q < B * B / 4; q += FW_THREADS) {
-        const int i = q / (B / 4), j4 = (q % (B / 4)) * 4;
-        *(float4*)(dst + (long long)i * ld + j4) = make_float4(s[i][j4], s[i][j4 + 1], s[i][j4 + 2], s[i][j4 + 3]);
+        if (rm) *(float4*)&rm[i][j4] = v;
+        if (tr) {
+            tr[j4][i] = v.x; tr[j4 + 1][i] = v.y; tr[j4 + 2][i] = v.z; tr[j4 + 3][i] = v.w;
+        }
     }
 }
 
 struct __align__(16) FwSmem {
     union {
         struct {
-            float s[B][B + 1];
-            float dg[B][B + 1];
+            float dg[B][B + 4];     // the closed diagonal block, row-major
+            float dgT[B][B + 4];    // and transposed
+            float rowbuf[2][B];     // row k of the tile being closed
+            float colbuf[2][B];     // column k
         } panel;
         struct {
             float at[B][B + 4];     // the (bi, kb) block transposed: at[k][i]
@@ -262,10 +295,10 @@ k_fw_batch(FwBatch p)
         for (int gi = blockIdx.x; gi < act; gi += gridDim.x) {
             const FWGraph g = p.gs[gi];
             float* d = blk(p.D, g, kb, kb);
-            load_block(sm.panel.s, d, g.np);
-            __syncthreads();
-            panel_steps(sm.panel.s, sm.panel.s, 0);
-            store_block(d, g.np, sm.panel.s);
+            float acc[4][4];
+            tile_load(acc, d, g.np);
+            closure(acc, sm.panel.dg, sm.panel.dgT, sm.panel.rowbuf, sm.panel.colbuf, 0);
+            tile_store(d, g.np, acc);
             __syncthreads();
         }
         grid.sync();
@@ -279,11 +312,12 @@ k_fw_batch(FwBatch p)
             int other = row ? local : local - (g.nb - 1);
             if (other >= kb) other++;
             float* d = row ? blk(p.D, g, kb, other) : blk(p.D, g, other, kb);
-            load_block(sm.panel.dg, blk(p.D, g, kb, kb), g.np);
-            load_block(sm.panel.s, d, g.np);
+            block_to_smem(blk(p.D, g, kb, kb), g.np, row ? nullptr : sm.panel.dg, row ? sm.panel.dgT : nullptr);
+            float acc[4][4];
+            tile_load(acc, d, g.np);
             __syncthreads();
-            panel_steps(sm.panel.s, sm.panel.dg, row ? 1 : 2);
-            store_block(d, g.np, sm.panel.s);
+            closure(acc, sm.panel.dg, sm.panel.dgT, sm.panel.rowbuf, sm.panel.colbuf, row ? 1 : 2);
+            tile_store(d, g.np, acc);
             __syncthreads();
         }
         grid.sync();
@@ -297,15 +331,8 @@ k_fw_batch(FwBatch p)
             int bi = local / m, bj = local % m;
             if (bi >= kb) bi++;
             if (bj >= kb) bj++;
-            const float* a = blk(p.D, g, bi, kb);
-            const float* b = blk(p.D, g, kb, bj);
-            for (int q = threadIdx.x; q < B * B / 4; q += FW_THREADS) {
-                const int i = q / (B / 4), j4 = (q % (B / 4)) * 4;
-                const float4 va = *(const float4*)(a + (long long)i * g.np + j4);
-                sm.prod.at[j4][i] = va.x; sm.prod.at[j4 + 1][i] = va.y;
-                sm.prod.at[j4 + 2][i] = va.z; sm.prod.at[j4 + 3][i] = va.w;
-                *(float4*)&sm.prod.bk[i][j4] = *(const float4*)(b + (long long)i * g.np + j4);
-            }
+            block_to_smem(blk(p.D, g, bi, kb), g.np, nullptr, sm.prod.at);
+            block_to_smem(blk(p.D, g, kb, bj), g.np, sm.prod.bk, nullptr);
             float* c = blk(p.D, g, bi, bj);
             float acc[4][4];
 #pragma unroll
