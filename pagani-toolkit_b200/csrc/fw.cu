@@ -220,8 +220,7 @@ struct __align__(16) FwSmem {
     double red[FW_THREADS / 32];
 };
 
-__global__ void __launch_bounds__(FW_THREADS, 2)
-k_fw_batch(FwBatch p)
+__device__ __forceinline__ void fw_batch_body(const FwBatch& p)
 {
     cg::grid_group grid = cg::this_grid();
     __shared__ FwSmem sm;
@@ -398,6 +397,14 @@ k_fw_batch(FwBatch p)
     }
 }
 
+// The kernel under two register budgets (2 or 4 resident CTAs per SM); the
+// autotuner times both on the real batch (same arithmetic, same results).
+template <int MINB>
+__global__ void __launch_bounds__(FW_THREADS, MINB) k_fw_batch(FwBatch p)
+{
+    fw_batch_body(p);
+}
+
 __global__ void k_fw_copy_out(const FWGraph* __restrict__ gs, const float* __restrict__ D, float* __restrict__ out)
 {
     const FWGraph g = gs[0];
@@ -437,7 +444,10 @@ struct FwPlan {
     int* node0_out;     // caller's node offsets
     long long total;
     int grid;
+    int minb;           // register budget of the kernel instance (resident CTAs per SM)
 };
+
+static pg_status fw_launch(pg_ctx* ctx, FwPlan* P, bool profiled);
 
 static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, bool onnela, FwPlan* P)
 {
@@ -525,34 +535,27 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
     P->perm = dperm;
     P->node0_out = dn0;
     P->total = node0;
-    int per_sm = 0;
-    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fw_batch, FW_THREADS, 0));
-    if (per_sm < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "FW: kernel does not fit an SM");
+    int per2 = 0, per4 = 0;
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_fw_batch<2>, FW_THREADS, 0));
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per4, k_fw_batch<4>, FW_THREADS, 0));
+    if (per2 < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "FW: kernel does not fit an SM");
+    // choices: (register budget, resident CTAs per SM)
     std::vector<TuneChoice> cands;
-    for (int c = 1; c <= std::min(per_sm, 4); c++) cands.push_back({c, 0});
-    TuneChoice best{std::min(per_sm, 2), 0};
+    for (int c = 1; c <= std::min(per2, 2); c++) cands.push_back({2, c});
+    for (int c = 3; c <= std::min(per4, 4); c++) cands.push_back({4, c});
+    TuneChoice best{2, std::min(per2, 2)};
     const std::string key = tune_key("fw_batch", off > 0 ? (long long)std::sqrt((double)off / ng) : 0, ng);
     PG_TRY(tune_pick(ctx, key, cands, &best, [&](const TuneChoice& c) -> pg_status {
-        P->grid = ctx->sm_count * c.a;
-        PG_CUDA(ctx, cudaMemsetAsync(b.onnela_next, 0, sizeof(int), ctx->stream));
-        cudaLaunchAttribute attr;
-        attr.id = cudaLaunchAttributeCooperative;
-        attr.val.cooperative = 1;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(P->grid);
-        cfg.blockDim = dim3(FW_THREADS);
-        cfg.stream = ctx->stream;
-        cfg.attrs = &attr;
-        cfg.numAttrs = 1;
-        PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_fw_batch, b));
-        PG_LAUNCHED(ctx);
-        return PG_OK;
+        P->minb = c.a;
+        P->grid = ctx->sm_count * c.b;
+        return fw_launch(ctx, P, false);
     }));
-    P->grid = ctx->sm_count * best.a;
+    P->minb = best.a;
+    P->grid = ctx->sm_count * best.b;
     return PG_OK;
 }
 
-static pg_status fw_launch(pg_ctx* ctx, FwPlan* P)
+static pg_status fw_launch(pg_ctx* ctx, FwPlan* P, bool profiled)
 {
     PG_CUDA(ctx, cudaMemsetAsync(P->b.onnela_next, 0, sizeof(int), ctx->stream));
     cudaLaunchAttribute attr;
@@ -564,8 +567,9 @@ static pg_status fw_launch(pg_ctx* ctx, FwPlan* P)
     cfg.stream = ctx->stream;
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
-    const int h = pg_prof_begin(ctx, "k_fw_batch");
-    PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_fw_batch, P->b));
+    const int h = profiled ? pg_prof_begin(ctx, "k_fw_batch") : -1;
+    if (P->minb == 4) PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_fw_batch<4>, P->b));
+    else PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_fw_batch<2>, P->b));
     PG_LAUNCHED(ctx);
     pg_prof_end(ctx, h);
     return PG_OK;
@@ -579,7 +583,7 @@ extern "C" pg_status pg_fw_paths(pg_ctx* ctx, const pg_graph* g, float* dist, fl
     const pg_graph* one[1] = {g};
     FwPlan P;
     PG_TRY(fw_plan(ctx, one, 1, false, &P));
-    PG_TRY(fw_launch(ctx, &P));
+    PG_TRY(fw_launch(ctx, &P, true));
     if (dist) {
         float* tmp;
         PG_TRY(pg_wst(ctx, "fw.out", (size_t)n * n + 1, &tmp));
@@ -602,7 +606,7 @@ extern "C" pg_status pg_fw_batched(pg_ctx* ctx, const pg_graph* const* graphs, i
     const bool onnela = cp || cp_mean;
     FwPlan P;
     PG_TRY(fw_plan(ctx, graphs, count, onnela, &P));
-    PG_TRY(fw_launch(ctx, &P));
+    PG_TRY(fw_launch(ctx, &P, true));
     float *deff, *dcp;
     double *dlp, *dcpm;
     PG_TRY(pg_wst(ctx, "fwb.eff", (size_t)P.total + 1, &deff));
