@@ -1,9 +1,10 @@
 // paths.cu -- hop path length and nodal efficiency (APSP_BFS,
 // U/BFS_MulCPU/BFS_MulCPU/APSP_BFS.cpp:27-147) by bit-parallel multi-source
 // BFS: 64*NW sources run together, one bit per source in NW 64-bit words per
-// node.  A level is a pull sweep: node v ORs the frontier words of its
-// neighbours, keeps the bits it has not seen, and stops scanning once every
-// missing source bit is found.  Because the graph is undirected,
+// node.  Level 1 is a push from the batch's sources; every later level is a
+// pull sweep: node v ORs the frontier words of its neighbours, keeps the
+// bits it has not seen, and stops scanning once every missing source bit is
+// found (tested every 128 neighbours).  Because the graph is undirected,
 // d(s, v) = d(v, s), so node v counts the sources it reaches at each
 // distance itself: cnt[v][d] (exact integers, summed over all batches), and
 // at the end inv[v] = sum_d cnt[v][d] / d with d ascending -- the oracle's and
@@ -114,21 +115,28 @@ k_msbfs_all(PathArgs p)
                     acc.w[q] = 0ULL;
                 }
                 if (any_need) {
+                    // every lane ORs its neighbours' frontier words; the warp
+                    // combines them (and tests for early exit) every 4 chunks
+                    // of 32 neighbours -- extra ORs only add bits of the
+                    // frontier, so the result does not depend on when it stops
                     const int32_t s = p.R[v], e = p.R[v + 1];
-                    for (int32_t base = s; base < e; base += 32) {
-                        const int32_t f = base + lane;
-                        if (f < e) {
-                            const Words<NW> fu = cur[p.C[f]];
+                    for (int32_t base = s; base < e; base += 128) {
 #pragma unroll
-                            for (int q = 0; q < NW; q++) acc.w[q] |= fu.w[q];
+                        for (int c = 0; c < 4; c++) {
+                            const int32_t f = base + c * 32 + lane;
+                            if (f < e) {
+                                const Words<NW> fu = cur[p.C[f]];
+#pragma unroll
+                                for (int q = 0; q < NW; q++) acc.w[q] |= fu.w[q];
+                            }
                         }
                         bool done = true;
 #pragma unroll
                         for (int q = 0; q < NW; q++) {
-                            unsigned long long x = acc.w[q];
-                            for (int o = 16; o; o >>= 1) x |= __shfl_xor_sync(0xffffffffu, x, o);
-                            acc.w[q] = x;
-                            done &= (x & need.w[q]) == need.w[q];
+                            const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)acc.w[q]);
+                            const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(acc.w[q] >> 32));
+                            acc.w[q] = ((unsigned long long)hi << 32) | lo;
+                            done &= (acc.w[q] & need.w[q]) == need.w[q];
                         }
                         if (done) break;
                     }
