@@ -203,19 +203,6 @@ __device__ __forceinline__ void block_to_smem(const float* src, int ld, float (*
     }
 }
 
-// Asynchronous 16-byte copies of a 64 x 64 block into a row-major shared
-// block (cp.async, no registers), as a commit group of the calling thread.
-__device__ __forceinline__ void block_async(float (*dst)[B + 4], const float* src, int ld)
-{
-#pragma unroll
-    for (int it = 0; it < B * B / 4 / FW_THREADS; it++) {
-        const int q = threadIdx.x + it * FW_THREADS;
-        const int i = q >> 4, j4 = (q & 15) << 2;
-        const unsigned d = (unsigned)__cvta_generic_to_shared(&dst[i][j4]);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + (long long)i * ld + j4) : "memory");
-    }
-}
-
 struct __align__(16) FwSmem {
     union {
         struct {
@@ -225,8 +212,8 @@ struct __align__(16) FwSmem {
             float colbuf[2][B];     // column k
         } panel;
         struct {
-            float a[2][B][B + 4];   // the (bi, kb) block, row-major, two buffers
-            float b[2][B][B + 4];   // the (kb, bj) block
+            float at[B][B + 4];     // the (bi, kb) block transposed: at[k][i]
+            float bk[B][B + 4];     // the (kb, bj) block: bk[k][j]
         } prod;
         double row[ONNELA_MAX_N];  // Onnela: the node's row, dense
     };
@@ -236,8 +223,7 @@ struct __align__(16) FwSmem {
 __device__ __forceinline__ void fw_batch_body(const FwBatch& p)
 {
     cg::grid_group grid = cg::this_grid();
-    extern __shared__ __align__(16) unsigned char fw_smem_raw[];
-    FwSmem& sm = *reinterpret_cast<FwSmem*>(fw_smem_raw);
+    __shared__ FwSmem sm;
     const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
     // ---- A: +inf matrices with a zero diagonal; weight maxima
@@ -334,59 +320,43 @@ __device__ __forceinline__ void fw_batch_body(const FwBatch& p)
             __syncthreads();
         }
         grid.sync();
-        // 3: the other blocks, register-tiled min-plus; the operand blocks of
-        // the CTA's next task load (cp.async) while this one computes
+        // 3: the other blocks, register-tiled min-plus
         const long long n3 = p.p3[act];
-        auto task = [&](long long t, const FWGraph*& gp, int& bi, int& bj) {
+        for (long long t = blockIdx.x; t < n3; t += gridDim.x) {
             const int gi = task_graph(p.p3, act, t);
-            gp = &p.gs[gi];
-            const int m = gp->nb - 1;
+            const FWGraph g = p.gs[gi];
+            const int m = g.nb - 1;
             const int local = (int)(t - p.p3[gi]);
-            bi = local / m;
-            bj = local % m;
+            int bi = local / m, bj = local % m;
             if (bi >= kb) bi++;
             if (bj >= kb) bj++;
-        };
-        auto prefetch = [&](long long t, int buf) {
-            if (t < n3) {
-                const FWGraph* gp;
-                int bi, bj;
-                task(t, gp, bi, bj);
-                block_async(sm.prod.a[buf], blk(p.D, *gp, bi, kb), gp->np);
-                block_async(sm.prod.b[buf], blk(p.D, *gp, kb, bj), gp->np);
-            }
-            asm volatile("cp.async.commit_group;" ::: "memory");
-        };
-        prefetch(blockIdx.x, 0);
-        int it = 0;
-        for (long long t = blockIdx.x; t < n3; t += gridDim.x, it++) {
-            const int buf = it & 1;
-            prefetch(t + gridDim.x, buf ^ 1);
-            const FWGraph* gp;
-            int bi, bj;
-            task(t, gp, bi, bj);
-            float* c = blk(p.D, *gp, bi, bj);
-            const int ld = gp->np;
+            block_to_smem(blk(p.D, g, bi, kb), g.np, nullptr, sm.prod.at);
+            block_to_smem(blk(p.D, g, kb, bj), g.np, sm.prod.bk, nullptr);
+            float* c = blk(p.D, g, bi, bj);
             float acc[4][4];
-            tile_load(acc, c, ld);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");   // this task's group is complete
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const float4 v = *(const float4*)(c + (long long)(ty * 4 + r) * g.np + tx * 4);
+                acc[r][0] = v.x; acc[r][1] = v.y; acc[r][2] = v.z; acc[r][3] = v.w;
+            }
             __syncthreads();
-            const float (*A)[B + 4] = sm.prod.a[buf];
-            const float (*Bk)[B + 4] = sm.prod.b[buf];
 #pragma unroll 8
             for (int k = 0; k < B; k++) {
-                const float4 bj4 = *(const float4*)&Bk[k][tx * 4];
-                const float av[4] = {A[ty * 4][k], A[ty * 4 + 1][k], A[ty * 4 + 2][k], A[ty * 4 + 3][k]};
+                const float4 ai = *(const float4*)&sm.prod.at[k][ty * 4];
+                const float4 bj4 = *(const float4*)&sm.prod.bk[k][tx * 4];
+                const float av[4] = {ai.x, ai.y, ai.z, ai.w};
                 const float bv[4] = {bj4.x, bj4.y, bj4.z, bj4.w};
 #pragma unroll
                 for (int r = 0; r < 4; r++)
 #pragma unroll
                     for (int q = 0; q < 4; q++) acc[r][q] = fminf(acc[r][q], av[r] + bv[q]);
             }
-            tile_store(c, ld, acc);
-            __syncthreads();   // the buffer is reloaded two tasks later
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                *(float4*)(c + (long long)(ty * 4 + r) * g.np + tx * 4) =
+                    make_float4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+            __syncthreads();
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");
         grid.sync();
     }
     // ---- C: row sums of 1/d over finite, non-tiny distances (CUBFW_Lp.cpp:77-83,99-104)
@@ -566,15 +536,13 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
     P->node0_out = dn0;
     P->total = node0;
     int per2 = 0, per4 = 0;
-    PG_CUDA(ctx, cudaFuncSetAttribute(k_fw_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwSmem)));
-    PG_CUDA(ctx, cudaFuncSetAttribute(k_fw_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FwSmem)));
-    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_fw_batch<2>, FW_THREADS, sizeof(FwSmem)));
-    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per4, k_fw_batch<4>, FW_THREADS, sizeof(FwSmem)));
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_fw_batch<2>, FW_THREADS, 0));
+    PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per4, k_fw_batch<4>, FW_THREADS, 0));
     if (per2 < 1) return pg_fail(ctx, PG_ERR_INTERNAL, "FW: kernel does not fit an SM");
     // choices: (register budget, resident CTAs per SM)
     std::vector<TuneChoice> cands;
     for (int c = 1; c <= std::min(per2, 2); c++) cands.push_back({2, c});
-    for (int c = 3; c <= std::min(per4, 4); c++) cands.push_back({4, c});   // when the shared memory allows
+    for (int c = 3; c <= std::min(per4, 4); c++) cands.push_back({4, c});
     TuneChoice best{2, std::min(per2, 2)};
     const std::string key = tune_key("fw_batch", off > 0 ? (long long)std::sqrt((double)off / ng) : 0, ng);
     PG_TRY(tune_pick(ctx, key, cands, &best, [&](const TuneChoice& c) -> pg_status {
@@ -596,7 +564,6 @@ static pg_status fw_launch(pg_ctx* ctx, FwPlan* P, bool profiled)
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P->grid);
     cfg.blockDim = dim3(FW_THREADS);
-    cfg.dynamicSmemBytes = sizeof(FwSmem);
     cfg.stream = ctx->stream;
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
