@@ -745,11 +745,13 @@ int or_newman_weighted(const int32_t* R, const int32_t* C, const float* Vw, int6
  * 2a + 1) and the round schedule of the GPU kernel: a round
  * holds the attempts deferred by the previous round plus fresh ones, up to
  * B = or_maslov_round_size(M); every attempt of a round is evaluated on the
- * state the previous round left; an attempt the reference would reject there
- * is decided; a valid attempt claims its two slots and the table entries of
- * its two new pairs (lowest attempt index wins); attempts owning all four
- * commit (they touch disjoint slots and create distinct pairs, so they
- * commute) and the others are deferred.  Every requested attempt is
+ * state the previous round left; a valid attempt claims its two slots and the
+ * table entries of its two new pairs (lowest attempt index wins); attempts
+ * owning all four commit (they touch disjoint slots and create distinct
+ * pairs, so they commute); valid attempts that lost, and rejected attempts
+ * whose reads a lower-index valid attempt may write (it claimed one of their
+ * slots or checked pair entries, or commits the removal of a checked pair),
+ * are deferred; the other rejected attempts are decided.  Every requested attempt is
  * evaluated once; the result is the GPU kernel's bit for bit. */
 static inline uint64_t mix64(uint64_t z)
 {
@@ -858,9 +860,8 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
     /* claims of valid attempts, then the writes of committed ones */
     uint64_t* slot_owner = (uint64_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(uint64_t));
     uint64_t* table = (uint64_t*)malloc((size_t)H * sizeof(uint64_t));
-    uint64_t* slot_wr = (uint64_t*)malloc((size_t)(M > 0 ? M : 1) * sizeof(uint64_t));
     uint64_t* pair_wr = (uint64_t*)malloc((size_t)H * sizeof(uint64_t));
-    for (int64_t q = 0; q < M; q++) slot_owner[q] = slot_wr[q] = UINT64_MAX;
+    for (int64_t q = 0; q < M; q++) slot_owner[q] = UINT64_MAX;
     for (uint32_t q = 0; q < H; q++) table[q] = pair_wr[q] = UINT64_MAX;
     MsItem* items = (MsItem*)malloc((size_t)B * sizeof(MsItem));
     unsigned char* commit = (unsigned char*)malloc((size_t)B);
@@ -897,26 +898,29 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
                 if (table[t->h[1]] > t->a) table[t->h[1]] = t->a;
             }
         }
-        /* valid attempts owning all four claims commit: record their writes */
+        /* valid attempts owning all four claims commit; they record the two
+         * pairs they remove */
         for (int64_t it = 0; it < total; it++) {
             MsItem* t = &items[it];
             commit[it] = t->state == 2 && slot_owner[t->i] == t->a && slot_owner[t->j] == t->a &&
                          table[t->h[0]] == t->a && table[t->h[1]] == t->a;
             if (!commit[it]) continue;
-            uint32_t o1 = pair_entry(t->v[0], t->v[1], N, hmask), o2 = pair_entry(t->v[2], t->v[3], N, hmask);
-            slot_wr[t->i] = slot_wr[t->j] = t->a;
-            uint32_t w[4] = {o1, o2, t->h[0], t->h[1]};
-            for (int q = 0; q < 4; q++) if (pair_wr[w[q]] > t->a) pair_wr[w[q]] = t->a;
+            uint32_t w[2] = {pair_entry(t->v[0], t->v[1], N, hmask), pair_entry(t->v[2], t->v[3], N, hmask)};
+            for (int q = 0; q < 2; q++) if (pair_wr[w[q]] > t->a) pair_wr[w[q]] = t->a;
         }
-        /* apply the commits; a rejected attempt whose reads a lower-index
-         * commit wrote is deferred, as is every valid attempt that lost */
+        /* apply the commits; every valid attempt that lost is deferred, and so
+         * is a rejected attempt when a lower-index valid attempt claimed one of
+         * its slots or a pair entry it checked, or a lower-index commit removes
+         * a pair it checked (conservative: such an attempt may not commit) */
         int64_t nn = 0;
         for (int64_t it = 0; it < total; it++) {
             MsItem* t = &items[it];
             if (t->state == 2 && !commit[it]) { pnext[nn++] = t->a; continue; }
             if (t->state < 2) {
-                int stale = slot_wr[t->i] < t->a || slot_wr[t->j] < t->a;
-                if (t->state == 1) stale |= pair_wr[t->h[0]] < t->a || pair_wr[t->h[1]] < t->a;
+                int stale = slot_owner[t->i] < t->a || slot_owner[t->j] < t->a;
+                if (t->state == 1)
+                    stale |= table[t->h[0]] < t->a || table[t->h[1]] < t->a ||
+                             pair_wr[t->h[0]] < t->a || pair_wr[t->h[1]] < t->a;
                 if (stale) pnext[nn++] = t->a;
                 continue;
             }
@@ -936,7 +940,7 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
         }
         for (int64_t it = 0; it < total; it++) {
             MsItem* t = &items[it];
-            slot_owner[t->i] = slot_owner[t->j] = slot_wr[t->i] = slot_wr[t->j] = UINT64_MAX;
+            slot_owner[t->i] = slot_owner[t->j] = UINT64_MAX;
             table[t->h[0]] = table[t->h[1]] = pair_wr[t->h[0]] = pair_wr[t->h[1]] = UINT64_MAX;
             pair_wr[pair_entry(t->v[0], t->v[1], N, hmask)] = UINT64_MAX;
             pair_wr[pair_entry(t->v[2], t->v[3], N, hmask)] = UINT64_MAX;
@@ -945,7 +949,7 @@ int64_t or_maslov(const int32_t* R, const int32_t* C, const float* V, int N, uin
         np = nn;
         fresh += take;
     }
-    free(slot_owner); free(table); free(slot_wr); free(pair_wr); free(items); free(commit); free(pend); free(pnext);
+    free(slot_owner); free(table); free(pair_wr); free(items); free(commit); free(pend); free(pnext);
     maslov_rebuild(R, N, M, ea, eb, ew, R_out, C_out, V_out);
     free(ea); free(eb); free(ew); free(bits);
     return committed;

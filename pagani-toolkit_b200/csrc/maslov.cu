@@ -17,11 +17,13 @@
 //     oldest attempt; slots in an owner array, pairs in a direct-mapped table
 //     where a collision of two pairs only costs a deferral); attempts that
 //     own all four claims commit;
-//   - every attempt whose evaluation read something (a slot, or the bit of a
-//     pair it needed absent) that a lower-index commit of the round writes,
-//     and every valid attempt that lost a claim, is deferred to the next
-//     round and evaluated again there; the other rejected attempts are
-//     decided.
+//   - every valid attempt that lost a claim is deferred to the next round
+//     and evaluated again there, and so is every rejected attempt whose
+//     evaluation read something a lower-index attempt of the round may
+//     write: a slot or a checked pair entry that a lower-index valid attempt
+//     claimed (conservative: that attempt may not commit), or a checked pair
+//     that a lower-index commit removes (committers record the pairs they
+//     remove); the other rejected attempts are decided.
 // Each decided attempt thus saw exactly the state the lower-index commits of
 // its round leave (commits touch disjoint slots and create distinct pairs,
 // and a valid attempt's new pairs are absent from the round's state), so a
@@ -127,12 +129,12 @@ __global__ void k_ms_upper_count(const int32_t* __restrict__ R, const int32_t* _
 }
 
 __global__ void k_ms_reset(MsControl* __restrict__ st, uint64_t attempts, unsigned long long* __restrict__ slot_owner,
-                           unsigned long long* __restrict__ slot_wr, long long M, unsigned long long* __restrict__ table,
-                           unsigned long long* __restrict__ pair_wr, uint32_t hsize)
+                           long long M, unsigned long long* __restrict__ table, unsigned long long* __restrict__ pair_wr,
+                           uint32_t hsize)
 {
     const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long nt = (long long)gridDim.x * blockDim.x;
-    for (long long q = tid; q < M; q += nt) slot_owner[q] = slot_wr[q] = ~0ULL;
+    for (long long q = tid; q < M; q += nt) slot_owner[q] = ~0ULL;
     for (long long q = tid; q < hsize; q += nt) table[q] = pair_wr[q] = ~0ULL;
     if (tid == 0) {
         st->n_pending[0] = st->n_pending[1] = 0;
@@ -225,12 +227,8 @@ k_ms_rounds(MsArgs p)
                 atomicMin(&p.st->oldest[cur ^ 1], t.a);
                 continue;
             }
-            p.slot_wr[t.i] = me;          // committed slots are disjoint
-            p.slot_wr[t.j] = me;
-            atomicMin(&p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)], me);
+            atomicMin(&p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)], me);   // the pairs it removes
             atomicMin(&p.pair_wr[pair_slot(t.v[2], t.v[3], n, p.hmask)], me);
-            atomicMin(&p.pair_wr[t.h[0]], me);
-            atomicMin(&p.pair_wr[t.h[1]], me);
             const int V1 = t.v[0], V2 = t.v[1], V3 = t.v[2], V4 = t.v[3];
             put_edge(p.bits, n, V1, V2, false);
             put_edge(p.bits, n, V3, V4, false);
@@ -250,13 +248,18 @@ k_ms_rounds(MsArgs p)
         mine = __reduce_add_sync(0xffffffffu, (unsigned)mine);
         if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&p.st->committed, mine);
         grid.sync();
-        // ---- rejected attempts whose reads a lower-index commit wrote are deferred
+        // ---- a rejected attempt is deferred when a lower-index valid attempt
+        // claimed one of its slots or a pair entry it checked, or a lower-index
+        // commit removes a pair it checked (conservative: the claimant may not
+        // have committed)
         for (long long it = tid; it < (long long)total; it += nt) {
             const MsItem t = items[it];
             if (t.state >= 2) continue;
             const unsigned long long me = tag | (uint32_t)(t.a - base);
-            bool defer = p.slot_wr[t.i] < me || p.slot_wr[t.j] < me;
-            if (t.state == 1) defer |= p.pair_wr[t.h[0]] < me || p.pair_wr[t.h[1]] < me;
+            bool defer = p.slot_owner[t.i] < me || p.slot_owner[t.j] < me;
+            if (t.state == 1)
+                defer |= p.table[t.h[0]] < me || p.table[t.h[1]] < me || p.pair_wr[t.h[0]] < me ||
+                         p.pair_wr[t.h[1]] < me;
             if (defer) {
                 pnext[atomicAdd(&p.st->n_pending[cur ^ 1], 1ULL)] = t.a;
                 atomicMin(&p.st->oldest[cur ^ 1], t.a);
@@ -332,7 +335,6 @@ pg_status ms_prepare(pg_ctx* ctx, const pg_graph* g, uint64_t seed, int64_t atte
     PG_TRY(pg_wst(ctx, "ms.bits", words + 1, &a->bits));
     PG_TRY(pg_wst(ctx, "ms.slot_owner", (size_t)M + 1, &a->slot_owner));
     PG_TRY(pg_wst(ctx, "ms.table", (size_t)H, &a->table));
-    PG_TRY(pg_wst(ctx, "ms.slot_wr", (size_t)M + 1, &a->slot_wr));
     PG_TRY(pg_wst(ctx, "ms.pair_wr", (size_t)H, &a->pair_wr));
     PG_TRY(pg_wst(ctx, "ms.items", (size_t)B, (MsItem**)&a->items));
     PG_TRY(pg_wst(ctx, "ms.pend_a", (size_t)B, &a->pend_a));
@@ -356,8 +358,8 @@ pg_status ms_enqueue(pg_ctx* ctx, const pg_graph* g, MsArgs* a)
 {
     const int grid = ctx->sm_count * 4;
     PG_CUDA(ctx, cudaMemsetAsync(a->bits, 0, sizeof(unsigned long long) * a->words, ctx->stream));
-    k_ms_reset<<<grid, 256, 0, ctx->stream>>>(a->st, a->attempts, a->slot_owner, a->slot_wr, a->M, a->table,
-                                               a->pair_wr, a->hmask + 1);
+    k_ms_reset<<<grid, 256, 0, ctx->stream>>>(a->st, a->attempts, a->slot_owner, a->M, a->table, a->pair_wr,
+                                               a->hmask + 1);
     PG_LAUNCHED(ctx);
     k_ms_upper_count<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, a->n, a->cnt);
     PG_LAUNCHED(ctx);

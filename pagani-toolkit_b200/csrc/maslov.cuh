@@ -29,8 +29,7 @@ struct MsArgs {
     // the round's oldest (lowest wins)
     unsigned long long* slot_owner;  // per slot: lowest claiming attempt
     unsigned long long* table;       // per pair entry: lowest claiming attempt
-    unsigned long long* slot_wr;     // per slot: the committed attempt writing it
-    unsigned long long* pair_wr;     // per pair entry: lowest committed attempt writing it
+    unsigned long long* pair_wr;     // per pair entry: lowest committed attempt removing that pair
     void* items;                     // per round item: the evaluated attempt
     unsigned long long *pend_a, *pend_b;
     MsControl* st;
