@@ -37,6 +37,7 @@ def build(ref: bool | None = None) -> None:
         ref = os.path.isdir(ref_root)
     if ref:
         targets.append("ref")
+    targets.append("big")
     subprocess.run(["make", "-s", "-C", HERE, f"REF_ROOT={ref_root}", *targets], check=True)
 
 
