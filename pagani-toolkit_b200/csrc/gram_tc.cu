@@ -10,7 +10,7 @@
 // of D against the exact dot product of the rounded z-scores stays below
 // 1e-4, far inside the 2e-3 guard band that the FP64 recheck covers.
 //
-// Structure: one persistent CTA of 6 warps per SM over the upper-triangle
+// Structure: one persistent CTA of 10 warps per SM over the upper-triangle
 // tiles in row-major order, warp-specialised:
 //   - warp 0 (one lane) streams K in 64-element chunks (128 B rows, 128B
 //     swizzle) with TMA into a 3-stage shared-memory ring (A_hi, A_lo, B_hi,
@@ -18,31 +18,27 @@
 //   - warp 1 (one lane) issues 12 UMMA (M=128, N=128, K=16, bf16 x bf16 ->
 //     fp32) per chunk into one of TWO TMEM accumulators (256 columns), a
 //     tcgen05.commit releasing every stage and, per tile, the accumulator;
-//   - warps 2-5 run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
-//     (rows) with tcgen05.ld 32x32b.x32, 32 columns at a time, classifies
-//     every pair (histogram, decided edge, FP64 band) in registers and hands
-//     the accumulator back (4 arrivals), so the next tile's MMAs run while
-//     this tile's epilogue does.
+//   - warps 2-9 run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+//     (rows), the two warps of a lane quarter 64 columns each, with
+//     tcgen05.ld 32x32b.x32, 32 columns at a time, classify every pair
+//     (histogram, decided edge, FP64 band) in registers and hand the
+//     accumulator back (8 arrivals), so the next tile's MMAs run while this
+//     tile's epilogue does.  The epilogue, not the tensor pipe or the TMA
+//     stream, bounds a tile (ncu: tensor pipe 9 %, fixed-latency waits on
+//     top), hence two warps per lane quarter.
 // Every mbarrier wait is bounded by the global timer and gives up at once
 // when another warp has given up; the kernel then records an error, waits
 // (bounded) for its own MMAs and TMA copies, frees TMEM and returns.
-//
-// For T <= 256 (every configuration here but the 1,200-sample ROI graphs)
-// k_gram_tc_ra runs instead: the same roles, but a CTA works through units of
-// up to 16 tiles of one row block whose operands stay resident in shared
-// memory, so only the column blocks stream (half the bytes per tile); the
-// kernel is bound by the TMA bytes in flight, not by the tensor pipe.
 #include "build_graph.cuh"
 #include "tma.cuh"
 #include <cuda.h>
-#include <algorithm>
-#include <vector>
 
 namespace {
 using namespace pg_tma;
 constexpr int BM = 128, BN = 128, KC = 64;
 constexpr int STAGES = 3;
-constexpr int WARPS = 6;
+constexpr int EPI_WARPS = 8;                    // two per TMEM lane quarter, 64 columns each
+constexpr int WARPS = 2 + EPI_WARPS;
 constexpr int THREADS = WARPS * 32;
 constexpr uint32_t TILE_BYTES = BM * KC * 2;       // 16 KB per operand tile
 constexpr uint32_t STAGE_BYTES = 4 * TILE_BYTES;   // A_hi, A_lo, B_hi, B_lo
@@ -97,7 +93,7 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&ctl->tfull[b], 1);
-            mbar_init(&ctl->tempty[b], 4);
+            mbar_init(&ctl->tempty[b], EPI_WARPS);
         }
         mbar_init(&ctl->drainbar, 1);
         mbar_init(&ctl->stallbar, 1);
@@ -191,8 +187,10 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             }
         }
     } else {
-        // ---- epilogue: row 32 (warp % 4) + lane of the tile, 32 columns at a time
+        // ---- epilogue: row 32 (warp % 4) + lane of the tile; the two warps of a
+        // lane quarter take 64 columns each, 32 at a time
         const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         int tl = 0;
         for (long long L = first; L < nt; L += stride, tl++) {
             int bi, bj;
@@ -206,7 +204,7 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             const int i = bi * BM + quarter * 32 + lane;
             const uint32_t src = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * ACC_COLS);
 #pragma unroll 1
-            for (int cb = 0; cb < BN / 32; cb++) {
+            for (int cb = half * (BN / 64); cb < (half + 1) * (BN / 64); cb++) {
                 uint32_t r[32];
                 tmem_ld32(src + (uint32_t)(cb * 32), r);
                 const int j0 = bj * BN + cb * 32;
@@ -262,251 +260,6 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-// ------------------------------------------------- resident row operands
-// Variant for T <= 256 (at most 4 chunks of 64 time points): a unit is up to
-// UNIT_W consecutive tiles (bi, bj0 ..) of one row block; the row block's
-// hi and lo operands (128 rows x T, <= 128 KB) are loaded once per unit and
-// stay in shared memory while only the column blocks stream through a ring
-// of BST stages (32 KB: B_hi, B_lo of one chunk) -- half the bytes per tile.
-// Same roles, barriers, bounded waits and epilogue as k_gram_tc.
-constexpr int UNIT_W = 16;
-constexpr int RA_MAX_NK = 4;
-constexpr uint32_t A_BYTES = 2 * RA_MAX_NK * TILE_BYTES;      // 128 KB
-constexpr uint32_t BSTAGE_BYTES = 2 * TILE_BYTES;             // 32 KB
-
-template <int BST>
-struct CtlRA {
-    unsigned long long full[BST];
-    unsigned long long empty[BST];
-    unsigned long long afull, aempty;
-    unsigned long long tfull[2];
-    unsigned long long tempty[2];
-    unsigned long long drainbar;
-    unsigned long long stallbar;
-    long long issued, consumed;     // B chunks
-    long long a_issued, a_consumed; // units whose row operands were loaded / taken by the MMA warp
-    uint32_t tmem_base;
-    int abort;
-};
-
-template <int BST>
-constexpr size_t ra_smem_bytes() { return 1024 + A_BYTES + BST * BSTAGE_BYTES + sizeof(CtlRA<BST>) + 64; }
-
-template <int MODE, int BST>
-__global__ void __launch_bounds__(THREADS, 1)
-k_gram_tc_ra(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo, int nb, int nk,
-             const int2* __restrict__ units, int nunits, EpiParams p, unsigned long long stall_ns,
-             int* __restrict__ err)
-{
-    extern __shared__ unsigned char smem_raw[];
-    __shared__ unsigned int sh_hist[MODE == EPI_HIST ? HIST_BINS : 1];
-    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    unsigned char* abase = smem;                    // row operands: chunk c hi at 2c, lo at 2c + 1
-    unsigned char* bbase = smem + A_BYTES;          // column ring
-    CtlRA<BST>* ctl = (CtlRA<BST>*)(bbase + BST * BSTAGE_BYTES);
-    volatile int* abort_flag = &ctl->abort;
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-
-    if (MODE == EPI_HIST)
-        for (int b = t; b < HIST_BINS; b += THREADS) sh_hist[b] = 0;
-    if (t == 0) {
-        for (int s = 0; s < BST; s++) {
-            mbar_init(&ctl->full[s], 1);
-            mbar_init(&ctl->empty[s], 1);
-        }
-        mbar_init(&ctl->afull, 1);
-        mbar_init(&ctl->aempty, 1);
-        for (int b = 0; b < 2; b++) {
-            mbar_init(&ctl->tfull[b], 1);
-            mbar_init(&ctl->tempty[b], 4);
-        }
-        mbar_init(&ctl->drainbar, 1);
-        mbar_init(&ctl->stallbar, 1);
-        ctl->issued = ctl->consumed = 0;
-        ctl->a_issued = ctl->a_consumed = 0;
-        ctl->abort = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&ctl->tmem_base)),
-                     "r"(TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = ctl->tmem_base;
-
-    const long long first = (long long)blockIdx.x * (MODE == EPI_HIST ? p.tile_stride : 1);
-    const long long stride = (MODE == EPI_HIST ? (long long)p.tile_stride : 1LL) * gridDim.x;
-    unsigned int below = 0u, neg = 0u;
-    auto unit_tiles = [&](long long u, int& bi, int& bj0, int& cnt) {
-        const int2 e = units[u];
-        bi = e.x;
-        bj0 = e.y;
-        cnt = min(UNIT_W, nb - bj0);
-    };
-
-    if (warp == 0) {
-        // ---- TMA producer
-        if (lane == 0) {
-            if (stall_ns && !mbar_wait_abort(&ctl->stallbar, 0, abort_flag, stall_ns)) *abort_flag = 1;
-            long long q = 0, ua = 0;
-            for (long long u = first; u < nunits && !*abort_flag; u += stride, ua++) {
-                int bi, bj0, cnt;
-                unit_tiles(u, bi, bj0, cnt);
-                // the previous unit's MMAs must be done with the row operands
-                if (!mbar_wait_abort(&ctl->aempty, (uint32_t)(ua & 1) ^ 1u, abort_flag)) {
-                    *abort_flag = 1;
-                    break;
-                }
-                mbar_expect_tx(&ctl->afull, 2u * nk * TILE_BYTES);
-                for (int c = 0; c < nk; c++) {
-                    tma_load(abase + (size_t)(2 * c) * TILE_BYTES, &map_hi, c * KC, bi * BM, &ctl->afull);
-                    tma_load(abase + (size_t)(2 * c + 1) * TILE_BYTES, &map_lo, c * KC, bi * BM, &ctl->afull);
-                }
-                ctl->a_issued = ua + 1;
-                for (int x = 0; x < cnt && !*abort_flag; x++) {
-                    const int bj = bj0 + x;
-                    for (int c = 0; c < nk; c++) {
-                        const int s = (int)(q % BST);
-                        if (!mbar_wait_abort(&ctl->empty[s], (uint32_t)((q / BST) & 1) ^ 1u, abort_flag)) {
-                            *abort_flag = 1;
-                            break;
-                        }
-                        unsigned char* st = bbase + (size_t)s * BSTAGE_BYTES;
-                        mbar_expect_tx(&ctl->full[s], BSTAGE_BYTES);
-                        tma_load(st, &map_hi, c * KC, bj * BN, &ctl->full[s]);
-                        tma_load(st + TILE_BYTES, &map_lo, c * KC, bj * BN, &ctl->full[s]);
-                        q++;
-                        ctl->issued = q;
-                    }
-                }
-            }
-        }
-    } else if (warp == 1) {
-        // ---- MMA issuer
-        if (lane == 0) {
-            long long q = 0, ua = 0;
-            int tl = 0;
-            bool ok = true;
-            for (long long u = first; u < nunits && ok && !*abort_flag; u += stride, ua++) {
-                int bi, bj0, cnt;
-                unit_tiles(u, bi, bj0, cnt);
-                if (!mbar_wait_abort(&ctl->afull, (uint32_t)(ua & 1), abort_flag)) { ok = false; break; }
-                ctl->a_consumed = ua + 1;
-                tc_fence_after();
-                for (int x = 0; x < cnt && ok; x++, tl++) {
-                    const int buf = tl & 1;
-                    if (!mbar_wait_abort(&ctl->tempty[buf], (uint32_t)((tl >> 1) & 1) ^ 1u, abort_flag)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t dst = tmem + (uint32_t)(buf * ACC_COLS);
-                    for (int c = 0; c < nk; c++) {
-                        const int s = (int)(q % BST);
-                        if (!mbar_wait_abort(&ctl->full[s], (uint32_t)((q / BST) & 1), abort_flag)) {
-                            ok = false;
-                            break;
-                        }
-                        tc_fence_after();
-                        unsigned char* st = bbase + (size_t)s * BSTAGE_BYTES;
-                        const unsigned long long ahi = sdesc(abase + (size_t)(2 * c) * TILE_BYTES);
-                        const unsigned long long alo = sdesc(abase + (size_t)(2 * c + 1) * TILE_BYTES);
-                        const unsigned long long bhi = sdesc(st), blo = sdesc(st + TILE_BYTES);
-#pragma unroll
-                        for (int kk = 0; kk < KC / 16; kk++) {
-                            const unsigned long long o = (unsigned long long)(kk * 32) >> 4;
-                            umma(dst, ahi + o, bhi + o, (c | kk) != 0);
-                            umma(dst, ahi + o, blo + o, 1u);
-                            umma(dst, alo + o, bhi + o, 1u);
-                        }
-                        umma_commit(&ctl->empty[s]);
-                        q++;
-                        ctl->consumed = q;
-                    }
-                    if (ok) umma_commit(&ctl->tfull[buf]);
-                }
-                if (ok) umma_commit(&ctl->aempty);   // the row operands are free once these MMAs completed
-            }
-            if (!ok) *abort_flag = 1;
-        }
-    } else {
-        // ---- epilogue: row 32 (warp % 4) + lane of the tile, 32 columns at a time
-        const int quarter = warp & 3;
-        int tl = 0;
-        bool ok = true;
-        for (long long u = first; u < nunits && ok; u += stride) {
-            int bi, bj0, cnt;
-            unit_tiles(u, bi, bj0, cnt);
-            for (int x = 0; x < cnt; x++, tl++) {
-                const int bj = bj0 + x;
-                const int buf = tl & 1;
-                if (!mbar_wait_abort(&ctl->tfull[buf], (uint32_t)((tl >> 1) & 1), abort_flag)) {
-                    *abort_flag = 1;
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const int i = bi * BM + quarter * 32 + lane;
-                const uint32_t src = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * ACC_COLS);
-#pragma unroll 1
-                for (int cb = 0; cb < BN / 32; cb++) {
-                    uint32_t r[32];
-                    tmem_ld32(src + (uint32_t)(cb * 32), r);
-                    const int j0 = bj * BN + cb * 32;
-                    if (MODE == EPI_HIST) {
-#pragma unroll
-                        for (int c = 0; c < 32; c++) {
-                            const int j = j0 + c;
-                            if (i < j && j < p.N) epi_hist(__uint_as_float(r[c]), p, sh_hist, below, neg);
-                        }
-                    } else {
-                        unsigned int m1 = 0u, m2 = 0u;
-#pragma unroll
-                        for (int c = 0; c < 32; c++) {
-                            const int j = j0 + c;
-                            const int cls = (i < j && j < p.N) ? epi_class(__uint_as_float(r[c]), p) : 0;
-                            m1 |= (unsigned)(cls == 1) << c;
-                            m2 |= (unsigned)(cls == 2) << c;
-                        }
-                        epi_emit_masks(m1, m2, p, [&](int q, int& ii, int& jj, float& v) {
-                            ii = i;
-                            jj = j0 + q;
-                            v = __uint_as_float(r[q]);
-                        });
-                    }
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&ctl->tempty[buf]);
-            }
-        }
-    }
-    if (warp == 1 && lane == 0) {
-        umma_commit(&ctl->drainbar);
-        mbar_wait(&ctl->drainbar, 0);
-    }
-    __syncthreads();
-    if (*abort_flag && t == 0) {
-        atomicExch(err, 1);
-        for (long long q = ctl->consumed; q < ctl->issued; q++)
-            if (!mbar_wait(&ctl->full[(int)(q % BST)], (uint32_t)((q / BST) & 1))) break;
-        for (long long ua = ctl->a_consumed; ua < ctl->a_issued; ua++)
-            if (!mbar_wait(&ctl->afull, (uint32_t)(ua & 1))) break;
-    }
-    if (MODE == EPI_HIST) {
-        epi_hist_flush(below, neg, p);
-        __syncthreads();
-        for (int b = t; b < HIST_BINS; b += THREADS)
-            if (sh_hist[b]) atomicAdd(&p.hist[b], sh_hist[b]);
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
-}
-
 bool make_map(CUtensorMap* m, const __nv_bfloat16* base, int rows, int cols)
 {
     EncodeTiledFn fn = encode_fn();
@@ -542,28 +295,7 @@ pg_status launch_gram_tc(pg_ctx* ctx, const ZOperands& z, int mode, const EpiPar
     // a pending failure-path test stall applies to this launch only
     const unsigned long long stall = ctx->debug_gram_stall_ns;
     ctx->debug_gram_stall_ns = 0;
-    if (nk <= RA_MAX_NK) {
-        // units of up to UNIT_W tiles of one row block, row-major
-        std::vector<int2> hu;
-        for (int bi = 0; bi < nb; bi++)
-            for (int bj0 = bi; bj0 < nb; bj0 += UNIT_W) hu.push_back(make_int2(bi, bj0));
-        int2* du;
-        PG_TRY(pg_wst(ctx, "tc.units", hu.size(), &du));
-        PG_TRY(pg_h2d(ctx, du, hu.data(), sizeof(int2) * hu.size()));
-        const int nunits = (int)hu.size();
-        const int g2 = (int)std::min<long long>(ctx->sm_count, nunits);
-        if (mode == EPI_HIST) {
-            constexpr size_t sm = ra_smem_bytes<2>();
-            PG_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc_ra<EPI_HIST, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)sm));
-            k_gram_tc_ra<EPI_HIST, 2><<<g2, THREADS, sm, ctx->stream>>>(mhi, mlo, nb, nk, du, nunits, p, stall, err);
-        } else {
-            constexpr size_t sm = ra_smem_bytes<3>();
-            PG_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc_ra<EPI_EMIT, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)sm));
-            k_gram_tc_ra<EPI_EMIT, 3><<<g2, THREADS, sm, ctx->stream>>>(mhi, mlo, nb, nk, du, nunits, p, stall, err);
-        }
-    } else if (mode == EPI_HIST) {
+    if (mode == EPI_HIST) {
         PG_CUDA(ctx, cudaFuncSetAttribute(k_gram_tc<EPI_HIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)SMEM_BYTES));
         k_gram_tc<EPI_HIST><<<(int)grid, THREADS, SMEM_BYTES, ctx->stream>>>(mhi, mlo, nb, nk, p, stall, err);
