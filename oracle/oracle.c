@@ -773,7 +773,7 @@ int64_t or_maslov_round_size(int64_t M)
 static uint32_t maslov_table_size(int64_t B)
 {
     uint32_t h = 1024;
-    while ((int64_t)h < 16 * B) h <<= 1;
+    while ((int64_t)h < 64 * B) h <<= 1;
     return h;
 }
 

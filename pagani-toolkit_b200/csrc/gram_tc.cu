@@ -10,7 +10,7 @@
 // of D against the exact dot product of the rounded z-scores stays below
 // 1e-4, far inside the 2e-3 guard band that the FP64 recheck covers.
 //
-// Structure: one persistent CTA of 10 warps per SM over the upper-triangle
+// Structure: one persistent CTA of 18 warps per SM over the upper-triangle
 // tiles in row-major order, warp-specialised:
 //   - warp 0 (one lane) streams K in 64-element chunks (128 B rows, 128B
 //     swizzle) with TMA into a 3-stage shared-memory ring (A_hi, A_lo, B_hi,
@@ -18,14 +18,13 @@
 //   - warp 1 (one lane) issues 12 UMMA (M=128, N=128, K=16, bf16 x bf16 ->
 //     fp32) per chunk into one of TWO TMEM accumulators (256 columns), a
 //     tcgen05.commit releasing every stage and, per tile, the accumulator;
-//   - warps 2-9 run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
-//     (rows), the two warps of a lane quarter 64 columns each, with
-//     tcgen05.ld 32x32b.x32, 32 columns at a time, classify every pair
-//     (histogram, decided edge, FP64 band) in registers and hand the
-//     accumulator back (8 arrivals), so the next tile's MMAs run while this
-//     tile's epilogue does.  The epilogue, not the tensor pipe or the TMA
-//     stream, bounds a tile (ncu: tensor pipe 9 %, fixed-latency waits on
-//     top), hence two warps per lane quarter.
+//   - warps 2-17 run the epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+//     (rows), the four warps of a lane quarter 32 columns each, with
+//     tcgen05.ld 32x32b.x32, classify every pair (histogram, decided edge,
+//     FP64 band) in registers and hand the accumulator back (16 arrivals),
+//     so the next tile's MMAs run while this tile's epilogue does.  The
+//     epilogue, not the tensor pipe or the TMA stream, bounds a tile (ncu:
+//     fixed-latency waits on top), hence several warps per lane quarter.
 // Every mbarrier wait is bounded by the global timer and gives up at once
 // when another warp has given up; the kernel then records an error, waits
 // (bounded) for its own MMAs and TMA copies, frees TMEM and returns.
@@ -37,7 +36,7 @@ namespace {
 using namespace pg_tma;
 constexpr int BM = 128, BN = 128, KC = 64;
 constexpr int STAGES = 3;
-constexpr int EPI_WARPS = 8;                    // two per TMEM lane quarter, 64 columns each
+constexpr int EPI_WARPS = 16;                   // four per TMEM lane quarter, 32 columns each
 constexpr int WARPS = 2 + EPI_WARPS;
 constexpr int THREADS = WARPS * 32;
 constexpr uint32_t TILE_BYTES = BM * KC * 2;       // 16 KB per operand tile
@@ -187,10 +186,11 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             }
         }
     } else {
-        // ---- epilogue: row 32 (warp % 4) + lane of the tile; the two warps of a
-        // lane quarter take 64 columns each, 32 at a time
+        // ---- epilogue: row 32 (warp % 4) + lane of the tile; the warps of a
+        // lane quarter share its 128 columns, 32 at a time
         const int quarter = warp & 3;
-        const int half = (warp - 2) >> 2;
+        const int part = (warp - 2) >> 2;               // 0 .. EPI_WARPS / 4 - 1
+        constexpr int CHUNKS = (BN / 32) / (EPI_WARPS / 4);
         int tl = 0;
         for (long long L = first; L < nt; L += stride, tl++) {
             int bi, bj;
@@ -204,7 +204,7 @@ k_gram_tc(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CU
             const int i = bi * BM + quarter * 32 + lane;
             const uint32_t src = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * ACC_COLS);
 #pragma unroll 1
-            for (int cb = half * (BN / 64); cb < (half + 1) * (BN / 64); cb++) {
+            for (int cb = part * CHUNKS; cb < (part + 1) * CHUNKS; cb++) {
                 uint32_t r[32];
                 tmem_ld32(src + (uint32_t)(cb * 32), r);
                 const int j0 = bj * BN + cb * 32;

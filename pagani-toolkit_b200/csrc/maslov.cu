@@ -309,7 +309,7 @@ int64_t ms_round_size(int64_t M)
 uint32_t ms_table_size(int64_t B)
 {
     uint32_t h = 1024;
-    while ((int64_t)h < 16 * B) h <<= 1;
+    while ((int64_t)h < 64 * B) h <<= 1;
     return h;
 }
 
