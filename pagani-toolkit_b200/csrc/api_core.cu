@@ -83,6 +83,8 @@ extern "C" pg_status pg_destroy(pg_ctx* ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->ws) cudaFree(kv.second.p);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    for (auto& kv : ctx->hws) cudaFreeHost(kv.second.p);
+    for (auto& st : ctx->pool) cudaStreamDestroy(st);
     for (auto& e : ctx->ev) cudaEventDestroy(e);
     for (auto& sp : ctx->prof_open) {
         cudaEventDestroy(sp.a);
@@ -226,6 +228,38 @@ pg_status pg_pinned(pg_ctx* ctx, size_t bytes, void** out)
         ctx->pinned_bytes = bytes;
     }
     *out = ctx->pinned;
+    return PG_OK;
+}
+
+pg_status pg_hws(pg_ctx* ctx, const char* key, size_t bytes, void** out)
+{
+    auto& b = ctx->hws[key];
+    if (b.bytes < bytes) {
+        if (b.p) {
+            PG_CUDA(ctx, cudaDeviceSynchronize());
+            cudaFreeHost(b.p);
+            b.p = nullptr;
+            b.bytes = 0;
+        }
+        const size_t want = bytes + bytes / 8;
+        if (cudaMallocHost(&b.p, want) != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return pg_fail(ctx, PG_ERR_NOMEM, "pinned buffer '%s': cannot allocate %zu bytes", key, want);
+        }
+        b.bytes = want;
+    }
+    *out = b.p;
+    return PG_OK;
+}
+
+pg_status pg_stream_pool(pg_ctx* ctx, size_t count)
+{
+    while (ctx->pool.size() < count) {
+        cudaStream_t st;
+        PG_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        ctx->pool.push_back(st);
+    }
     return PG_OK;
 }
 

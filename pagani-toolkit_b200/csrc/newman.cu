@@ -31,7 +31,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <string>
+#include <thread>
 
 namespace cg = cooperative_groups;
 
@@ -45,6 +47,19 @@ constexpr size_t SMEM_CAP = 220 * 1024;        // dynamic shared memory of a tea
 constexpr long long MEDIUM_EDGES = 1LL << 22;  // at most this many edges: one team per group
 constexpr int CLUSTER = 16;                    // largest team (CTAs of one cluster)
 constexpr long long MIN_CTA_EDGES = 8192;      // a team CTA keeps at least this many edges
+constexpr long long ASYNC_CTA_EDGES = 24576;   // dependency-driven phase: edges per team CTA before doubling
+constexpr int RESERVE_SMS = 8;                 // dependency-driven phase: SMs kept free of teams
+constexpr size_t POOL_STREAMS = 128;           // dependency-driven phase: streams made ahead
+// Per group results: lambda, it0, res0, it1, res1, subP, subN, shifted, and
+// the device clock (ns) when its team started and ended.
+constexpr int OUT_W = 10;
+
+__device__ __forceinline__ double nm_clock()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (double)t;
+}
 
 // In-group degree of every member (label of neighbour == label of node).
 __global__ void k_nm_gdeg(const int32_t* __restrict__ R, const int32_t* __restrict__ C,
@@ -65,7 +80,10 @@ __global__ void k_nm_gdeg(const int32_t* __restrict__ R, const int32_t* __restri
 // Induced CSR rows in CSR order, columns renumbered to the position of the
 // neighbour inside its group (the reference keeps original ids and a
 // node-indexed scatter array, which is the same arithmetic).  Group g's n+1
-// row offsets (relative to its first edge) sit at sR[goff[g] + g ...].
+// row offsets (relative to its first edge) sit at sR[2 goff[g] ...]: twice
+// the member offset, so that the offsets of groups nested inside one
+// another's member ranges (a group and the children of a finished sibling)
+// never overlap.
 __global__ void k_nm_gfill(const int32_t* __restrict__ R, const int32_t* __restrict__ C,
                            const int32_t* __restrict__ label, const int32_t* __restrict__ pos,
                            const int32_t* __restrict__ AD, int32_t P, const long long* __restrict__ soff,
@@ -76,11 +94,11 @@ __global__ void k_nm_gfill(const int32_t* __restrict__ R, const int32_t* __restr
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     for (int p = gw; p < P; p += nw) {
         const int i = AD[p], li = label[i], q = gidx[p];
-        const long long e0 = eoff[q];
+        const long long e0 = eoff[q], g0 = goff[q];
         long long w = soff[p];
         if (lane == 0) {
-            sR[p + q] = (int32_t)(w - e0);
-            if (p + 1 == goff[q + 1]) sR[p + q + 1] = (int32_t)(soff[p + 1] - e0);
+            sR[g0 + p] = (int32_t)(w - e0);
+            if (p + 1 == goff[q + 1]) sR[g0 + p + 1] = (int32_t)(soff[p + 1] - e0);
         }
         for (int32_t base = R[i]; base < R[i + 1]; base += 32) {
             int32_t e = base + lane;
@@ -107,6 +125,73 @@ __global__ void k_nm_gsumbg(const int32_t* __restrict__ R, const int32_t* __rest
         sumBG[p] = __dsub_rn((double)kg[p], t);
         kdeg[p] = (double)k;
     }
+}
+
+// Children of a split (dependency-driven phase): every member of the batch
+// gets its group's id as label and its position inside the group.
+__global__ void k_nm_gprep(const int32_t* __restrict__ AD, const int32_t* __restrict__ gidx,
+                           const long long* __restrict__ goff, int32_t P, int32_t id0, int32_t* __restrict__ label,
+                           int32_t* __restrict__ pos)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        const int q = gidx[p];
+        label[AD[p]] = id0 + q;
+        pos[AD[p]] = p - (int)goff[q];
+    }
+}
+
+// Exclusive prefix sum of the P in-group degrees in one CTA; soff[P] = total,
+// copied to pinned host memory (hsoff) before the host's flag is raised.
+__global__ void __launch_bounds__(1024) k_nm_gscan(const int32_t* __restrict__ kg, int32_t P,
+                                                   long long* __restrict__ soff, long long* __restrict__ hsoff,
+                                                   int* __restrict__ hready)
+{
+    __shared__ long long wsum[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    long long carry = 0;
+    for (int base = 0; base < P; base += blockDim.x) {
+        const int p = base + threadIdx.x;
+        const long long x = p < P ? kg[p] : 0;
+        long long sc = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, sc, o);
+            if (lane >= o) sc += y;
+        }
+        if (lane == 31) wsum[w] = sc;
+        __syncthreads();
+        if (w == 0) {
+            long long t = lane < nw ? wsum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            if (lane < nw) wsum[lane] = t;
+        }
+        __syncthreads();
+        if (p < P) {
+            const long long e = carry + (w ? wsum[w - 1] : 0) + sc - x;
+            soff[p] = e;
+            hsoff[p] = e;
+        }
+        carry += wsum[nw - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        soff[P] = carry;
+        hsoff[P] = carry;
+    }
+    // the same offsets in pinned host memory, then the host's flag
+    __threadfence_system();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence_system();
+        *(volatile int*)hready = 1;
+    }
+}
+
+__global__ void k_nm_iota(int32_t* __restrict__ x, int32_t n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = i;
 }
 
 // One group: rows are the group's members in ascending node id; sR holds
@@ -402,7 +487,7 @@ struct Inputs {
     const long long* goff;   // group start in member order (G+1)
     const long long* eoff;   // group start in edge order (G+1)
     const int32_t* AD;
-    const int32_t* sR;       // group g's n+1 row offsets start at goff[g] + g
+    const int32_t* sR;       // group g's n+1 row offsets start at 2 goff[g]
     const int32_t* sC;
     const double* kdeg;
     const double* sumBG;
@@ -414,6 +499,12 @@ struct Inputs {
     const float* wv;         // weighted tool: value array taken by position (null: unweighted)
     long long wn;
     double* out;             // per group: lambda, it0, res0, it1, res1, subP, subN, shifted
+    // dependency-driven phase (null otherwise): pinned host memory the teams
+    // write directly -- results per group, the final vector by member
+    // position, and a flag per group raised last
+    double* hout;
+    double* hv;
+    int* hdone;
 };
 
 __device__ __forceinline__ Group global_group(const Inputs& in, int gi)
@@ -422,7 +513,7 @@ __device__ __forceinline__ Group global_group(const Inputs& in, int gi)
     Group g;
     g.ng = (int)(in.goff[gi + 1] - p0);
     g.AD = in.AD + p0;
-    g.sR = in.sR + p0 + gi;
+    g.sR = in.sR + 2 * p0;
     g.sC = in.sC + in.eoff[gi];
     g.kdeg = in.kdeg + p0;
     g.sumBG = in.sumBG + p0;
@@ -452,7 +543,7 @@ __device__ void sub_partition(const Group& g, const Inputs& in, int gi, Red& red
     }
     red.sum(x, 2, ph);
     if (writer) {
-        double* o = in.out + (size_t)gi * 8;
+        double* o = in.out + (size_t)gi * OUT_W;
         o[0] = lam; o[1] = it0; o[2] = r0; o[3] = it1; o[4] = r1; o[5] = x[0]; o[6] = x[1]; o[7] = shifted;
     }
 }
@@ -892,6 +983,7 @@ k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes, uint16_t* __
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ Partials ps;
     __shared__ int sL, sIn;
+    const double t_start = nm_clock();
     cg::cluster_group cl = cg::this_cluster();
     const int nb = Kind::kCluster ? (int)cl.num_blocks() : 1, rank = Kind::kCluster ? (int)cl.block_rank() : 0;
     const int gi = glist[blockIdx.x / nb];
@@ -947,9 +1039,24 @@ k_nm_team(const int* __restrict__ glist, Inputs in, int smem_bytes, uint16_t* __
         x2[1] += tm.rep[p] <= 0.0;
     }
     block_sum(ps, x2, ph);
+    double o[OUT_W] = {lam, (double)it0, res0, (double)it1, res1, x2[0], x2[1], (double)shifted, t_start, 0.0};
     if (rank == 0 && threadIdx.x == 0) {
-        double* o = in.out + (size_t)gi * 8;
-        o[0] = lam; o[1] = it0; o[2] = res0; o[3] = it1; o[4] = res1; o[5] = x2[0]; o[6] = x2[1]; o[7] = shifted;
+        o[9] = nm_clock();
+        for (int k = 0; k < OUT_W; k++) in.out[(size_t)gi * OUT_W + k] = o[k];
+    }
+    if (in.hdone) {
+        // straight to the host: every CTA its own rows of the vector, then
+        // (after every CTA's system-scope fence and a team barrier) the
+        // results and the flag, so the host sees all of it once the flag is up
+        const long long p0 = in.goff[gi];
+        for (int lp = threadIdx.x; lp < tm.nown; lp += blockDim.x) in.hv[p0 + tm.r0 + lp] = tm.rep[tm.r0 + lp];
+        __threadfence_system();
+        Kind::barrier();
+        if (rank == 0 && threadIdx.x == 0) {
+            for (int k = 0; k < OUT_W; k++) in.hout[(size_t)gi * OUT_W + k] = o[k];
+            __threadfence_system();
+            *(volatile int*)(in.hdone + gi) = 1;
+        }
     }
 }
 
@@ -1199,7 +1306,7 @@ k_nm_grid(int gi, Inputs in, double* __restrict__ part, uint16_t* __restrict__ c
     }
     red.sum(x, 2, ph);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        double* o = in.out + (size_t)gi * 8;
+        double* o = in.out + (size_t)gi * OUT_W;
         o[0] = lam; o[1] = it0; o[2] = res0; o[3] = it1; o[4] = res1; o[5] = x[0]; o[6] = x[1]; o[7] = shifted;
     }
 }
@@ -1230,6 +1337,375 @@ __global__ void k_nm_q(const int32_t* __restrict__ R, const int32_t* __restrict_
     }
     if (lane == 0 && in) atomicAdd(inside, in);
 }
+
+// ------------------------------------------------------- dependency-driven phase
+// Once every pending group fits a team, groups stop waiting for the rest of
+// their generation.  Each group's power iteration is a launch of its own on
+// a stream of its own, and the team writes its results and final vector
+// straight into pinned host memory and then raises a flag there; the host
+// polls the flags, decides a group at once and, on a split, builds the two
+// children's sub-graphs and launches them.  (Host functions queued behind
+// the teams were tried first: a host function holds the hardware queue it
+// shares with other streams until the team before it ends, which delayed
+// unrelated launches by tens of ms.)  Labels are handed out afterwards by
+// replaying the reference's round order over the finished tree, so they are
+// those of the sequential reference.
+//
+// Buffers nest: a group owns member positions [s, s + n) and induced edges
+// [es, es + E); its children's positions and edges are subranges of those
+// (a child's induced edges are edges of its parent's sub-graph).  Arrays
+// with one entry per member (AD, gidx, kg, v, v0, kdeg, sumBG) are indexed
+// by position, the scan and sR of a batch (its n + 1 or n + 2 entries) at
+// twice the batch's first position; groups in flight own disjoint ranges,
+// so none of these overlap.  The member and edge offsets of a batch's two
+// groups are read by each team when it starts, which may be after its
+// sibling has ended and split at the same first position, so they sit in
+// slots of their own, four per batch.
+using TeamFn = void (*)(const int*, Inputs, int, uint16_t*);
+
+struct NmAsync {
+    struct Node {
+        int s = 0, n = 0;
+        long long es = 0, E = 0;
+        int c = 1;
+        int stream = -1;
+        int child = -1;        // tree index of the first child; the second follows
+        bool split = false;
+        int parent = -1;
+        double out[OUT_W] = {};
+        // launch arguments, kept while the group waits for SMs
+        Inputs in = {};
+        int gi = 0;
+        uint16_t* sl = nullptr;
+        cudaEvent_t dep = nullptr;   // the stream waits for this event first
+    };
+    struct Batch {
+        int s, P, nA, first, stream;
+        long long es;
+    };
+    pg_ctx* ctx;
+    const pg_graph* g;
+    TeamFn k_solo, k_clu;
+    Inputs base;               // M, err_sq, gpu_rule_above, weights
+    int lo;                    // device label of tree index 0
+    size_t smem_cap;
+    int max_cluster;
+    long long cta_edges;       // a team doubles its CTAs while each holds more edges than this
+    const int32_t* hR;
+    int32_t *label, *pos, *AD, *gidx, *kg, *sR, *sC, *iota;
+    long long *agoff, *aeoff, *asoff, *ainner;
+    double *v, *v0, *sumBG, *kdeg, *aout;
+    uint16_t* slices;
+    int32_t *hAD, *hgidx;
+    long long *hsoff, *hgoff, *heoff, *hinner;
+    double *hv, *hout;
+    std::vector<Node> tree;
+    std::vector<Batch> batches;
+    // pinned host flags raised by the device: a team's end (per tree node)
+    // and a batch's scan (per batch)
+    int *hdone, *hready;
+    // the same pinned buffers as the device addresses them
+    double *dhout, *dhv;
+    long long* dhsoff;
+    int *dhdone, *dhready;
+
+    pg_status map_pinned()
+    {
+        PG_CUDA(ctx, cudaHostGetDevicePointer((void**)&dhout, hout, 0));
+        PG_CUDA(ctx, cudaHostGetDevicePointer((void**)&dhv, hv, 0));
+        PG_CUDA(ctx, cudaHostGetDevicePointer((void**)&dhsoff, hsoff, 0));
+        PG_CUDA(ctx, cudaHostGetDevicePointer((void**)&dhdone, hdone, 0));
+        PG_CUDA(ctx, cudaHostGetDevicePointer((void**)&dhready, hready, 0));
+        return PG_OK;
+    }
+    std::vector<int> free_streams, running, waiting, queued;
+    std::vector<cudaEvent_t> events;
+    // team CTAs in flight and their cap: a team CTA holds a whole SM
+    // (registers and shared memory), so SMs beyond the cap stay free for the
+    // small kernels that build the next children; without it those kernels
+    // queued behind the teams for tens of ms
+    int inflight = 0, budget = 0;
+
+    pg_status take_stream(int* out)
+    {
+        if (!free_streams.empty()) {
+            *out = free_streams.back();
+            free_streams.pop_back();
+            return PG_OK;
+        }
+        PG_TRY(pg_stream_pool(ctx, ctx->pool.size() + 1));
+        *out = (int)ctx->pool.size() - 1;
+        return PG_OK;
+    }
+
+    // CTAs of a group's team: the fewest whose shared memory holds the
+    // group, doubled while each CTA keeps more than cta_edges edges.  A
+    // function of the group alone, so results do not depend on timing.
+    int pick_cluster(const long long* so, int n) const
+    {
+        std::vector<int32_t> rel(n + 1);
+        for (int p = 0; p <= n; p++) rel[p] = (int32_t)(so[p] - so[0]);
+        auto need = [&](int c) {
+            size_t m = 0;
+            for (int r = 0; r < c; r++) {
+                const int a = team_split(rel.data(), n, r, c), b = team_split(rel.data(), n, r + 1, c);
+                m = std::max(m, team_layout(n, b - a).need_min);
+            }
+            return m;
+        };
+        int c = 0;
+        for (int cc = 1; cc <= max_cluster && !c; cc *= 2)
+            if (need(cc) <= smem_cap) c = cc;
+        while (c && c * 2 <= max_cluster && (long long)rel[n] / c > cta_edges) c *= 2;
+        return c;
+    }
+
+    // Queued groups start in the order they became ready, each as soon as
+    // its CTAs fit under the cap (a later, smaller team may pass a larger
+    // one that does not fit yet).  Replaying measured group times through
+    // a model of this loop, first-ready-first beat most-edges-first by
+    // 10-15 % of the phase: the small groups it held back sat on long chains.
+    pg_status pump()
+    {
+        size_t keep = 0;
+        for (size_t k = 0; k < queued.size(); k++) {
+            const int t = queued[k];
+            if (inflight + tree[t].c <= budget) PG_TRY(launch_group(t));
+            else queued[keep++] = t;
+        }
+        queued.resize(keep);
+        return PG_OK;
+    }
+
+    pg_status launch_group(int t)
+    {
+        if (tree[t].stream < 0) PG_TRY(take_stream(&tree[t].stream));
+        const Node nd = tree[t];
+        cudaStream_t st = ctx->pool[nd.stream];
+        if (nd.dep) PG_CUDA(ctx, cudaStreamWaitEvent(st, nd.dep, 0));
+        inflight += nd.c;
+        const Inputs& in = nd.in;
+        uint16_t* sl = nd.sl;
+        const int* gl = iota + nd.gi;
+        if (nd.c == 1) {
+            k_solo<<<1, TEAM_THREADS, smem_cap, st>>>(gl, in, (int)smem_cap, sl);
+        } else {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = nd.c;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3((unsigned)nd.c);
+            cfg.blockDim = dim3(TEAM_THREADS);
+            cfg.dynamicSmemBytes = smem_cap;
+            cfg.stream = st;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            PG_CUDA(ctx, cudaLaunchKernelEx(&cfg, k_clu, gl, in, (int)smem_cap, sl));
+        }
+        PG_LAUNCHED(ctx);
+        running.push_back(t);
+        return PG_OK;
+    }
+
+    // Group t has ended: decide it as Sub_Partition does and, on a split,
+    // start building the children (members partitioned stably by the sign
+    // rule of the relabelling, Modularity_CPU.cpp:126-151).
+    pg_status finish(int t)
+    {
+        inflight -= tree[t].c;
+        std::memcpy(tree[t].out, hout + (size_t)OUT_W * t, sizeof tree[t].out);
+        const double* o = tree[t].out;
+        const long long subP = (long long)o[5], subN = (long long)o[6];
+        tree[t].split = o[0] > LAMBDA && subP > 1 && subN > 1;
+        if (!tree[t].split) {
+            free_streams.push_back(tree[t].stream);
+            return PG_OK;
+        }
+        const double coef = (double)(subP - subN) + 0.5;
+        const int s = tree[t].s, n = tree[t].n;
+        std::vector<int32_t> second;
+        int nA = 0;
+        long long degA = 0, degB = 0;
+        for (int p = 0; p < n; p++) {
+            const int32_t id = hAD[s + p];
+            const long long d = hR[id + 1] - hR[id];
+            if (hv[s + p] * coef > 0.0) {
+                hAD[s + nA++] = id;
+                degA += d;
+            } else {
+                second.push_back(id);
+                degB += d;
+            }
+        }
+        for (int p = 0; p < n; p++) hgidx[s + p] = p < nA ? 0 : 1;
+        std::memcpy(hAD + s + nA, second.data(), sizeof(int32_t) * second.size());
+        const size_t b4 = 4 * batches.size();   // the batch's own offsets (read by its teams when they start)
+        hgoff[b4] = 0;
+        hgoff[b4 + 1] = nA;
+        hgoff[b4 + 2] = n;
+        hinner[s] = degA;
+        hinner[s + 1] = degB;
+        const int first = (int)tree.size();
+        Node a, b;
+        a.s = s;
+        a.n = nA;
+        b.s = s + nA;
+        b.n = n - nA;
+        a.parent = b.parent = t;
+        tree[t].child = first;
+        tree.push_back(a);
+        tree.push_back(b);
+        Batch bt{s, n, nA, first, tree[t].stream, tree[t].es};
+        const int bi = (int)batches.size();
+        batches.push_back(bt);
+        cudaStream_t st = ctx->pool[bt.stream];
+        PG_CUDA(ctx, cudaMemcpyAsync(AD + s, hAD + s, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+        PG_CUDA(ctx, cudaMemcpyAsync(gidx + s, hgidx + s, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+        PG_CUDA(ctx, cudaMemcpyAsync(agoff + b4, hgoff + b4, 3 * sizeof(long long),
+                                     cudaMemcpyHostToDevice, st));
+        PG_CUDA(ctx, cudaMemcpyAsync(ainner + s, hinner + s, 2 * sizeof(long long), cudaMemcpyHostToDevice, st));
+        const int blocks = std::max(1, std::min((n + 255) / 256, ctx->sm_count));
+        k_nm_gprep<<<blocks, 256, 0, st>>>(AD + s, gidx + s, agoff + b4, n, lo + first, label, pos);
+        PG_LAUNCHED(ctx);
+        const int wblocks = std::max(1, std::min((n + 7) / 8, ctx->sm_count * 4));
+        k_nm_gdeg<<<wblocks, 256, 0, st>>>(g->R, g->C, label, AD + s, n, kg + s);
+        PG_LAUNCHED(ctx);
+        k_nm_gscan<<<1, 1024, 0, st>>>(kg + s, n, asoff + 2 * (size_t)s, dhsoff + 2 * (size_t)s, dhready + bi);
+        PG_LAUNCHED(ctx);
+        waiting.push_back(bi);
+        return PG_OK;
+    }
+
+    // The children's in-group degrees are known: fill their sub-graphs and
+    // launch both power iterations.
+    pg_status start_batch(int bi)
+    {
+        const Batch bt = batches[bi];
+        const size_t s = bt.s, s2 = 2 * s;
+        const long long* so = hsoff + s2;
+        const long long EA = so[bt.nA], EB = so[bt.P] - so[bt.nA];
+        const size_t b4 = 4 * (size_t)bi;
+        heoff[b4] = 0;
+        heoff[b4 + 1] = EA;
+        heoff[b4 + 2] = EA + EB;
+        Node& a = tree[bt.first];
+        Node& b = tree[bt.first + 1];
+        a.es = bt.es;
+        a.E = EA;
+        b.es = bt.es + EA;
+        b.E = EB;
+        a.c = pick_cluster(so, bt.nA);
+        b.c = pick_cluster(so + bt.nA, bt.P - bt.nA);
+        if (!a.c || !b.c) return pg_fail(ctx, PG_ERR_INTERNAL, "modularity: a child group does not fit a team");
+        cudaStream_t st = ctx->pool[bt.stream];
+        PG_CUDA(ctx, cudaMemcpyAsync(aeoff + b4, heoff + b4, 3 * sizeof(long long), cudaMemcpyHostToDevice, st));
+        const int wblocks = std::max(1, std::min((bt.P + 7) / 8, ctx->sm_count * 4));
+        k_nm_gfill<<<wblocks, 256, 0, st>>>(g->R, g->C, label, pos, AD + s, bt.P, asoff + s2, agoff + b4, aeoff + b4,
+                                            gidx + s, sR + s2, sC + bt.es);
+        PG_LAUNCHED(ctx);
+        const int blocks = std::max(1, std::min((bt.P + 255) / 256, ctx->sm_count));
+        k_nm_gsumbg<<<blocks, 256, 0, st>>>(g->R, AD + s, kg + s, gidx + s, ainner + s, bt.P, base.M, sumBG + s,
+                                            kdeg + s);
+        PG_LAUNCHED(ctx);
+        cudaEvent_t ev;
+        PG_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        events.push_back(ev);
+        PG_CUDA(ctx, cudaEventRecord(ev, st));
+        Inputs in = base;
+        in.goff = agoff + b4;
+        in.eoff = aeoff + b4;
+        in.AD = AD + s;
+        in.sR = sR + s2;
+        in.sC = sC + bt.es;
+        in.kdeg = kdeg + s;
+        in.sumBG = sumBG + s;
+        in.v = v + s;
+        in.v0 = v0 + s;
+        in.out = aout + (size_t)OUT_W * bt.first;
+        in.hout = dhout + (size_t)OUT_W * bt.first;
+        in.hv = dhv + s;
+        in.hdone = dhdone + bt.first;
+        uint16_t* sl = slices + 2 * bt.es + 64 * (long long)s;
+        for (int k = 0; k < 2; k++) {
+            Node& nd = tree[bt.first + k];
+            nd.in = in;
+            nd.gi = k;
+            nd.sl = sl;
+            nd.stream = k == 0 ? bt.stream : -1;   // the first child runs behind its sub-graph's kernels
+            nd.dep = k == 0 ? nullptr : ev;
+            queued.push_back(bt.first + k);
+        }
+        return PG_OK;
+    }
+
+    pg_status loop()
+    {
+        // a flag that never rises (a failed kernel) must not spin forever:
+        // while nothing moves, the streams of the running teams are queried
+        // now and then, and 120 s without progress is an error
+        auto last = std::chrono::steady_clock::now();
+        long long idle = 0;
+        while (!running.empty() || !waiting.empty() || !queued.empty()) {
+            PG_TRY(pump());
+            bool any = false;
+            for (size_t i = 0; i < running.size();) {
+                const int t = running[i];
+                if (__atomic_load_n(&hdone[t], __ATOMIC_ACQUIRE)) {
+                    running[i] = running.back();
+                    running.pop_back();
+                    PG_TRY(finish(t));
+                    any = true;
+                } else {
+                    i++;
+                }
+            }
+            for (size_t i = 0; i < waiting.size();) {
+                const int bi = waiting[i];
+                if (__atomic_load_n(&hready[bi], __ATOMIC_ACQUIRE)) {
+                    waiting[i] = waiting.back();
+                    waiting.pop_back();
+                    PG_TRY(start_batch(bi));
+                    any = true;
+                } else {
+                    i++;
+                }
+            }
+            if (any) {
+                idle = 0;
+                last = std::chrono::steady_clock::now();
+                continue;
+            }
+            if (++idle % 4096 == 0) {
+                for (int t : running) {
+                    const cudaError_t e = cudaStreamQuery(ctx->pool[tree[t].stream]);
+                    if (e != cudaSuccess && e != cudaErrorNotReady)
+                        return pg_fail(ctx, PG_ERR_CUDA, "modularity: team of group %d: %s", t, cudaGetErrorString(e));
+                }
+                cudaGetLastError();   // not-ready answers are not errors
+                if (std::chrono::steady_clock::now() - last > std::chrono::seconds(120))
+                    return pg_fail(ctx, PG_ERR_TIMEOUT, "modularity: no team ended for 120 s");
+            }
+            std::this_thread::yield();
+        }
+        return PG_OK;
+    }
+
+    // Runs the tree below the initial groups to the end; on an error waits
+    // for the work in flight (its host functions write into this object).
+    pg_status run()
+    {
+        pg_status st = loop();
+        const cudaError_t e = cudaDeviceSynchronize();
+        for (cudaEvent_t ev : events) cudaEventDestroy(ev);
+        events.clear();
+        if (st != PG_OK) return st;
+        if (e != cudaSuccess)
+            return pg_fail(ctx, PG_ERR_CUDA, "modularity: dependency-driven phase: %s", cudaGetErrorString(e));
+        return PG_OK;
+    }
+};
 }  // namespace
 
 // The partition of pg_newman; wv (device, wn values) is the weighted tool's
@@ -1278,6 +1754,27 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
     PG_TRY(pg_wst(ctx, "nm.c16", (size_t)nnz + 8, &c16));
     uint16_t* slices;   // team CTAs whose sliced rows do not fit shared memory
     PG_TRY(pg_wst(ctx, "nm.slices", (size_t)2 * nnz + 64 * (size_t)n + 64, &slices));
+    PG_TRY(pg_wst(ctx, "nm.sR", 2 * (size_t)n + 4, &sR));   // n+1 offsets per group at twice its first member
+    // dependency-driven phase: every buffer is taken here, before any of its
+    // streams runs (growing a buffer later would free it under them)
+    NmAsync as;
+    const size_t max_nodes = 2 * (size_t)n + 4;   // tree nodes of the phase (initial groups and children)
+    PG_TRY(pg_wst(ctx, "nm.agoff", 4 * (size_t)n + 8, &as.agoff));   // 4 per batch (one batch per split)
+    PG_TRY(pg_wst(ctx, "nm.aeoff", 4 * (size_t)n + 8, &as.aeoff));
+    PG_TRY(pg_wst(ctx, "nm.asoff", 2 * (size_t)n + 4, &as.asoff));
+    PG_TRY(pg_wst(ctx, "nm.ainner", (size_t)n + 4, &as.ainner));
+    PG_TRY(pg_wst(ctx, "nm.aout", OUT_W * max_nodes, &as.aout));
+    PG_TRY(pg_wst(ctx, "nm.iota", (size_t)n + 4, &as.iota));
+    PG_TRY(pg_hwst(ctx, "nm.hAD", (size_t)n + 4, &as.hAD));
+    PG_TRY(pg_hwst(ctx, "nm.hgidx", (size_t)n + 4, &as.hgidx));
+    PG_TRY(pg_hwst(ctx, "nm.hsoff", 2 * (size_t)n + 4, &as.hsoff));
+    PG_TRY(pg_hwst(ctx, "nm.hgoff", 4 * (size_t)n + 8, &as.hgoff));
+    PG_TRY(pg_hwst(ctx, "nm.heoff", 4 * (size_t)n + 8, &as.heoff));
+    PG_TRY(pg_hwst(ctx, "nm.hinner", (size_t)n + 4, &as.hinner));
+    PG_TRY(pg_hwst(ctx, "nm.hv", (size_t)n + 4, &as.hv));
+    PG_TRY(pg_hwst(ctx, "nm.hout", OUT_W * max_nodes, &as.hout));
+    PG_TRY(pg_hwst(ctx, "nm.hdone", max_nodes, &as.hdone));
+    PG_TRY(pg_hwst(ctx, "nm.hready", (size_t)n + 4, &as.hready));
     int max_cluster = CLUSTER;  // 16 needs the non-portable opt-in
     if (cudaFuncSetAttribute(k_clu, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
@@ -1307,9 +1804,15 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
     char line[512];
     std::vector<int32_t> hAD(n), hgidx(n), hpos(n, 0);
     // wall time per kind of power-iteration launch, reported in the log
-    double t_small = 0, t_large = 0, t_setup = 0;
-    long long it_small = 0, it_large = 0;
+    double t_small = 0, t_large = 0, t_setup = 0, t_async = 0;
+    long long it_small = 0, it_large = 0, it_async = 0;
     int generations = 0;
+    // dependency-driven phase: device label of tree index 0 (-1: not reached),
+    // round of every tree node, labels in use
+    int async_lo = -1, label_bound = 0, async_groups = 0, chain_groups = 0;
+    double chain_ms = 0.0, span_ms = 0.0, busy_ctas = 0.0;
+    std::vector<int> ref_of;
+    const long long async_cta_edges = ASYNC_CTA_EDGES;
     auto now = [] { return std::chrono::steady_clock::now(); };
     auto ms_since = [&](std::chrono::steady_clock::time_point t0) {
         return std::chrono::duration<double, std::milli>(now() - t0).count();
@@ -1338,11 +1841,10 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 }
         }
         if (P == 0) { Round = hi + 1; continue; }
-        PG_TRY(pg_wst(ctx, "nm.sR", (size_t)P + G + 2, &sR));   // n+1 offsets per group
         PG_TRY(pg_wst(ctx, "nm.goff", (size_t)G + 1, &goff));
         PG_TRY(pg_wst(ctx, "nm.eoff", (size_t)G + 1, &eoff));
         PG_TRY(pg_wst(ctx, "nm.inner", (size_t)G, &innerM));
-        PG_TRY(pg_wst(ctx, "nm.out", (size_t)G * 8, &out));
+        PG_TRY(pg_wst(ctx, "nm.out", (size_t)G * OUT_W, &out));
         PG_TRY(pg_wst(ctx, "nm.glist", (size_t)G, &glist));
         PG_TRY(pg_wst(ctx, "nm.base", (size_t)G, &dbase));
         PG_TRY(pg_wst(ctx, "nm.coef", (size_t)G, &dcoef));
@@ -1371,6 +1873,7 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
         in.goff = goff; in.eoff = eoff; in.AD = AD; in.sR = sR; in.sC = sC; in.kdeg = kdeg; in.sumBG = sumBG;
         in.v = v; in.v0 = v0; in.M = M; in.gpu_rule_above = gpu_rule_above; in.out = out; in.err_sq = err_sq;
         in.wv = wv; in.wn = wn;
+        in.hout = nullptr; in.hv = nullptr; in.hdone = nullptr;
         // Shared memory of the largest CTA of group q split over c CTAs,
         // before its sliced columns
         auto team_need = [&](int q, int c) {
@@ -1425,6 +1928,119 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 csz[best] *= 2;
             }
         }
+        if (large.empty()) {
+            // ---- every pending group fits a team: dependency-driven from here on
+            auto t_as = now();
+            as.ctx = ctx;
+            as.g = g;
+            as.k_solo = k_solo;
+            as.k_clu = k_clu;
+            as.base = in;
+            as.base.out = as.aout;
+            as.lo = lo;
+            as.smem_cap = smem_cap;
+            as.max_cluster = max_cluster;
+            as.cta_edges = async_cta_edges;
+            as.hR = hR.data();
+            as.label = label; as.pos = pos; as.AD = AD; as.gidx = gidx; as.kg = kg; as.sR = sR; as.sC = sC;
+            as.v = v; as.v0 = v0; as.sumBG = sumBG; as.kdeg = kdeg; as.slices = slices;
+            k_nm_iota<<<ctx->sm_count, 256, 0, ctx->stream>>>(as.iota, n + 4);
+            PG_LAUNCHED(ctx);
+            PG_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+            std::memcpy(as.hAD, hAD.data(), sizeof(int32_t) * P);
+            // streams are created here, with the device idle: creating one
+            // while teams run blocked the host for up to ~100 ms
+            PG_TRY(pg_stream_pool(ctx, POOL_STREAMS));
+            for (int k = (int)ctx->pool.size() - 1; k >= 0; k--) as.free_streams.push_back(k);
+            PG_TRY(as.map_pinned());
+            std::memset(as.hdone, 0, sizeof(int) * max_nodes);
+            std::memset(as.hready, 0, sizeof(int) * ((size_t)n + 4));
+            Inputs in0 = in;
+            in0.out = as.aout;
+            in0.hout = as.dhout;
+            in0.hv = as.dhv;
+            in0.hdone = as.dhdone;
+            for (int q = 0; q < G; q++) {
+                NmAsync::Node nd;
+                nd.s = (int)hgoff[q];
+                nd.n = (int)(hgoff[q + 1] - hgoff[q]);
+                nd.es = heoff[q];
+                nd.E = heoff[q + 1] - heoff[q];
+                as.tree.push_back(nd);
+            }
+            as.budget = std::max(max_cluster, ctx->sm_count - RESERVE_SMS);
+            for (int q = 0; q < G; q++) {
+                NmAsync::Node& nd = as.tree[q];
+                if (nd.n == 0) continue;
+                nd.c = as.pick_cluster(&hsoff[hgoff[q]], nd.n);
+                if (!nd.c) return pg_fail(ctx, PG_ERR_INTERNAL, "modularity: a group does not fit a team");
+                nd.in = in0;
+                nd.gi = q;
+                nd.sl = slices;
+                nd.dep = ctx->ev[0];
+                as.queued.push_back(q);
+            }
+            PG_TRY(as.run());
+            t_async += ms_since(t_as);
+            // ---- the reference's rounds over the finished tree, in order
+            std::vector<int> round_tree((size_t)hi + as.tree.size() + 4, -1);
+            for (int q = 0; q < G; q++)
+                if (as.tree[q].n > 0) round_tree[lo + q] = q;
+            ref_of.assign(as.tree.size(), -1);
+            for (int round = lo; round <= Max_Result; round++) {
+                const int t = round_tree[round];
+                if (t < 0) continue;
+                ref_of[t] = round;
+                const NmAsync::Node& nd = as.tree[t];
+                const double* o = nd.out;
+                it_async += (long long)(o[1] + o[3]);
+                if (log) {
+                    int len = snprintf(line, sizeof line, "Round:\t%d\tnumber of nodes:\t%d\tIterations:\t%d\tresidual:\t%g\t",
+                                       round, nd.n, (int)o[1], o[2]);
+                    if (o[7] != 0.0)
+                        len += snprintf(line + len, sizeof line - len, "Iterations:\t%d\tresidual:\t%g\t", (int)o[3], o[4]);
+                    snprintf(line + len, sizeof line - len, "Eigen Value: %g\tDivide?: %d", o[0], (int)nd.split);
+                    log(line, user);
+                }
+                if (nd.split) {
+                    round_tree[Max_Result + 1] = nd.child;
+                    round_tree[Max_Result + 2] = nd.child + 1;
+                    Max_Result += 2;
+                } else {
+                    if (round >= (int)adjust.size()) adjust.resize(round + 1, 0);
+                    adjust[round] = Index++;
+                }
+                Module_Num += nd.split;
+            }
+            // the chain of groups that ended last: its run time against the
+            // phase's span shows what waiting for SMs and the host costs
+            {
+                double t_begin = 1e300, t_end = 0.0, busy = 0.0;
+                int last = -1;
+                for (size_t t = 0; t < as.tree.size(); t++) {
+                    const NmAsync::Node& nd = as.tree[t];
+                    if (nd.n == 0) continue;
+                    t_begin = std::min(t_begin, nd.out[8]);
+                    if (nd.out[9] > t_end) {
+                        t_end = nd.out[9];
+                        last = (int)t;
+                    }
+                    busy += nd.c * (nd.out[9] - nd.out[8]);
+                }
+                for (int t = last; t >= 0; t = as.tree[t].parent) {
+                    chain_groups++;
+                    chain_ms += (as.tree[t].out[9] - as.tree[t].out[8]) * 1e-6;
+                }
+                if (last >= 0) {
+                    span_ms = (t_end - t_begin) * 1e-6;
+                    busy_ctas = busy / (t_end - t_begin);
+                }
+            }
+            async_lo = lo;
+            label_bound = std::max(Max_Result, lo + (int)as.tree.size());
+            async_groups = (int)as.tree.size();
+            break;
+        }
         // glist by cluster size, largest first; one launch per size
         std::vector<int> lists;
         struct Bucket { int c; size_t b, e; size_t smem; };
@@ -1437,7 +2053,7 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
             bk.e = lists.size();
             if (bk.e > bk.b) buckets.push_back(bk);
         }
-        std::vector<double> hout((size_t)G * 8, 0.0);
+        std::vector<double> hout((size_t)G * OUT_W, 0.0);
         if (!lists.empty())
             PG_CUDA(ctx, cudaMemcpyAsync(glist, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice,
                                          ctx->stream));
@@ -1505,10 +2121,10 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
             }
             PG_LAUNCHED(ctx);
         }
-        PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * 8));
+        PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * OUT_W));
         t_large += ms_since(t0);
-        for (int q : team) it_small += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
-        for (int q : large) it_large += (long long)(hout[(size_t)q * 8 + 1] + hout[(size_t)q * 8 + 3]);
+        for (int q : team) it_small += (long long)(hout[(size_t)q * OUT_W + 1] + hout[(size_t)q * OUT_W + 3]);
+        for (int q : large) it_large += (long long)(hout[(size_t)q * OUT_W + 1] + hout[(size_t)q * OUT_W + 3]);
         // ---- decisions in round order (labels exactly as the sequential reference)
         std::vector<int> hbase(G, -1);
         std::vector<double> hcoef(G, 0.0);
@@ -1517,7 +2133,7 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
             const int round = lo + q;
             const long long ng = hgoff[q + 1] - hgoff[q];
             if (ng == 0) continue;
-            const double* o = &hout[(size_t)q * 8];
+            const double* o = &hout[(size_t)q * OUT_W];
             const long long subP = (long long)o[5], subN = (long long)o[6];
             const bool issub = o[0] > LAMBDA && subP > 1 && subN > 1;
             if (log) {
@@ -1549,21 +2165,25 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
         Round = hi + 1;
     }
     // Q from module degree sums (Modularity_CPU.cpp:116-124 in closed form)
+    label_bound = std::max(label_bound, Max_Result);
     unsigned long long* Kc;
-    PG_TRY(pg_wst(ctx, "nm.Kc", (size_t)Max_Result + 4, &Kc));
-    PG_CUDA(ctx, cudaMemsetAsync(Kc, 0, sizeof(unsigned long long) * (Max_Result + 2), ctx->stream));
+    PG_TRY(pg_wst(ctx, "nm.Kc", (size_t)label_bound + 4, &Kc));
+    PG_CUDA(ctx, cudaMemsetAsync(Kc, 0, sizeof(unsigned long long) * (label_bound + 2), ctx->stream));
     PG_CUDA(ctx, cudaMemsetAsync(acc, 0, sizeof(unsigned long long), ctx->stream));
     k_nm_q<<<grid, 256, 0, ctx->stream>>>(g->R, g->C, label, n, acc, Kc);
     PG_LAUNCHED(ctx);
     unsigned long long inside = 0;
-    std::vector<unsigned long long> K(Max_Result + 1);
+    std::vector<unsigned long long> K(label_bound + 1);
     PG_TRY(pg_d2h(ctx, &inside, acc, sizeof inside));
-    PG_TRY(pg_d2h(ctx, K.data(), Kc, sizeof(unsigned long long) * (Max_Result + 1)));
+    PG_TRY(pg_d2h(ctx, K.data(), Kc, sizeof(unsigned long long) * (label_bound + 1)));
     double sq = 0.0;
-    for (int c = 0; c <= Max_Result; c++) sq += (double)K[c] * (double)K[c];
+    for (int c = 0; c <= label_bound; c++) sq += (double)K[c] * (double)K[c];
     const double q = ((double)inside - sq / 2 / M) / (2.0 * M);
     PG_TRY(pg_d2h(ctx, hl.data(), label, sizeof(int32_t) * n));
-    for (int i = 0; i < n; i++) labels[i] = adjust[hl[i]];
+    for (int i = 0; i < n; i++) {
+        const int l = hl[i];
+        labels[i] = adjust[async_lo >= 0 && l >= async_lo ? ref_of[l - async_lo] : l];
+    }
     if (Q) *Q = q;
     if (n_modules) *n_modules = Module_Num;
     if (log) {
@@ -1571,8 +2191,10 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
         log(line, user);
         snprintf(line, sizeof line,
                  "Timing (ms): generations %d, setup %.1f, team groups %.1f (%lld iterations), "
-                 "cooperative groups %.1f (%lld)",
-                 generations, t_setup, t_small, it_small, t_large, it_large);
+                 "cooperative groups %.1f (%lld), dependency-driven phase %.1f (%d groups, %lld iterations; "
+                 "device span %.1f, last chain %d groups running %.1f, mean team CTAs busy %.1f)",
+                 generations, t_setup, t_small, it_small, t_large, it_large, t_async, async_groups, it_async, span_ms,
+                 chain_groups, chain_ms, busy_ctas);
         log(line, user);
     }
     return PG_OK;

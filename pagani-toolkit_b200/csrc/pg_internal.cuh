@@ -26,6 +26,10 @@ struct pg_ctx {
     // Pinned host staging for small D2H/H2D transfers.
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // Pinned host buffers keyed by name, grown on demand, and a pool of
+    // non-blocking streams: for host loops that keep many streams busy.
+    std::map<std::string, Buf> hws;
+    std::vector<cudaStream_t> pool;
     // Optional per-kernel device time (pg_profile_enable): event pairs around
     // the launches of named kernels, resolved when read.
     bool prof = false;
@@ -95,6 +99,16 @@ inline pg_status pg_wst(pg_ctx* ctx, const char* key, size_t count, T** out)
 }
 // Pinned host staging buffer of at least `bytes`.
 pg_status pg_pinned(pg_ctx* ctx, size_t bytes, void** out);
+// Pinned host buffer named `key`, at least `bytes` long (contents undefined;
+// growing it synchronises the device).
+pg_status pg_hws(pg_ctx* ctx, const char* key, size_t bytes, void** out);
+template <class T>
+inline pg_status pg_hwst(pg_ctx* ctx, const char* key, size_t count, T** out)
+{
+    return pg_hws(ctx, key, count * sizeof(T) + 256, (void**)out);
+}
+// At least `count` streams in ctx->pool.
+pg_status pg_stream_pool(pg_ctx* ctx, size_t count);
 
 // Copies between host and device on the context stream, synchronous.
 pg_status pg_d2h(pg_ctx* ctx, void* dst, const void* src, size_t bytes);
