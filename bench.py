@@ -732,9 +732,9 @@ def run(args):
                                        "launches of one batch at 58k (profiles/k_brandes_subject58k.md)",
                      "bound_note": "the DRAM traffic is 0.065 of the algorithmic bytes: batching shares every "
                                    "CSR read among 128 sources and the per-node state is served by L2; ncu on the "
-                                   "16k subject (profiles/k_brandes_subject16k.md) shows L2 hit rate 96.6 %, issue "
-                                   "active 50.9 % and long-scoreboard stalls on top -- issue and L2 latency bound "
-                                   "the sweep, not HBM",
+                                   "16k subject (profiles/k_brandes_subject16k.md) shows L2 hit rate 92.2 %, L2 "
+                                   "throughput 18.1 %, issue active 39.2 % and long-scoreboard then barrier stalls "
+                                   "on top -- L2 latency and the level barriers bound the sweep, not HBM",
                      "algorithmic_bytes_per_launch": bytes_batch,
                      "per_launch": "one 128-source batch (its k_brandes launches); algorithmic bytes of the "
                                    "backward sweep only",

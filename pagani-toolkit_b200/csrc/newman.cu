@@ -48,7 +48,7 @@ constexpr long long MEDIUM_EDGES = 1LL << 22;  // at most this many edges: one t
 constexpr int CLUSTER = 16;                    // largest team (CTAs of one cluster)
 constexpr long long MIN_CTA_EDGES = 8192;      // a team CTA keeps at least this many edges
 constexpr long long ASYNC_CTA_EDGES = 24576;   // dependency-driven phase: edges per team CTA before doubling
-constexpr int RESERVE_SMS = 8;                 // dependency-driven phase: SMs kept free of teams
+constexpr int RESERVE_SMS = 4;                 // dependency-driven phase: SMs kept free of teams
 constexpr size_t POOL_STREAMS = 128;           // dependency-driven phase: streams made ahead
 // Per group results: lambda, it0, res0, it1, res1, subP, subN, shifted, and
 // the device clock (ns) when its team started and ended.
