@@ -44,6 +44,7 @@
 #include "maslov.cuh"
 #include <algorithm>
 #include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
 
 namespace cg = cooperative_groups;
 
@@ -159,6 +160,23 @@ __device__ __forceinline__ uint64_t stream_bits(uint64_t key, uint64_t q)
     return mix64(key + q * 0x9E3779B97F4A7C15ULL);
 }
 
+// Defers attempt a to the next round.  The threads deferring together
+// append with one atomic (their order in the list does not matter: claims
+// are ordered by attempt index), and fold the oldest deferred attempt with
+// one atomicMin; one atomic per deferred attempt on these two counters
+// serialised in L2.
+__device__ __forceinline__ void ms_defer(unsigned long long a, unsigned long long base, MsControl* st, int slot,
+                                         unsigned long long* pnext)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long at = 0;
+    if (g.thread_rank() == 0) at = atomicAdd(&st->n_pending[slot], (unsigned long long)g.size());
+    at = g.shfl(at, 0) + g.thread_rank();
+    pnext[at] = a;
+    const unsigned rel = cg::reduce(g, (unsigned)(a - base), cg::less<unsigned>());
+    if (g.thread_rank() == 0) atomicMin(&st->oldest[slot], base + rel);
+}
+
 __global__ void __launch_bounds__(MS_THREADS)
 k_ms_rounds(MsArgs p)
 {
@@ -176,6 +194,7 @@ k_ms_rounds(MsArgs p)
     // this round's entries are below every older one and nothing needs to be
     // cleared between rounds.
     unsigned long long fresh = 0;
+    unsigned long long committed = 0;   // this thread's commits, added once at the end
     for (uint32_t round = 0;; round++) {
         const int cur = round & 1;
         const unsigned long long np = vst->n_pending[cur];
@@ -223,8 +242,7 @@ k_ms_rounds(MsArgs p)
             const unsigned long long me = tag | (uint32_t)(t.a - base);
             if (!(p.slot_owner[t.i] == me && p.slot_owner[t.j] == me && p.table[t.h[0]] == me &&
                   p.table[t.h[1]] == me)) {
-                pnext[atomicAdd(&p.st->n_pending[cur ^ 1], 1ULL)] = t.a;
-                atomicMin(&p.st->oldest[cur ^ 1], t.a);
+                ms_defer(t.a, base, p.st, cur ^ 1, pnext);
                 continue;
             }
             atomicMin(&p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)], me);   // the pairs it removes
@@ -245,8 +263,7 @@ k_ms_rounds(MsArgs p)
             }
             mine++;
         }
-        mine = __reduce_add_sync(0xffffffffu, (unsigned)mine);
-        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&p.st->committed, mine);
+        committed += mine;
         grid.sync();
         // ---- a rejected attempt is deferred when a lower-index valid attempt
         // claimed one of its slots or a pair entry it checked, or a lower-index
@@ -260,10 +277,7 @@ k_ms_rounds(MsArgs p)
             if (t.state == 1)
                 defer |= p.table[t.h[0]] < me || p.table[t.h[1]] < me || p.pair_wr[t.h[0]] < me ||
                          p.pair_wr[t.h[1]] < me;
-            if (defer) {
-                pnext[atomicAdd(&p.st->n_pending[cur ^ 1], 1ULL)] = t.a;
-                atomicMin(&p.st->oldest[cur ^ 1], t.a);
-            }
+            if (defer) ms_defer(t.a, base, p.st, cur ^ 1, pnext);
         }
         fresh += take;
         if (tid == 0) p.st->rounds = round + 1;
@@ -272,6 +286,8 @@ k_ms_rounds(MsArgs p)
         pend = pnext;
         pnext = tmp;
     }
+    committed = __reduce_add_sync(0xffffffffu, (unsigned)committed);
+    if ((threadIdx.x & 31) == 0 && committed) atomicAdd(&p.st->committed, committed);
 }
 
 // Rows of the rewired graph: R is unchanged (degrees are preserved), so each
