@@ -167,6 +167,14 @@ __device__ __forceinline__ void closure(float (&acc)[4][4], const float (*dg)[B 
     }
 }
 
+// min(a, b, c) in one instruction (sm_100)
+__device__ __forceinline__ float min3f(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 __device__ __forceinline__ void tile_load(float (&acc)[4][4], const float* src, int ld)
 {
     const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
@@ -340,16 +348,21 @@ __device__ __forceinline__ void fw_batch_body(const FwBatch& p)
                 acc[r][0] = v.x; acc[r][1] = v.y; acc[r][2] = v.z; acc[r][3] = v.w;
             }
             __syncthreads();
-#pragma unroll 8
-            for (int k = 0; k < B; k++) {
+            // two k per step through the three-input minimum: one ALU
+            // instruction per two updates (the min-plus is bound by that
+            // pipe); min is exact, so the result equals the one-k loop's
+#pragma unroll 4
+            for (int k = 0; k < B; k += 2) {
                 const float4 ai = *(const float4*)&sm.prod.at[k][ty * 4];
                 const float4 bj4 = *(const float4*)&sm.prod.bk[k][tx * 4];
-                const float av[4] = {ai.x, ai.y, ai.z, ai.w};
-                const float bv[4] = {bj4.x, bj4.y, bj4.z, bj4.w};
+                const float4 ai1 = *(const float4*)&sm.prod.at[k + 1][ty * 4];
+                const float4 bj1 = *(const float4*)&sm.prod.bk[k + 1][tx * 4];
+                const float av[4] = {ai.x, ai.y, ai.z, ai.w}, av1[4] = {ai1.x, ai1.y, ai1.z, ai1.w};
+                const float bv[4] = {bj4.x, bj4.y, bj4.z, bj4.w}, bv1[4] = {bj1.x, bj1.y, bj1.z, bj1.w};
 #pragma unroll
                 for (int r = 0; r < 4; r++)
 #pragma unroll
-                    for (int q = 0; q < 4; q++) acc[r][q] = fminf(acc[r][q], av[r] + bv[q]);
+                    for (int q = 0; q < 4; q++) acc[r][q] = min3f(acc[r][q], av[r] + bv[q], av1[r] + bv1[q]);
             }
 #pragma unroll
             for (int r = 0; r < 4; r++)
