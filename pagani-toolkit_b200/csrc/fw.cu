@@ -557,7 +557,11 @@ static pg_status fw_plan(pg_ctx* ctx, const pg_graph* const* graphs, int ng, boo
     for (int c = 1; c <= std::min(per2, 2); c++) cands.push_back({2, c});
     for (int c = 3; c <= std::min(per4, 4); c++) cands.push_back({4, c});
     TuneChoice best{2, std::min(per2, 2)};
-    const std::string key = tune_key("fw_batch", off > 0 ? (long long)std::sqrt((double)off / ng) : 0, ng);
+    // shape bucket: log2 of the rms padded graph size and log2 of the number
+    // of graphs (passed as the "mean degree" of the key); a 160- and a
+    // 512-graph batch of the same sizes must not share a choice
+    const long long rms = off > 0 ? (long long)std::sqrt((double)off / ng) : 0;
+    const std::string key = tune_key("fw_batch", rms, (long long)ng * std::max(1LL, rms));
     PG_TRY(tune_pick(ctx, key, cands, &best, [&](const TuneChoice& c) -> pg_status {
         P->minb = c.a;
         P->grid = ctx->sm_count * c.b;
