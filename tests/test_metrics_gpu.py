@@ -302,6 +302,28 @@ def test_newman_whole_grid_groups(ctx):
     assert nm == nm_or and np.array_equal(labels, lab_or)
 
 
+def test_newman_same_result_every_run(ctx):
+    """Once every pending group fits a team, groups run as soon as their
+    parent is decided, so the order in which they run and end changes from
+    call to call.  Labels, Q and every round's log line (iterations,
+    residual, eigenvalue) must not: each team's size is a function of its
+    group alone and labels are handed out in the reference's round order."""
+    from pagani import synth
+    bold = synth.bold_series(9000, 120, 10, 1234)
+    g, _ = ctx.build_graph(bold, mode="s", value=2.0, sign="abs")
+    runs = []
+    for _ in range(3):
+        log = []
+        labels, Q, nm = ctx.newman(g, log=log)
+        rounds = [l for l in log if l.startswith("Round:")]
+        runs.append((labels, Q, nm, rounds))
+    assert any("dependency-driven phase" in l and "(0 groups" not in l for l in log)
+    for labels, Q, nm, rounds in runs[1:]:
+        assert nm == runs[0][2] and Q == runs[0][1]
+        assert np.array_equal(labels, runs[0][0])
+        assert rounds == runs[0][3]
+
+
 def test_dense_brandes_levels_take_the_tensor_core_path(ctx):
     """Per-kernel profiling shows where Brandes ran: a dense graph takes two
     tensor-core launches (levels 2 and 3) and two gather launches per
