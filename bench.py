@@ -471,6 +471,7 @@ def kernel_case(args):
       fw_batch -- FW + Onnela of --graphs ROI graphs, n ~ U{90..1024} (k_fw_batch)
       gram     -- one split-BF16 build at 1 % (k_gram_tc)
       brandes  -- betweenness at 1 % (k_brandes, k_bc_dense)
+      newman   -- modularity at 1 % (k_nm_grid, k_nm_team)
     Prints one JSON line with the call's device time."""
     import torch
     import pagani
@@ -483,7 +484,7 @@ def kernel_case(args):
         call = lambda: ctx.fw_batched(graphs)  # noqa: E731
     else:
         bold = synth.bold_series(N_VOX, T_LEN, N_SIG, synth.subject_seed(2, 0))
-        sp = 1.0 if args.case in ("gram", "brandes") else COHORT_SPARSITY
+        sp = 1.0 if args.case in ("gram", "brandes", "newman") else COHORT_SPARSITY
         g, _ = ctx.build_graph(bold, mode="s", value=sp, sign="abs")
         m = g.info[1] // 2
         if args.case == "paths":
@@ -493,6 +494,8 @@ def kernel_case(args):
             call = lambda: ctx.maslov(g, 7, COHORT_SWAPS * m)[0].free()  # noqa: E731
         elif args.case == "gram":
             call = lambda: ctx.build_graph(bold, mode="s", value=1.0, sign="abs")[0].free()  # noqa: E731
+        elif args.case == "newman":
+            call = lambda: ctx.newman(g)  # noqa: E731
         else:
             call = lambda: ctx.betweenness(g)  # noqa: E731
     call()
@@ -521,7 +524,7 @@ def main():
                     help="subjects of the cohort configuration timed beside the step (0: skip)")
     ap.add_argument("--no-precision-report", action="store_true")
     ap.add_argument("--no-roi-batch", action="store_true", help="skip the 512-graph weighted batch figure")
-    ap.add_argument("--case", default="step", choices=["step", "paths", "maslov", "fw_batch", "gram", "brandes"],
+    ap.add_argument("--case", default="step", choices=["step", "paths", "maslov", "fw_batch", "gram", "brandes", "newman"],
                     help="profiling aid: one small workload of one kernel family instead of the benchmark")
     ap.add_argument("--graphs", type=int, default=64, help="--case fw_batch: graphs in the batch")
     ap.add_argument("--voxels", type=int, default=N_VOX,
