@@ -92,10 +92,9 @@ k_msbfs_all(PathArgs p)
                 found_total += (unsigned)cnt;
             }
             for (int o = 16; o; o >>= 1) found_total += __shfl_xor_sync(0xffffffffu, found_total, o);
-            if (lane == 0 && found_total) {
-                p.flags[1] = 1;
-                if (p.hist && 1 <= p.max_hop) atomicAdd(&p.hist[1], found_total);
-            }
+            if (lane == 0 && found_total && p.hist && 1 <= p.max_hop) atomicAdd(&p.hist[1], found_total);
+            // one store per CTA: a store per warp to the same flag serialised in L2
+            if (__syncthreads_or(found_total != 0) && threadIdx.x == 0) p.flags[1] = 1;
         }
         grid.sync();
         if (tid == 0) p.flags[0] = 0;
@@ -159,10 +158,8 @@ k_msbfs_all(PathArgs p)
                 }
                 found_total += (unsigned)cnt;
             }
-            if (lane == 0 && found_total) {
-                p.flags[d % 3] = 1;
-                if (p.hist && d <= p.max_hop) atomicAdd(&p.hist[d], found_total);
-            }
+            if (lane == 0 && found_total && p.hist && d <= p.max_hop) atomicAdd(&p.hist[d], found_total);
+            if (__syncthreads_or(found_total != 0) && threadIdx.x == 0) p.flags[d % 3] = 1;
             grid.sync();
             if (tid == 0) p.flags[(d + 2) % 3] = 0;   // last read before this barrier, next written after the next
             if (!((volatile int*)p.flags)[d % 3]) break;
