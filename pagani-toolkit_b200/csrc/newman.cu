@@ -1371,6 +1371,7 @@ struct NmAsync {
         int stream = -1;
         int child = -1;        // tree index of the first child; the second follows
         bool split = false;
+        bool grid = false;     // ran on the whole grid before the phase began
         int parent = -1;
         double out[OUT_W] = {};
         // launch arguments, kept while the group waits for SMs
@@ -1425,6 +1426,7 @@ struct NmAsync {
     // small kernels that build the next children; without it those kernels
     // queued behind the teams for tens of ms
     int inflight = 0, budget = 0;
+    bool no_fit = false;       // a child too large for a team (only after an early start)
 
     pg_status take_stream(int* out)
     {
@@ -1598,7 +1600,10 @@ struct NmAsync {
         b.E = EB;
         a.c = pick_cluster(so, bt.nA);
         b.c = pick_cluster(so + bt.nA, bt.P - bt.nA);
-        if (!a.c || !b.c) return pg_fail(ctx, PG_ERR_INTERNAL, "modularity: a child group does not fit a team");
+        if (!a.c || !b.c) {
+            no_fit = true;
+            return pg_fail(ctx, PG_ERR_INTERNAL, "modularity: a child group does not fit a team");
+        }
         cudaStream_t st = ctx->pool[bt.stream];
         PG_CUDA(ctx, cudaMemcpyAsync(aeoff + b4, heoff + b4, 3 * sizeof(long long), cudaMemcpyHostToDevice, st));
         const int wblocks = std::max(1, std::min((bt.P + 7) / 8, ctx->sm_count * 4));
@@ -1711,9 +1716,14 @@ struct NmAsync {
 // The partition of pg_newman; wv (device, wn values) is the weighted tool's
 // value array, null for the unweighted tool.
 static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, long long wn, int32_t gpu_rule_above,
-                            int32_t* labels, double* Q, int32_t* n_modules, pg_log_fn log, void* user)
+                            int32_t* labels, double* Q, int32_t* n_modules, pg_log_fn log, void* user, bool early_ok,
+                            bool* retry)
 {
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    // log lines are handed to `log` when the call succeeds, so that a call
+    // run again (see pg_newman) reports every round once
+    std::vector<std::string> lines;
+    auto emit = [&](const char* l) { lines.emplace_back(l); };
     const bool weighted = wv != nullptr;
     auto k_coop = weighted ? k_nm_coop<true> : k_nm_coop<false>;
     auto k_grid = weighted ? k_nm_grid<true> : k_nm_grid<false>;
@@ -1928,7 +1938,53 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 csz[best] *= 2;
             }
         }
-        if (large.empty()) {
+        // whole-grid groups first (each needs the whole GPU).  When every
+        // child of theirs fits a team, the dependency-driven phase starts
+        // right after them and takes this generation's teams along, instead
+        // of running those alone and holding every child back until the
+        // generation is decided
+        std::vector<double> hout((size_t)G * OUT_W, 0.0);
+        bool early = false;
+        if (!large.empty()) {
+            auto t0 = now();
+            for (int q : large) {
+                int qq = q;
+                // column blocks as large as the shared memory of the CTA with the
+                // most rows allows; the gather kernel when even 1024 do not fit
+                const int ng = (int)(hgoff[q + 1] - hgoff[q]);
+                std::vector<int32_t> rel(ng + 1);
+                for (int p = 0; p <= ng; p++) rel[p] = (int32_t)(hsoff[hgoff[q] + p] - heoff[q]);
+                int most = 0;
+                for (int r = 0; r < coop_grid; r++)
+                    most = std::max(most, team_split(rel.data(), ng, r + 1, coop_grid) - team_split(rel.data(), ng, r, coop_grid));
+                int cb_log = 0;
+                for (int lg = 14; lg >= 10 && !cb_log; lg--) {
+                    const int nblk = (ng + (1 << lg) - 1) >> lg;
+                    if (grid_layout(most, nblk, 1 << lg).need <= smem_cap) cb_log = lg;
+                }
+                if (cb_log && grid_per_sm >= 1) {
+                    const size_t need = grid_layout(most, (ng + (1 << cb_log) - 1) >> cb_log, 1 << cb_log).need;
+                    void* args[] = {(void*)&qq, (void*)&in, (void*)&part, (void*)&c16, (void*)&cb_log};
+                    PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_grid, dim3(coop_grid), dim3(COOP_THREADS), args,
+                                                             need, ctx->stream));
+                } else {
+                    void* args[] = {(void*)&qq, (void*)&in, (void*)&part};
+                    PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_coop, dim3(coop_grid), dim3(COOP_THREADS), args, 0,
+                                                             ctx->stream));
+                }
+                PG_LAUNCHED(ctx);
+            }
+            PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * OUT_W));
+            t_large += ms_since(t0);
+            for (int q : large) it_large += (long long)(hout[(size_t)q * OUT_W + 1] + hout[(size_t)q * OUT_W + 3]);
+            early = early_ok;
+            for (int q : large) {
+                const double* o = &hout[(size_t)q * OUT_W];
+                const long long subP = (long long)o[5], subN = (long long)o[6];
+                if (o[0] > LAMBDA && subP > 1 && subN > 1 && (subP > TEAM_MAX_ROWS || subN > TEAM_MAX_ROWS)) early = false;
+            }
+        }
+        if (large.empty() || early) {
             // ---- every pending group fits a team: dependency-driven from here on
             auto t_as = now();
             as.ctx = ctx;
@@ -1969,9 +2025,20 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 as.tree.push_back(nd);
             }
             as.budget = std::max(max_cluster, ctx->sm_count - RESERVE_SMS);
+            for (int q : large) {   // already run on the whole grid (early start only)
+                NmAsync::Node& nd = as.tree[q];
+                nd.c = 0;
+                nd.grid = true;
+                PG_TRY(as.take_stream(&nd.stream));
+                std::memcpy(as.hout + (size_t)OUT_W * q, &hout[(size_t)q * OUT_W], sizeof(double) * OUT_W);
+                as.hout[(size_t)OUT_W * q + 8] = as.hout[(size_t)OUT_W * q + 9] = 0.0;   // not a team: no clock
+                PG_TRY(pg_d2h(ctx, as.hv + nd.s, v + nd.s, sizeof(double) * nd.n));
+                as.hdone[q] = 1;
+                as.running.push_back(q);
+            }
             for (int q = 0; q < G; q++) {
                 NmAsync::Node& nd = as.tree[q];
-                if (nd.n == 0) continue;
+                if (nd.n == 0 || nd.grid) continue;
                 nd.c = as.pick_cluster(&hsoff[hgoff[q]], nd.n);
                 if (!nd.c) return pg_fail(ctx, PG_ERR_INTERNAL, "modularity: a group does not fit a team");
                 nd.in = in0;
@@ -1980,7 +2047,15 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 nd.dep = ctx->ev[0];
                 as.queued.push_back(q);
             }
-            PG_TRY(as.run());
+            {
+                const pg_status st = as.run();
+                if (st != PG_OK) {
+                    // a child of a whole-grid group did not fit a team: the
+                    // caller runs the call again without the early start
+                    if (retry) *retry = as.no_fit && early;
+                    return st;
+                }
+            }
             t_async += ms_since(t_as);
             // ---- the reference's rounds over the finished tree, in order
             std::vector<int> round_tree((size_t)hi + as.tree.size() + 4, -1);
@@ -1993,14 +2068,14 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 ref_of[t] = round;
                 const NmAsync::Node& nd = as.tree[t];
                 const double* o = nd.out;
-                it_async += (long long)(o[1] + o[3]);
+                if (!nd.grid) it_async += (long long)(o[1] + o[3]);
                 if (log) {
                     int len = snprintf(line, sizeof line, "Round:\t%d\tnumber of nodes:\t%d\tIterations:\t%d\tresidual:\t%g\t",
                                        round, nd.n, (int)o[1], o[2]);
                     if (o[7] != 0.0)
                         len += snprintf(line + len, sizeof line - len, "Iterations:\t%d\tresidual:\t%g\t", (int)o[3], o[4]);
                     snprintf(line + len, sizeof line - len, "Eigen Value: %g\tDivide?: %d", o[0], (int)nd.split);
-                    log(line, user);
+                    emit(line);
                 }
                 if (nd.split) {
                     round_tree[Max_Result + 1] = nd.child;
@@ -2019,7 +2094,7 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 int last = -1;
                 for (size_t t = 0; t < as.tree.size(); t++) {
                     const NmAsync::Node& nd = as.tree[t];
-                    if (nd.n == 0) continue;
+                    if (nd.n == 0 || nd.grid) continue;
                     t_begin = std::min(t_begin, nd.out[8]);
                     if (nd.out[9] > t_end) {
                         t_end = nd.out[9];
@@ -2053,7 +2128,6 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
             bk.e = lists.size();
             if (bk.e > bk.b) buckets.push_back(bk);
         }
-        std::vector<double> hout((size_t)G * OUT_W, 0.0);
         if (!lists.empty())
             PG_CUDA(ctx, cudaMemcpyAsync(glist, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice,
                                          ctx->stream));
@@ -2093,38 +2167,8 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
             PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         }
         t_small += ms_since(t0);
-        t0 = now();
-        for (int q : large) {
-            int qq = q;
-            // column blocks as large as the shared memory of the CTA with the
-            // most rows allows; the gather kernel when even 1024 do not fit
-            const int ng = (int)(hgoff[q + 1] - hgoff[q]);
-            std::vector<int32_t> rel(ng + 1);
-            for (int p = 0; p <= ng; p++) rel[p] = (int32_t)(hsoff[hgoff[q] + p] - heoff[q]);
-            int most = 0;
-            for (int r = 0; r < coop_grid; r++)
-                most = std::max(most, team_split(rel.data(), ng, r + 1, coop_grid) - team_split(rel.data(), ng, r, coop_grid));
-            int cb_log = 0;
-            for (int lg = 14; lg >= 10 && !cb_log; lg--) {
-                const int nblk = (ng + (1 << lg) - 1) >> lg;
-                if (grid_layout(most, nblk, 1 << lg).need <= smem_cap) cb_log = lg;
-            }
-            if (cb_log && grid_per_sm >= 1) {
-                const size_t need = grid_layout(most, (ng + (1 << cb_log) - 1) >> cb_log, 1 << cb_log).need;
-                void* args[] = {(void*)&qq, (void*)&in, (void*)&part, (void*)&c16, (void*)&cb_log};
-                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_grid, dim3(coop_grid), dim3(COOP_THREADS), args,
-                                                         need, ctx->stream));
-            } else {
-                void* args[] = {(void*)&qq, (void*)&in, (void*)&part};
-                PG_CUDA(ctx, cudaLaunchCooperativeKernel((void*)k_coop, dim3(coop_grid), dim3(COOP_THREADS), args, 0,
-                                                         ctx->stream));
-            }
-            PG_LAUNCHED(ctx);
-        }
         PG_TRY(pg_d2h(ctx, hout.data(), out, sizeof(double) * G * OUT_W));
-        t_large += ms_since(t0);
         for (int q : team) it_small += (long long)(hout[(size_t)q * OUT_W + 1] + hout[(size_t)q * OUT_W + 3]);
-        for (int q : large) it_large += (long long)(hout[(size_t)q * OUT_W + 1] + hout[(size_t)q * OUT_W + 3]);
         // ---- decisions in round order (labels exactly as the sequential reference)
         std::vector<int> hbase(G, -1);
         std::vector<double> hcoef(G, 0.0);
@@ -2142,7 +2186,7 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
                 if (o[7] != 0.0)
                     len += snprintf(line + len, sizeof line - len, "Iterations:\t%d\tresidual:\t%g\t", (int)o[3], o[4]);
                 snprintf(line + len, sizeof line - len, "Eigen Value: %g\tDivide?: %d", o[0], (int)issub);
-                log(line, user);
+                emit(line);
             }
             if (issub) {
                 hbase[q] = Max_Result;
@@ -2188,14 +2232,15 @@ static pg_status newman_run(pg_ctx* ctx, const pg_graph* g, const float* wv, lon
     if (n_modules) *n_modules = Module_Num;
     if (log) {
         snprintf(line, sizeof line, "Number of Modules: %d,\tQ=%.6g", Module_Num, q);
-        log(line, user);
+        emit(line);
         snprintf(line, sizeof line,
                  "Timing (ms): generations %d, setup %.1f, team groups %.1f (%lld iterations), "
                  "cooperative groups %.1f (%lld), dependency-driven phase %.1f (%d groups, %lld iterations; "
                  "device span %.1f, last chain %d groups running %.1f, mean team CTAs busy %.1f)",
                  generations, t_setup, t_small, it_small, t_large, it_large, t_async, async_groups, it_async, span_ms,
                  chain_groups, chain_ms, busy_ctas);
-        log(line, user);
+        emit(line);
+        for (const std::string& l : lines) log(l.c_str(), user);
     }
     return PG_OK;
 }
@@ -2204,7 +2249,10 @@ extern "C" pg_status pg_newman(pg_ctx* ctx, const pg_graph* g, int32_t gpu_rule_
                                int32_t* n_modules, pg_log_fn log, void* user)
 {
     if (!ctx || !g || !labels) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman: null argument");
-    return newman_run(ctx, g, nullptr, 0, gpu_rule_above, labels, Q, n_modules, log, user);
+    bool retry = false;
+    const pg_status st = newman_run(ctx, g, nullptr, 0, gpu_rule_above, labels, Q, n_modules, log, user, true, &retry);
+    if (st == PG_OK || !retry) return st;
+    return newman_run(ctx, g, nullptr, 0, gpu_rule_above, labels, Q, n_modules, log, user, false, nullptr);
 }
 
 extern "C" pg_status pg_newman_weighted(pg_ctx* ctx, const pg_graph* g, const pg_graph* weights_of,
@@ -2215,5 +2263,8 @@ extern "C" pg_status pg_newman_weighted(pg_ctx* ctx, const pg_graph* g, const pg
     const pg_graph* w = weights_of ? weights_of : g;
     if (!w->V) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman_weighted: the weight graph has no weights");
     if (w->device != g->device) return pg_fail(ctx, PG_ERR_INVALID, "pg_newman_weighted: graphs on different devices");
-    return newman_run(ctx, g, w->V, w->nnz, gpu_rule_above, labels, Q, n_modules, log, user);
+    bool retry = false;
+    const pg_status st = newman_run(ctx, g, w->V, w->nnz, gpu_rule_above, labels, Q, n_modules, log, user, true, &retry);
+    if (st == PG_OK || !retry) return st;
+    return newman_run(ctx, g, w->V, w->nnz, gpu_rule_above, labels, Q, n_modules, log, user, false, nullptr);
 }
