@@ -177,7 +177,7 @@ __device__ __forceinline__ void ms_defer(unsigned long long a, unsigned long lon
     if (g.thread_rank() == 0) atomicMin(&st->oldest[slot], base + rel);
 }
 
-__global__ void __launch_bounds__(MS_THREADS)
+__global__ void __launch_bounds__(MS_THREADS, 4)   // four CTAs per SM: at most two attempts per thread a round
 k_ms_rounds(MsArgs p)
 {
     cg::grid_group grid = cg::this_grid();
@@ -207,61 +207,105 @@ k_ms_rounds(MsArgs p)
             p.st->n_pending[cur ^ 1] = 0;
             p.st->oldest[cur ^ 1] = ~0ULL;
         }
+        // Every phase takes a thread's attempts two at a time and issues the
+        // loads of both before either result is used: a round has more
+        // attempts than resident threads, and the barrier after each phase
+        // waits for the threads with two dependent memory chains.  Within a
+        // phase no attempt writes what another reads, so the order inside a
+        // thread changes nothing.
         // ---- evaluate on the round's state; valid attempts claim
-        for (long long it = tid; it < (long long)total; it += nt) {
-            MsItem t;
-            t.a = it < (long long)np ? pend[it] : fresh + (it - np);
-            const uint64_t h1 = stream_bits(key, 2 * t.a), h2 = stream_bits(key, 2 * t.a + 1);
-            t.i = (int)(h1 % (uint64_t)p.M);
-            t.j = (int)(h2 % (uint64_t)p.M);
-            t.coin = (int)((h1 >> 63) ^ (h2 >> 63));
-            t.v[0] = p.ea[t.i]; t.v[1] = p.eb[t.i]; t.v[2] = p.ea[t.j]; t.v[3] = p.eb[t.j];
-            const int x1 = t.v[0], x2 = t.coin ? t.v[2] : t.v[3];   // new pair 1: 1-3 or 1-4
-            const int y1 = t.v[1], y2 = t.coin ? t.v[3] : t.v[2];   // new pair 2: 2-4 or 2-3
-            t.h[0] = pair_slot(x1, x2, n, p.hmask);
-            t.h[1] = pair_slot(y1, y2, n, p.hmask);
-            if (t.v[0] == t.v[2] || t.v[0] == t.v[3] || t.v[1] == t.v[2] || t.v[1] == t.v[3]) t.state = 0;
-            else if (has_edge(p.bits, n, x1, x2) || has_edge(p.bits, n, y1, y2)) t.state = 1;
-            else t.state = 2;
-            if (t.state == 2) {
-                const unsigned long long me = tag | (uint32_t)(t.a - base);
-                atomicMin(&p.slot_owner[t.i], me);
-                atomicMin(&p.slot_owner[t.j], me);
-                atomicMin(&p.table[t.h[0]], me);
-                atomicMin(&p.table[t.h[1]], me);
+        for (long long it0 = tid; it0 < (long long)total; it0 += 2 * nt) {
+            MsItem t[2];
+            bool ok[2], shared[2], e1[2], e2[2];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const long long it = it0 + k * nt;
+                ok[k] = it < (long long)total;
+                const long long ic = ok[k] ? it : it0;   // an idle half repeats the first attempt's reads
+                t[k].a = ic < (long long)np ? pend[ic] : fresh + (ic - np);
+                const uint64_t h1 = stream_bits(key, 2 * t[k].a), h2 = stream_bits(key, 2 * t[k].a + 1);
+                t[k].i = (int)(h1 % (uint64_t)p.M);
+                t[k].j = (int)(h2 % (uint64_t)p.M);
+                t[k].coin = (int)((h1 >> 63) ^ (h2 >> 63));
             }
-            items[it] = t;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                t[k].v[0] = p.ea[t[k].i]; t[k].v[1] = p.eb[t[k].i]; t[k].v[2] = p.ea[t[k].j]; t[k].v[3] = p.eb[t[k].j];
+            }
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int x1 = t[k].v[0], x2 = t[k].coin ? t[k].v[2] : t[k].v[3];   // new pair 1: 1-3 or 1-4
+                const int y1 = t[k].v[1], y2 = t[k].coin ? t[k].v[3] : t[k].v[2];   // new pair 2: 2-4 or 2-3
+                t[k].h[0] = pair_slot(x1, x2, n, p.hmask);
+                t[k].h[1] = pair_slot(y1, y2, n, p.hmask);
+                shared[k] = t[k].v[0] == t[k].v[2] || t[k].v[0] == t[k].v[3] || t[k].v[1] == t[k].v[2] ||
+                            t[k].v[1] == t[k].v[3];
+                // both probes (only of distinct end points, which the bitmap indexes)
+                e1[k] = !shared[k] && has_edge(p.bits, n, x1, x2);
+                e2[k] = !shared[k] && has_edge(p.bits, n, y1, y2);
+            }
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                if (!ok[k]) continue;
+                t[k].state = shared[k] ? 0 : (e1[k] || e2[k]) ? 1 : 2;
+                if (t[k].state == 2) {
+                    const unsigned long long me = tag | (uint32_t)(t[k].a - base);
+                    atomicMin(&p.slot_owner[t[k].i], me);
+                    atomicMin(&p.slot_owner[t[k].j], me);
+                    atomicMin(&p.table[t[k].h[0]], me);
+                    atomicMin(&p.table[t[k].h[1]], me);
+                }
+                items[it0 + k * nt] = t[k];
+            }
         }
         grid.sync();
         // ---- valid attempts owning all four claims commit (their writes are
         // recorded, then applied); valid attempts that lost are deferred
         unsigned long long mine = 0;
-        for (long long it = tid; it < (long long)total; it += nt) {
-            const MsItem t = items[it];
-            if (t.state != 2) continue;
-            const unsigned long long me = tag | (uint32_t)(t.a - base);
-            if (!(p.slot_owner[t.i] == me && p.slot_owner[t.j] == me && p.table[t.h[0]] == me &&
-                  p.table[t.h[1]] == me)) {
-                ms_defer(t.a, base, p.st, cur ^ 1, pnext);
-                continue;
+        for (long long it0 = tid; it0 < (long long)total; it0 += 2 * nt) {
+            MsItem t[2];
+            bool ok[2];
+            unsigned long long c[2][4];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const long long it = it0 + k * nt;
+                ok[k] = it < (long long)total;
+                t[k] = items[ok[k] ? it : it0];
+                ok[k] = ok[k] && t[k].state == 2;
             }
-            atomicMin(&p.pair_wr[pair_slot(t.v[0], t.v[1], n, p.hmask)], me);   // the pairs it removes
-            atomicMin(&p.pair_wr[pair_slot(t.v[2], t.v[3], n, p.hmask)], me);
-            const int V1 = t.v[0], V2 = t.v[1], V3 = t.v[2], V4 = t.v[3];
-            put_edge(p.bits, n, V1, V2, false);
-            put_edge(p.bits, n, V3, V4, false);
-            if (t.coin) {   // 1-3, 2-4 (Maslov.cpp:36-44)
-                put_edge(p.bits, n, V1, V3, true);
-                put_edge(p.bits, n, V2, V4, true);
-                p.eb[t.i] = V3;
-                p.ea[t.j] = V2;
-            } else {        // 1-4, 3-2 (Maslov.cpp:47-56)
-                put_edge(p.bits, n, V1, V4, true);
-                put_edge(p.bits, n, V2, V3, true);
-                p.eb[t.i] = V4;
-                p.eb[t.j] = V2;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                c[k][0] = p.slot_owner[t[k].i];
+                c[k][1] = p.slot_owner[t[k].j];
+                c[k][2] = p.table[t[k].h[0]];
+                c[k][3] = p.table[t[k].h[1]];
             }
-            mine++;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                if (!ok[k]) continue;
+                const unsigned long long me = tag | (uint32_t)(t[k].a - base);
+                if (!(c[k][0] == me && c[k][1] == me && c[k][2] == me && c[k][3] == me)) {
+                    ms_defer(t[k].a, base, p.st, cur ^ 1, pnext);
+                    continue;
+                }
+                atomicMin(&p.pair_wr[pair_slot(t[k].v[0], t[k].v[1], n, p.hmask)], me);   // the pairs it removes
+                atomicMin(&p.pair_wr[pair_slot(t[k].v[2], t[k].v[3], n, p.hmask)], me);
+                const int V1 = t[k].v[0], V2 = t[k].v[1], V3 = t[k].v[2], V4 = t[k].v[3];
+                put_edge(p.bits, n, V1, V2, false);
+                put_edge(p.bits, n, V3, V4, false);
+                if (t[k].coin) {   // 1-3, 2-4 (Maslov.cpp:36-44)
+                    put_edge(p.bits, n, V1, V3, true);
+                    put_edge(p.bits, n, V2, V4, true);
+                    p.eb[t[k].i] = V3;
+                    p.ea[t[k].j] = V2;
+                } else {        // 1-4, 3-2 (Maslov.cpp:47-56)
+                    put_edge(p.bits, n, V1, V4, true);
+                    put_edge(p.bits, n, V2, V3, true);
+                    p.eb[t[k].i] = V4;
+                    p.eb[t[k].j] = V2;
+                }
+                mine++;
+            }
         }
         committed += mine;
         grid.sync();
@@ -269,15 +313,35 @@ k_ms_rounds(MsArgs p)
         // claimed one of its slots or a pair entry it checked, or a lower-index
         // commit removes a pair it checked (conservative: the claimant may not
         // have committed)
-        for (long long it = tid; it < (long long)total; it += nt) {
-            const MsItem t = items[it];
-            if (t.state >= 2) continue;
-            const unsigned long long me = tag | (uint32_t)(t.a - base);
-            bool defer = p.slot_owner[t.i] < me || p.slot_owner[t.j] < me;
-            if (t.state == 1)
-                defer |= p.table[t.h[0]] < me || p.table[t.h[1]] < me || p.pair_wr[t.h[0]] < me ||
-                         p.pair_wr[t.h[1]] < me;
-            if (defer) ms_defer(t.a, base, p.st, cur ^ 1, pnext);
+        for (long long it0 = tid; it0 < (long long)total; it0 += 2 * nt) {
+            MsItem t[2];
+            bool ok[2];
+            unsigned long long c[2][6];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const long long it = it0 + k * nt;
+                ok[k] = it < (long long)total;
+                t[k] = items[ok[k] ? it : it0];
+                ok[k] = ok[k] && t[k].state < 2;
+            }
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                c[k][0] = p.slot_owner[t[k].i];
+                c[k][1] = p.slot_owner[t[k].j];
+                const bool chk = t[k].state == 1;
+                c[k][2] = chk ? p.table[t[k].h[0]] : ~0ULL;
+                c[k][3] = chk ? p.table[t[k].h[1]] : ~0ULL;
+                c[k][4] = chk ? p.pair_wr[t[k].h[0]] : ~0ULL;
+                c[k][5] = chk ? p.pair_wr[t[k].h[1]] : ~0ULL;
+            }
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                if (!ok[k]) continue;
+                const unsigned long long me = tag | (uint32_t)(t[k].a - base);
+                const bool defer = c[k][0] < me || c[k][1] < me || c[k][2] < me || c[k][3] < me || c[k][4] < me ||
+                                   c[k][5] < me;
+                if (defer) ms_defer(t[k].a, base, p.st, cur ^ 1, pnext);
+            }
         }
         fresh += take;
         if (tid == 0) p.st->rounds = round + 1;
